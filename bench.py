@@ -1,0 +1,355 @@
+"""Benchmark of the direct Fourier inversion hot path (FourierReconstructor
+insert_slice pipeline) on B200.
+
+One step = one batch of particles through the reference caller's per-particle
+pipeline (edge-mean, pad, CTF phase flip, shift, r2c) and the insertion of all
+symmetry copies into the resident volume.  Default workload: box 256 padded to
+384, gauss_5, d7, CTF, SNR 0.02 (the large single job of the reference's
+make3d use), synthetic seeded particles.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl gpu|reference]
+
+Prints one JSON line.  Multi-GPU runs are independent replicas (one
+reconstruction per GPU, no collective on the data path): value is the sum of
+particle-slices over ranks divided by the slowest rank's device time.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    # name: box, pad, mode, sym, ctf, snr, shift, weights, particles in the full job
+    "c4": dict(box=256, N=384, mode="gauss_5", sym="d7", ctf=True, snr=0.02, shift=4.0,
+               weights=(0.5, 1.0), job=200_000,
+               desc="box 256 pad 384, gauss_5, d7, CTF, SNR 0.02 (200k-particle job)"),
+    "c2": dict(box=128, N=192, mode="gauss_2", sym="c1", ctf=True, snr=0.05, shift=4.0,
+               weights=(0.5, 1.0), job=20_000,
+               desc="box 128 pad 192, gauss_2, c1, CTF, SNR 0.05 (20k-particle job)"),
+    "c1": dict(box=64, N=96, mode="gauss_2", sym="c1", ctf=False, snr=0.1, shift=2.0,
+               weights=None, job=2_000, desc="box 64 pad 96, gauss_2, c1 (2k-particle job)"),
+}
+
+
+def nsym_of(sym: str) -> int:
+    k, n = sym[0], int(sym[1:] or 1)
+    return n if k == "c" else 2 * n
+
+
+def pixels_per_slice(N: int) -> int:
+    """p(N): pixels kept by do_insert_slice_work (round(hypot) <= N/2)."""
+    n2 = N // 2
+    c = 0
+    for y in range(-n2, n2):
+        for x in range(0, n2 + 1):
+            if int(float(np.float32(np.hypot(x, y))) + 0.5) <= n2:
+                c += 1
+    return c
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi samples during the timed region (SM clock, throttle reasons)."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index),
+                                      f"--query-gpu={self.Q}", "--format=csv,noheader,nounits"],
+                                     capture_output=True, text=True, timeout=5).stdout.strip()
+                if out:
+                    self.rows.append([c.strip() for c in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4)
+                          if len(r) > 5 + i and r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+# ------------------------------------------------------------------ helpers
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return ws, rank, local
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(v: float, ws: int) -> float:
+    if ws == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], device="cuda", dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def load_traffic(workload: str, batch: int):
+    """DRAM traffic of one gather launch from the committed ncu summary,
+    scaled to `batch` particles (traffic grows with the particles staged and
+    is flat in the volume term): None when no capture exists."""
+    path = os.path.join(ROOT, "profiles", "gather_traffic.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        e = d[workload]
+        return float(e["fixed_bytes"]) + float(e["bytes_per_particle"]) * batch
+    except Exception:
+        return None
+
+
+# ------------------------------------------------------------------ CPU baseline
+def cpu_sample(wl: dict, seed: int, budget_s: float = 15.0, max_n: int = 64, threads: int = 0):
+    """The oracle's FP32 restatement (-O3 -ffast-math, OpenMP with private
+    volumes) on a bounded sample of the workload: prologue (numpy FFT) and
+    insertion.  Returns (particle-slices/s, sample size, threads, seconds)."""
+    from eman2_b200.synth import make_particles
+    from oracle import oracle
+    threads = threads or os.cpu_count() or 1
+    N, box = wl["N"], wl["box"]
+    n = max(1, min(max_n, threads))
+    total_n, total_t = 0, 0.0
+    vol = oracle.OracleVolume(N, "omp")
+    k = 0
+    while total_t < budget_s and total_n < max_n:
+        ps = make_particles(box, n, seed=seed + k, snr=wl["snr"], shift=wl["shift"],
+                            weights=wl["weights"], ctf=wl["ctf"])
+        t0 = time.perf_counter()
+        sl = np.stack([oracle.particle_to_slice(ps.images[i], N, ps.shifts[i],
+                                                {"defocus": float(ps.defocus[i])} if wl["ctf"] else None)
+                       for i in range(n)])
+        vol.insert_omp(sl, ps.rots, ps.weights, wl["mode"], wl["sym"], threads=threads)
+        total_t += time.perf_counter() - t0
+        total_n += n
+        k += 1
+        if total_t < budget_s / 4:
+            n = min(max_n - total_n, n * 2) or n
+    return total_n / total_t, total_n, threads, total_t
+
+
+# ------------------------------------------------------------------ GPU run
+def run_gpu(args, wl, ws, rank, local):
+    import torch
+
+    from eman2_b200 import Reconstructors, _lib
+    from eman2_b200.particles import particle_meta
+    from eman2_b200.synth import make_particles
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    lib = _lib.load()
+    B, N, batch = wl["box"], wl["N"], args.batch
+    ps = make_particles(B, batch, seed=1000 + rank, snr=wl["snr"], shift=wl["shift"],
+                        weights=wl["weights"], ctf=wl["ctf"], device=dev)
+    d_imgs = ps.images if isinstance(ps.images, torch.Tensor) else torch.as_tensor(ps.images, device=dev)
+    meta = particle_meta(ps.rots, ps.shifts, ps.weights, defocus=ps.defocus)
+    r = Reconstructors.get("fourier", {"size": [N] * 3, "sym": wl["sym"], "mode": wl["mode"]})
+    r.setup()
+    stream = torch.cuda.Stream(device=dev)
+    _lib.check(lib.fr_set_stream(r.handle, ctypes.c_void_p(stream.cuda_stream)))
+
+    def step(src):
+        r.insert_particles(src, meta)
+
+    for _ in range(args.warmup):
+        step(d_imgs)
+    torch.cuda.synchronize()
+    _lib.check(lib.fr_profile(1))
+    _lib.check(lib.fr_stats_reset())
+    barrier(ws)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            step(d_imgs)
+        e1.record(stream)
+        e1.synchronize()
+    torch.cuda.synchronize()
+    barrier(ws)
+    ms = e0.elapsed_time(e1)
+    st = _lib.stats()
+    _lib.check(lib.fr_profile(0))
+    ms_max = max_over_ranks(ms, ws)
+
+    # e2e: the same steps through the public API from pinned host memory
+    h_imgs = d_imgs.cpu().pin_memory()
+    for _ in range(max(1, args.warmup // 2)):
+        step(h_imgs)
+    torch.cuda.synchronize()
+    barrier(ws)
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(args.steps):
+        step(h_imgs)
+    f1.record(stream)
+    f1.synchronize()
+    barrier(ws)
+    e2e_ms = max_over_ranks(f0.elapsed_time(f1), ws)
+
+    # plain per-call path: one particle per call (scatter insertion)
+    plain = None
+    if rank == 0 and args.plain > 0:
+        m1 = [particle_meta(ps.rots[i:i + 1], ps.shifts[i:i + 1], ps.weights[i:i + 1],
+                            defocus=ps.defocus[i:i + 1]) for i in range(args.plain)]
+        for i in range(3):
+            r.insert_particles(d_imgs[i:i + 1], m1[i], schedule="scatter")
+        torch.cuda.synchronize()
+        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        g0.record(stream)
+        for i in range(args.plain):
+            r.insert_particles(d_imgs[i:i + 1], m1[i], schedule="scatter")
+        g1.record(stream)
+        g1.synchronize()
+        plain = args.plain / (g0.elapsed_time(g1) / 1e3)
+    return ms_max, e2e_ms, st, clk.summary(), plain
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
+    ap.add_argument("--workload", default="c4", choices=sorted(WORKLOADS))
+    ap.add_argument("--batch", type=int, default=2048, help="particles per step")
+    ap.add_argument("--plain", type=int, default=64, help="particles timed on the plain path")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    wl = WORKLOADS[args.workload]
+    ws, rank, local = dist_setup()
+    S = nsym_of(wl["sym"])
+    N = wl["N"]
+    metric = "particle-slices inserted/s"
+    config = {"workload": f"{args.workload}: {wl['desc']}", "box": wl["box"], "pad": N,
+              "mode": wl["mode"], "sym": wl["sym"], "particles_per_step": args.batch,
+              "l2": "inputs larger than L2 (particles + volume > 126 MB)",
+              "parallelism": f"replicas x{ws}"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        from eman2_b200.synth import make_particles  # noqa: F401
+        vals = []
+        for k in range(args.warmup + args.steps):
+            v, n, thr, secs = cpu_sample(wl, seed=5000 + k, budget_s=8.0, max_n=32)
+            if k >= args.warmup:
+                vals.append((v, n, thr, secs))
+        val = float(np.mean([v for v, *_ in vals]))
+        line = {"impl": "reference", "metric": metric, "value": val, "unit": "particle-slices/s",
+                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": float(np.mean([s for *_, s in vals])) * 1e3,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic", "config": config,
+                "cpu_baseline": {"value": val, "unit": "particle-slices/s", "cores": vals[0][2],
+                                 "kind": "port",
+                                 "sample": f"{vals[0][1]} particles per step of the workload"},
+                "e2e": {"value": val, "unit": "particle-slices/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    ms, e2e_ms, st, clk, plain = run_gpu(args, wl, ws, rank, local)
+    if rank != 0:
+        return
+    value = ws * args.steps * args.batch / (ms / 1e3)
+    e2e = ws * args.steps * args.batch / (e2e_ms / 1e3)
+    V = (N // 2 + 1) * N * N
+    alg_bytes = args.batch * (8 * (N // 2 + 1) * N + 64) + 24 * V
+    glaunch = max(1, st["gather_launches"])
+    gms = st["gather_ms"] / glaunch
+    achieved = alg_bytes / (gms / 1e3) / 1e9
+    peak, peak_kind = load_peaks()
+    traffic = load_traffic(args.workload, args.batch)
+    p = pixels_per_slice(N)
+    taps_per = S * p * (216 if wl["mode"] == "gauss_5" else 8 if wl["mode"] == "gauss_2" else 1)
+    line = {
+        "metric": metric, "value": value, "unit": "particle-slices/s", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded Gaussian-blob phantom projections, CTF, noise)",
+        "config": config,
+        "e2e": {"value": e2e, "unit": "particle-slices/s",
+                "h2d_bytes_per_step": args.batch * wl["box"] * wl["box"] * 4 + args.batch * 76,
+                "d2h_bytes_per_step": 4},
+        "gpu_launches": int(st["kernel_launches"]),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
+                     "kernel": "k_gather",
+                     "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": gms},
+        "taps": {"per_particle_upper": taps_per,
+                 "per_s_upper": taps_per * args.batch / (gms / 1e3)},
+        "clocks": clk,
+    }
+    if plain is not None:
+        line["plain_gpu"] = {"value": plain, "unit": "particle-slices/s", "sample": args.plain,
+                             "speedup_batched_vs_plain": value / plain}
+    if not args.no_cpu and ws == 1:
+        v, n, thr, secs = cpu_sample(wl, seed=7000)
+        line["cpu_baseline"] = {"value": v, "unit": "particle-slices/s", "cores": thr,
+                                "kind": "port",
+                                "sample": f"{n} particles of the workload, {secs:.1f} s"}
+    print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,802 @@
+// fr_api.cu -- the C ABI (include/eman2_b200.h): reconstruction handles,
+// parameter checks, device memory, cuFFT plans and the dispatch of the
+// prologue / insertion / agreement / finish kernels.
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/eman2_b200.h"
+#include "fr_handle.h"
+
+namespace fr {
+
+// ------------------------------------------------------------------ errors
+static thread_local std::string g_err;
+
+int fail(int code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+// --------------------------------------------------------------- accounting
+static std::atomic<long long> g_launches{0}, g_ins_launches{0}, g_slices{0}, g_gather_launches{0};
+static std::atomic<int> g_profile{0};
+static std::mutex g_stat_mu;
+static double g_insert_ms = 0.0, g_gather_ms = 0.0;
+
+void note_launch(int n) { g_launches += n; }
+
+// ----------------------------------------------------------- device consts
+static std::mutex g_mu;
+static std::map<int, Consts> g_consts;
+static std::map<std::pair<int, int>, Geom *> g_geoms[64];
+
+Consts &consts() {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(g_mu);
+  auto it = g_consts.find(dev);
+  if (it != g_consts.end()) return it->second;
+  Consts c;
+  // Util::fast_exp table (libEM/util.cpp:793): (float)exp(-i/50.0).
+  float tab[1000];
+  for (int i = 0; i < 1000; i++) tab[i] = (float)std::exp(-i / 50.0);
+  cudaMalloc(&c.d_exp, sizeof tab);
+  cudaMemcpy(c.d_exp, tab, sizeof tab, cudaMemcpyHostToDevice);
+  cudaMalloc(&c.d_err, sizeof(int));
+  cudaMemset(c.d_err, 0, sizeof(int));
+  // h = 1.0f / EMConsts::I2G and 1.0f / EMConsts::I5G (libEM/emobject.cpp:53-56,
+  // libEM/reconstructor_tools.cpp:152,344).
+  volatile float i2g = (float)(4.0 / (M_PI * M_PI));
+  volatile float i5g = (float)(10.4 / (M_PI * M_PI));
+  c.h2 = 1.0f / i2g;
+  c.h5 = 1.0f / i5g;
+  return g_consts[dev] = c;
+}
+
+// Pixel selection of do_insert_slice_work (libEM/reconstructor.cpp:1178-1181):
+// keep (x,y) when Util::hypot_fast_int(x,y) = round(hypot(x,y)) <= N/2,
+// i.e. (int)(hypotf(x,y) + 0.5f) <= N/2; corners keeps every pixel.
+static int hypot_fast_int(int x, int y) {
+  const float h = (float)std::sqrt((double)x * x + (double)y * y);
+  return (int)(h + 0.5f);
+}
+
+Geom *get_geom(int N, int corners) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(g_mu);
+  auto key = std::make_pair(N, corners);
+  auto &m = g_geoms[dev & 63];
+  auto it = m.find(key);
+  if (it != m.end()) return it->second;
+  Geom *g = new Geom();
+  g->N = N;
+  g->corners = corners;
+  const int n2 = N / 2;
+  g->xmax.assign(N, -1);
+  std::vector<int> rim;
+  int npix = 0;
+  for (int y = -n2; y < n2; y++) {
+    int xm = -1;
+    for (int x = 0; x <= n2; x++) {
+      const int r = hypot_fast_int(x, y);
+      if (!corners && r > n2) continue;   // (r > iny/2 && abs(inx-iny) < 3): square input
+      xm = x;                              // kept pixels form a prefix of the row
+      npix++;
+      // Pixels that can reach a cube face (|i|, |j| or |k| = N/2): their
+      // points satisfy some |p_a| >= N/2 - 3.5, hence |p| >= N/2 - 3.5.
+      if (std::sqrt((double)x * x + (double)y * y) >= n2 - 3.6) rim.push_back(x | ((y + n2) << 16));
+    }
+    g->xmax[y + n2] = xm;
+  }
+  g->npix = npix;
+  std::vector<float> rtab(N + 2);
+  for (int i = -n2; i <= n2 + 1; i++) rtab[i + n2] = (float)i / (float)N;
+  cudaMalloc(&g->d_xmax, sizeof(int) * N);
+  cudaMemcpy(g->d_xmax, g->xmax.data(), sizeof(int) * N, cudaMemcpyHostToDevice);
+  cudaMalloc(&g->d_rtab, sizeof(float) * (N + 2));
+  cudaMemcpy(g->d_rtab, rtab.data(), sizeof(float) * (N + 2), cudaMemcpyHostToDevice);
+  g->nrim = (int)rim.size();
+  cudaMalloc(&g->d_rim, sizeof(int) * std::max<size_t>(1, rim.size()));
+  if (!rim.empty())
+    cudaMemcpy(g->d_rim, rim.data(), sizeof(int) * rim.size(), cudaMemcpyHostToDevice);
+  m[key] = g;
+  return g;
+}
+
+// ---------------------------------------------------------------- symmetry
+// Transform::set_rotation "eman" branch (libEM/transform.cpp:654-666).
+void eman_matrix(double az, double alt, double phi, float *m) {
+  const double d2r = 3.141592653589793238462643383279502884197169399 / 180.0;
+  const double azp = az * d2r, altp = alt * d2r, phip = phi * d2r;
+  m[0] = (float)(cos(phip) * cos(azp) - cos(altp) * sin(azp) * sin(phip));
+  m[1] = (float)(cos(phip) * sin(azp) + cos(altp) * cos(azp) * sin(phip));
+  m[2] = (float)(sin(altp) * sin(phip));
+  m[3] = (float)(-sin(phip) * cos(azp) - cos(altp) * sin(azp) * cos(phip));
+  m[4] = (float)(-sin(phip) * sin(azp) + cos(altp) * cos(azp) * cos(phip));
+  m[5] = (float)(sin(altp) * cos(phip));
+  m[6] = (float)(sin(altp) * sin(azp));
+  m[7] = (float)(-sin(altp) * cos(azp));
+  m[8] = (float)cos(altp);
+}
+
+// Symmetry3D::get_symmetries (libEM/symmetry.cpp:1240-1246) for the cyclic
+// (CSym::get_sym, :1407-1417) and dihedral (DSym::get_sym, :1452-1470) groups;
+// the name parse follows Factory<Symmetry3D>::get (:76-100): "c" -> c1.
+int sym_ops(const std::string &sym_in, std::vector<float> &out) {
+  std::string sym;
+  for (char ch : sym_in) sym.push_back((char)tolower((unsigned char)ch));
+  if (sym.empty()) return -1;
+  const char kind = sym[0];
+  if (kind != 'c' && kind != 'd') return -1;
+  int nsym = 1;
+  if (sym.size() > 1) {
+    for (size_t i = 1; i < sym.size(); i++)
+      if (sym[i] < '0' || sym[i] > '9') return -1;
+    nsym = atoi(sym.c_str() + 1);
+  }
+  if (nsym <= 0) return -1;
+  out.clear();
+  float m[9];
+  if (kind == 'c') {
+    for (int n = 0; n < nsym; n++) {
+      const float az = (float)(n % nsym) * 360.0f / (float)nsym;
+      eman_matrix((double)az, 0.0, 0.0, m);
+      out.insert(out.end(), m, m + 9);
+    }
+    return nsym;
+  }
+  const int ns = 2 * nsym;
+  for (int n = 0; n < ns; n++) {
+    float az, alt;
+    if (n >= ns / 2) { az = (float)((n % ns) - ns / 2) * 360.0f / (float)(ns / 2); alt = 180.0f; }
+    else { az = (float)(n % ns) * 360.0f / (float)(ns / 2); alt = 0.0f; }
+    eman_matrix((double)az, (double)alt, 0.0, m);
+    out.insert(out.end(), m, m + 9);
+  }
+  return ns;
+}
+
+// ------------------------------------------------------------ device memory
+bool is_device_ptr(const void *p) {
+  if (!p) return false;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+// Device view of a caller buffer: device pointers pass through; host buffers
+// are copied into `stage` on `st`.
+int to_device(const void *src, size_t bytes, DevBuf &stage, cudaStream_t st,
+                     const void **out) {
+  if (is_device_ptr(src)) { *out = src; return FR_OK; }
+  TRY(stage.ensure(bytes));
+  CU(cudaMemcpyAsync(stage.p, src, bytes, cudaMemcpyHostToDevice, st));
+  *out = stage.p;
+  return FR_OK;
+}
+
+int from_device(void *dst, const void *dsrc, size_t bytes, cudaStream_t st) {
+  if (is_device_ptr(dst)) {
+    CU(cudaMemcpyAsync(dst, dsrc, bytes, cudaMemcpyDeviceToDevice, st));
+    CU(cudaStreamSynchronize(st));
+  } else {
+    CU(cudaMemcpyAsync(dst, dsrc, bytes, cudaMemcpyDeviceToHost, st));
+    CU(cudaStreamSynchronize(st));
+  }
+  return FR_OK;
+}
+
+}  // namespace fr
+
+using namespace fr;
+
+namespace fr {
+
+size_t vol_floats(int N) { return (size_t)N * N * (N + 2); }
+size_t norm_floats(int N) { return (size_t)N * N * (N / 2 + 1); }
+size_t slice_floats(int N) { return (size_t)N * (N + 2); }
+
+
+int check_state(fr_recon *r) {
+  if (!r) return fail(FR_ENULL, "null reconstructor handle");
+  if (r->state != 1)
+    return fail(FR_ESTATE, r->state == 0 ? "setup() has not been called"
+                                         : "finish() was called; call setup() again");
+  return FR_OK;
+}
+
+// Builds the job view for the insertion kernels.
+InsertJob make_job(fr_recon *r, const float2 *slices, const float *t3d, const float *pw,
+                          int np) {
+  InsertJob j;
+  j.data = r->vol_data.as<float>();
+  j.norm = r->vol_norm.as<float>();
+  j.slices = slices;
+  j.t3d = t3d;
+  j.pw = pw;
+  j.xmax = r->geom->d_xmax;
+  j.rtab = r->geom->d_rtab;
+  j.rim = r->geom->d_rim;
+  j.nrim = r->geom->nrim;
+  j.ssnr = nullptr;
+  j.nssnr = 0;
+  j.sscale = 1.0f;
+  j.N = r->N;
+  j.mode = r->mode;
+  j.nsym = r->nsym;
+  j.np = np;
+  j.tiles_x = j.tiles_y = j.tiles_z = 0;
+  return j;
+}
+
+// Scatter (and edge) launches split so grid.y stays within 65535 slices.
+int run_scatter(const InsertJob &j0, bool edge_only, cudaStream_t st) {
+  const int per = std::max(1, 65535 / j0.nsym);
+  for (int p0 = 0; p0 < j0.np; p0 += per) {
+    InsertJob j = j0;
+    j.np = std::min(per, j0.np - p0);
+    j.slices = j0.slices + (size_t)p0 * j0.N * (j0.N / 2 + 1);
+    j.t3d = j0.t3d + (size_t)p0 * j0.nsym * 9;
+    j.pw = j0.pw + p0;
+    if (j0.ssnr) j.ssnr = j0.ssnr + (size_t)p0 * j0.nssnr;
+    CU(edge_only ? launch_edge(j, st) : launch_scatter(j, st));
+  }
+  return FR_OK;
+}
+
+// Inserts np device slices (t3d already composed, weights per particle).
+int insert_device(fr_recon *r, const float2 *d_slices, const float *d_t3d, const float *d_pw,
+                         int np, int schedule, const float *d_ssnr, int nssnr) {
+  if (np == 0) return FR_OK;
+  cudaStream_t st = r->stream;
+  InsertJob j = make_job(r, d_slices, d_t3d, d_pw, np);
+  if (d_ssnr) {
+    j.ssnr = d_ssnr;
+    j.nssnr = nssnr;
+    j.sscale = (float)(2.0 * (nssnr - 1) / (float)r->N);
+  }
+  const int tuned = tuned_tile(r->N, r->mode, r->nsym);
+  int sched = schedule;
+  if (sched == FR_SCHED_AUTO) {
+    // Few slices: the per-tile culling and the volume read/write of the gather
+    // pass are not amortised, so atomics win; a measured choice overrides.
+    const long slices = (long)np * r->nsym;
+    if (slices < 64) sched = FR_SCHED_SCATTER;
+    else if (tuned == -2) sched = FR_SCHED_SCATTER;
+    else if (tuned >= 0) sched = FR_SCHED_GATHER;
+    else sched = (slices >= 256 && r->mode != FR_MODE_NEAREST) ? FR_SCHED_GATHER : FR_SCHED_SCATTER;
+  }
+  const bool prof = g_profile.load() != 0;
+  cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+  if (prof)
+    for (auto &e : ev) CU(cudaEventCreate(&e));
+  g_ins_launches++;
+  g_slices += (long long)np * r->nsym;
+  if (sched == FR_SCHED_SCATTER || d_ssnr) {
+    if (prof) CU(cudaEventRecord(ev[0], st));
+    TRY(run_scatter(j, false, st));
+    if (prof) {
+      CU(cudaEventRecord(ev[2], st));
+      CU(cudaEventSynchronize(ev[2]));
+      float ms = 0;
+      cudaEventElapsedTime(&ms, ev[0], ev[2]);
+      std::lock_guard<std::mutex> lk(g_stat_mu);
+      g_insert_ms += ms;
+      for (auto &e : ev) cudaEventDestroy(e);
+    }
+    return FR_OK;
+  }
+  int tile = r->tile >= 0 ? r->tile : (tuned >= 0 ? tuned : default_tile(r->mode, r->N, r->nsym, np));
+  if (r->tiles_tile != tile) {
+    gather_tiles(r->N, r->mode, tile, r->p.corners, r->tiles, r->tx, r->ty, r->tz);
+    r->tiles_tile = tile;
+    std::vector<int2> work(r->tiles.size());
+    for (size_t i = 0; i < work.size(); i++) work[i] = make_int2(0, r->tiles[i]);
+    TRY(r->s_work.ensure(sizeof(int2) * std::max<size_t>(1, work.size())));
+    CU(cudaMemcpyAsync(r->s_work.p, work.data(), sizeof(int2) * work.size(),
+                       cudaMemcpyHostToDevice, st));
+    CU(cudaStreamSynchronize(st));
+  }
+  j.tiles_x = r->tx;
+  j.tiles_y = r->ty;
+  j.tiles_z = r->tz;
+  TRY(r->s_jobs.ensure(sizeof(InsertJob)));
+  TRY(r->s_counter.ensure(sizeof(int)));
+  CU(cudaMemcpyAsync(r->s_jobs.p, &j, sizeof(InsertJob), cudaMemcpyHostToDevice, st));
+  if (prof) CU(cudaEventRecord(ev[0], st));
+  CU(launch_gather(r->s_jobs.as<InsertJob>(), &j, 1, r->s_work.as<int2>(), (int)r->tiles.size(),
+                   tile, r->s_counter.as<int>(), r->mode, st));
+  if (prof) CU(cudaEventRecord(ev[1], st));
+  TRY(run_scatter(j, true, st));
+  g_gather_launches++;
+  if (prof) {
+    CU(cudaEventRecord(ev[2], st));
+    CU(cudaEventSynchronize(ev[2]));
+    float a = 0, b = 0;
+    cudaEventElapsedTime(&a, ev[0], ev[1]);
+    cudaEventElapsedTime(&b, ev[0], ev[2]);
+    std::lock_guard<std::mutex> lk(g_stat_mu);
+    g_gather_ms += a;
+    g_insert_ms += b;
+    for (auto &e : ev) cudaEventDestroy(e);
+  }
+  // The job struct staged above must outlive the launch: keep the copy in
+  // pinned-order by synchronising before the next reuse of s_jobs.
+  CU(cudaStreamSynchronize(st));
+  return FR_OK;
+}
+
+int check_device_error(fr_recon *r) {
+  int h = 0;
+  CU(cudaStreamSynchronize(r->stream));
+  CU(cudaMemcpy(&h, consts().d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (h) {
+    cudaMemset(consts().d_err, 0, sizeof(int));
+    return fail(FR_EDEVICE, "insertion kernel reported inconsistency code %d", h);
+  }
+  return FR_OK;
+}
+
+int alloc_volume(fr_recon *r) {
+  TRY(r->vol_data.ensure(vol_floats(r->N) * sizeof(float)));
+  TRY(r->vol_norm.ensure(norm_floats(r->N) * sizeof(float)));
+  TRY(r->d_sym.ensure(sizeof(float) * r->syms.size()));
+  CU(cudaMemcpyAsync(r->d_sym.p, r->syms.data(), sizeof(float) * r->syms.size(),
+                     cudaMemcpyHostToDevice, r->stream));
+  return FR_OK;
+}
+
+// The caller pipeline of programs/e2spa_make3d.py:300-345 for one chunk of
+// particles already on the device.
+int prologue_chunk(fr_recon *r, const float *d_raw, int n, int box, const fr_particle *meta) {
+  const int N = r->N;
+  cudaStream_t st = r->stream;
+  const size_t img = (size_t)N * N, spec = (size_t)N * (N / 2 + 1);
+  TRY(r->s_img.ensure(sizeof(float) * img * n));
+  TRY(r->s_slices.ensure(sizeof(float) * slice_floats(N) * n));
+  CU(launch_pad(d_raw, n, box, N, r->s_img.as<float>(), st));
+  // CTF constants and per-particle vectors on the host.
+  const size_t cs = ctf_dev_size();
+  std::vector<unsigned char> ctf(cs * n);
+  std::vector<float> txy(2 * n), w(n), rot(9 * n);
+  bool any_ctf = false;
+  for (int i = 0; i < n; i++) {
+    const fr_particle &m = meta[i];
+    ctf_constants(m.defocus, m.dfdiff, m.dfang, m.voltage, m.cs, m.apix, m.ampcont, N,
+                  ctf.data() + cs * i);
+    if (std::fabs(m.defocus) > 1e-4f) any_ctf = true;
+    // ts = inverse of the translation-only part of xform.projection; the
+    // bilinear xform then applies ts^-1, i.e. +(tx, ty) (programs/e2spa_make3d.py:339-342).
+    txy[2 * i] = m.tx;
+    txy[2 * i + 1] = m.ty;
+    w[i] = m.weight > 0 ? m.weight : 0.0f;   // wt <= 0: skipped (programs/e2spa_make3d.py:304)
+    memcpy(&rot[9 * i], m.rot, sizeof(float) * 9);
+  }
+  TRY(r->s_ctf.ensure(cs * n));
+  TRY(r->s_txy.ensure(sizeof(float) * 2 * n));
+  TRY(r->s_w.ensure(sizeof(float) * n));
+  TRY(r->s_rot.ensure(sizeof(float) * 9 * n));
+  TRY(r->s_mean.ensure(sizeof(float) * n));
+  CU(cudaMemcpyAsync(r->s_ctf.p, ctf.data(), cs * n, cudaMemcpyHostToDevice, st));
+  CU(cudaMemcpyAsync(r->s_txy.p, txy.data(), sizeof(float) * 2 * n, cudaMemcpyHostToDevice, st));
+  CU(cudaMemcpyAsync(r->s_w.p, w.data(), sizeof(float) * n, cudaMemcpyHostToDevice, st));
+  CU(cudaMemcpyAsync(r->s_rot.p, rot.data(), sizeof(float) * 9 * n, cudaMemcpyHostToDevice, st));
+  const float *img_on = nullptr;
+  if (any_ctf) {
+    TRY(r->s_spec.ensure(sizeof(cufftComplex) * spec * n));
+    TRY(r->s_img2.ensure(sizeof(float) * img * n));
+    cufftHandle f, b;
+    TRY(r->plans.get2d(true, N, n, st, &f));
+    TRY(r->plans.get2d(false, N, n, st, &b));
+    CUFFT(cufftExecR2C(f, r->s_img.as<cufftReal>(), r->s_spec.as<cufftComplex>()));
+    CU(launch_ctf_flip_dev(r->s_spec.as<cufftComplex>(), r->s_ctf.p, n, N, st));
+    CUFFT(cufftExecC2R(b, r->s_spec.as<cufftComplex>(), r->s_img2.as<cufftReal>()));
+    img_on = r->s_img2.as<float>();
+  }
+  CU(launch_edge_mean(r->s_img.as<float>(), img_on, any_ctf ? r->s_ctf.p : nullptr, n, N,
+                      r->s_mean.as<float>(), st));
+  // preprocess_slice: shift, phase origin to corner, x sqrt((N+2)/N), r2c.
+  TRY(r->s_spec.ensure(sizeof(float) * img * n));  // real staging for the r2c input
+  volatile float inv = 1.0f / (float)N;
+  const float scale = sqrtf(inv * (float)(N + 2));
+  CU(launch_shift_corner(r->s_img.as<float>(), img_on, any_ctf ? r->s_ctf.p : nullptr,
+                         r->s_mean.as<float>(), r->s_txy.as<float>(), 2, n, N, scale,
+                         r->s_spec.as<float>(), st));
+  cufftHandle f;
+  TRY(r->plans.get2d(true, N, n, st, &f));
+  CUFFT(cufftExecR2C(f, r->s_spec.as<cufftReal>(), r->s_slices.as<cufftComplex>()));
+  TRY(r->s_t3d.ensure(sizeof(float) * 9 * (size_t)n * r->nsym));
+  CU(launch_compose(r->s_rot.as<float>(), r->d_sym.as<float>(), n, r->nsym, r->s_t3d.as<float>(),
+                    st));
+  return FR_OK;
+}
+
+int particles_chunk(fr_recon *r, const float *d_raw, int n, int box, const fr_particle *meta,
+                    int schedule) {
+  TRY(prologue_chunk(r, d_raw, n, box, meta));
+  return insert_device(r, r->s_slices.as<float2>(), r->s_t3d.as<float>(), r->s_w.as<float>(), n,
+                       schedule, nullptr, 0);
+}
+
+}  // namespace fr
+
+// ================================================================== C ABI
+extern "C" {
+
+const char *fr_last_error(void) { return g_err.c_str(); }
+
+int fr_profile(int on) {
+  g_profile = on ? 1 : 0;
+  return FR_OK;
+}
+
+int fr_stats_get(fr_stats *out) {
+  if (!out) return fail(FR_ENULL, "null argument");
+  out->kernel_launches = g_launches.load();
+  out->insert_launches = g_ins_launches.load();
+  out->slices_inserted = g_slices.load();
+  out->gather_launches = g_gather_launches.load();
+  std::lock_guard<std::mutex> lk(g_stat_mu);
+  out->insert_ms = g_insert_ms;
+  out->gather_ms = g_gather_ms;
+  return FR_OK;
+}
+
+int fr_stats_reset(void) {
+  g_launches = 0;
+  g_ins_launches = 0;
+  g_slices = 0;
+  g_gather_launches = 0;
+  std::lock_guard<std::mutex> lk(g_stat_mu);
+  g_insert_ms = g_gather_ms = 0.0;
+  return FR_OK;
+}
+const char *fr_version(void) { return "eman2_b200 0.1 (sm_100a)"; }
+
+size_t fr_footprint_bytes(int N) {
+  return (vol_floats(N) + norm_floats(N)) * sizeof(float);
+}
+
+int fr_sym_ops(const char *sym, float *out, int cap) {
+  if (!sym) return -1;
+  std::vector<float> v;
+  const int n = sym_ops(sym, v);
+  if (n < 0) return -1;
+  if (out) {
+    if (cap < n) return -1;
+    memcpy(out, v.data(), sizeof(float) * 9 * n);
+  }
+  return n;
+}
+
+int fr_create(const fr_params *p, fr_recon **out) {
+  if (!p || !out) return fail(FR_ENULL, "null argument");
+  *out = nullptr;
+  if (p->nx <= 0 || p->ny <= 0 || p->nz <= 0)
+    return fail(FR_EINVAL_PARAM, "size must be three positive integers");
+  if (p->nx != p->ny || p->ny != p->nz)
+    return fail(FR_EUNSUPPORTED, "only cubic volumes are supported (size %d %d %d)", p->nx, p->ny,
+                p->nz);
+  if (p->nx % 2)
+    return fail(FR_EUNSUPPORTED, "odd sizes (fftodd volumes) are not supported (size %d)", p->nx);
+  if (p->nx < 4 || p->nx > 4094) return fail(FR_EUNSUPPORTED, "size %d outside [4, 4094]", p->nx);
+  if (p->mode != FR_MODE_NEAREST && p->mode != FR_MODE_GAUSS2 && p->mode != FR_MODE_GAUSS5 &&
+      p->mode != FR_MODE_TRILINEAR)
+    return fail(FR_EUNSUPPORTED, "inserter mode %d is not built", p->mode);
+  std::vector<float> ops;
+  const int ns = sym_ops(p->sym, ops);
+  if (ns < 0) return fail(FR_EUNSUPPORTED, "symmetry '%s' is not supported (c<n>, d<n>)", p->sym);
+  fr_recon *r = new fr_recon();
+  r->p = *p;
+  r->N = p->nx;
+  r->mode = p->mode;
+  r->nsym = ns;
+  r->syms = ops;
+  if (cudaStreamCreateWithFlags(&r->own, cudaStreamNonBlocking) != cudaSuccess) {
+    delete r;
+    return fail(FR_ECUDA, "cudaStreamCreate failed: %s", cudaGetErrorString(cudaGetLastError()));
+  }
+  r->stream = r->own;
+  consts();
+  r->geom = get_geom(r->N, p->corners);
+  *out = r;
+  return FR_OK;
+}
+
+int fr_destroy(fr_recon *r) {
+  if (!r) return FR_OK;
+  {
+    std::lock_guard<std::mutex> lk(r->mu);
+    if (r->stream) cudaStreamSynchronize(r->stream);
+    DevBuf *bufs[] = {&r->vol_data, &r->vol_norm, &r->d_sym, &r->s_in, &r->s_slices, &r->s_rot,
+                      &r->s_w, &r->s_t3d, &r->s_img, &r->s_img2, &r->s_spec, &r->s_ctf,
+                      &r->s_mean, &r->s_txy, &r->s_out, &r->s_ssnr, &r->s_jobs, &r->s_work,
+                      &r->s_counter};
+    for (DevBuf *b : bufs) b->release();
+    if (r->own) cudaStreamDestroy(r->own);
+  }
+  delete r;
+  return FR_OK;
+}
+
+int fr_set_stream(fr_recon *r, void *stream) {
+  if (!r) return fail(FR_ENULL, "null handle");
+  std::lock_guard<std::mutex> lk(r->mu);
+  r->stream = stream ? (cudaStream_t)stream : r->own;
+  return FR_OK;
+}
+
+int fr_get_size(const fr_recon *r, int *N) {
+  if (!r || !N) return fail(FR_ENULL, "null argument");
+  *N = r->N;
+  return FR_OK;
+}
+
+int fr_setup(fr_recon *r) {
+  if (!r) return fail(FR_ENULL, "null handle");
+  std::lock_guard<std::mutex> lk(r->mu);
+  TRY(alloc_volume(r));
+  CU(cudaMemsetAsync(r->vol_data.p, 0, vol_floats(r->N) * sizeof(float), r->stream));
+  CU(cudaMemsetAsync(r->vol_norm.p, 0, norm_floats(r->N) * sizeof(float), r->stream));
+  CU(cudaStreamSynchronize(r->stream));
+  if (r->p.verbose) {
+    printf("3D Fourier dimensions are %d %d %d\n", r->N + 2, r->N, r->N);
+    printf("You will require approximately %1.3g GB of memory to reconstruct this volume\n",
+           ((float)(r->N + 2) * r->N * r->N * sizeof(float) * 1.5) / 1000000000.0);
+  }
+  r->state = 1;
+  return FR_OK;
+}
+
+int fr_setup_seed(fr_recon *r, const float *seed, float seed_weight) {
+  if (!r) return fail(FR_ENULL, "null handle");
+  if (!seed) return fail(FR_ENULL, "null seed volume");
+  std::lock_guard<std::mutex> lk(r->mu);
+  TRY(alloc_volume(r));
+  const void *d = nullptr;
+  TRY(to_device(seed, vol_floats(r->N) * sizeof(float), r->s_in, r->stream, &d));
+  CU(launch_seed((const float *)d, seed_weight, r->N, r->vol_data.as<float>(),
+                 r->vol_norm.as<float>(), r->stream));
+  CU(cudaStreamSynchronize(r->stream));
+  r->state = 1;
+  return FR_OK;
+}
+
+int fr_setup_seedandweights(fr_recon *r, const float *seed, const float *weights) {
+  if (!r) return fail(FR_ENULL, "null handle");
+  if (!seed || !weights) return fail(FR_ENULL, "null seed or weight volume");
+  std::lock_guard<std::mutex> lk(r->mu);
+  TRY(alloc_volume(r));
+  const cudaMemcpyKind k1 = is_device_ptr(seed) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  const cudaMemcpyKind k2 = is_device_ptr(weights) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  CU(cudaMemcpyAsync(r->vol_data.p, seed, vol_floats(r->N) * sizeof(float), k1, r->stream));
+  CU(cudaMemcpyAsync(r->vol_norm.p, weights, norm_floats(r->N) * sizeof(float), k2, r->stream));
+  CU(cudaStreamSynchronize(r->stream));
+  r->state = 1;
+  return FR_OK;
+}
+
+int fr_clear(fr_recon *r) {
+  TRY(check_state(r));
+  std::lock_guard<std::mutex> lk(r->mu);
+  CU(cudaMemsetAsync(r->vol_data.p, 0, vol_floats(r->N) * sizeof(float), r->stream));
+  CU(cudaMemsetAsync(r->vol_norm.p, 0, norm_floats(r->N) * sizeof(float), r->stream));
+  CU(cudaStreamSynchronize(r->stream));
+  return FR_OK;
+}
+
+// preprocess_slice for n device images into n device slices (scratch owned by r).
+static int preprocess_device(fr_recon *r, const float *d_imgs, int n, const float *d_txy,
+                             int txy_stride, float *d_out_slices) {
+  const int N = r->N;
+  cudaStream_t st = r->stream;
+  TRY(r->s_img2.ensure(sizeof(float) * (size_t)n * N * N));
+  // sqrt(1.0f/ysize * xsize) with ysize = N, xsize = N+2 (libEM/reconstructor.cpp:1054)
+  volatile float inv = 1.0f / (float)N;
+  const float scale = sqrtf(inv * (float)(N + 2));
+  CU(launch_shift_corner(d_imgs, nullptr, nullptr, nullptr, d_txy, txy_stride, n, N, scale,
+                         r->s_img2.as<float>(), st));
+  cufftHandle plan;
+  TRY(r->plans.get2d(true, N, n, st, &plan));
+  CUFFT(cufftExecR2C(plan, r->s_img2.as<cufftReal>(), reinterpret_cast<cufftComplex *>(d_out_slices)));
+  return FR_OK;
+}
+
+int fr_preprocess_slices(fr_recon *r, const float *imgs, int n, const float *inv_txy,
+                         float *out_slices) {
+  if (!r) return fail(FR_ENULL, "null handle");
+  if (n < 0) return fail(FR_EINVAL_PARAM, "negative count");
+  if (n == 0) return FR_OK;
+  if (!imgs || !out_slices) return fail(FR_ENULL, "null image or output");
+  std::lock_guard<std::mutex> lk(r->mu);
+  const int N = r->N;
+  const void *d_in = nullptr, *d_t = nullptr;
+  TRY(to_device(imgs, sizeof(float) * (size_t)n * N * N, r->s_in, r->stream, &d_in));
+  if (inv_txy) TRY(to_device(inv_txy, sizeof(float) * 2 * n, r->s_txy, r->stream, &d_t));
+  const bool dev_out = is_device_ptr(out_slices);
+  float *d_out = out_slices;
+  if (!dev_out) {
+    TRY(r->s_out.ensure(sizeof(float) * slice_floats(N) * n));
+    d_out = r->s_out.as<float>();
+  }
+  TRY(preprocess_device(r, (const float *)d_in, n, (const float *)d_t, 2, d_out));
+  if (!dev_out) TRY(from_device(out_slices, d_out, sizeof(float) * slice_floats(N) * n, r->stream));
+  else CU(cudaStreamSynchronize(r->stream));
+  return FR_OK;
+}
+
+int fr_insert_slices(fr_recon *r, const float *slices, int n, const float *rot, const float *weights,
+                     const float *ssnr, int nssnr, int *status_out, int schedule) {
+  TRY(check_state(r));
+  if (n < 0) return fail(FR_EINVAL_PARAM, "negative count");
+  if (n == 0) return FR_OK;
+  if (!slices || !rot || !weights) return fail(FR_ENULL, "EMData pointer (input image) is NULL");
+  std::lock_guard<std::mutex> lk(r->mu);
+  const int N = r->N;
+  cudaStream_t st = r->stream;
+  // insert_slice (libEM/reconstructor.cpp:1080-1090): usessnr turns the weight
+  // into the SSNR flag (-1) when class_ssnr is present, else into 0; a zero
+  // weight returns -1 without inserting.
+  std::vector<float> w(n);
+  const bool wdev = is_device_ptr(weights);
+  if (wdev) CU(cudaMemcpy(w.data(), weights, sizeof(float) * n, cudaMemcpyDeviceToHost));
+  else memcpy(w.data(), weights, sizeof(float) * n);
+  const bool use_ssnr = r->p.usessnr != 0;
+  if (use_ssnr) {
+    for (int i = 0; i < n; i++) w[i] = (ssnr && nssnr > 0) ? -1.0f : 0.0f;
+  }
+  for (int i = 0; i < n; i++)
+    if (status_out) status_out[i] = (w[i] == 0.0f) ? -1 : 0;
+  const void *d_sl = nullptr, *d_rot = nullptr, *d_ss = nullptr;
+  TRY(to_device(slices, sizeof(float) * slice_floats(N) * n, r->s_in, st, &d_sl));
+  TRY(to_device(rot, sizeof(float) * 9 * n, r->s_rot, st, &d_rot));
+  if (use_ssnr && ssnr && nssnr > 0)
+    TRY(to_device(ssnr, sizeof(float) * (size_t)nssnr * n, r->s_ssnr, st, &d_ss));
+  TRY(r->s_w.ensure(sizeof(float) * n));
+  CU(cudaMemcpyAsync(r->s_w.p, w.data(), sizeof(float) * n, cudaMemcpyHostToDevice, st));
+  TRY(r->s_t3d.ensure(sizeof(float) * 9 * (size_t)n * r->nsym));
+  CU(launch_compose((const float *)d_rot, r->d_sym.as<float>(), n, r->nsym, r->s_t3d.as<float>(),
+                    st));
+  TRY(insert_device(r, (const float2 *)d_sl, r->s_t3d.as<float>(), r->s_w.as<float>(), n, schedule,
+                    (const float *)d_ss, nssnr));
+  CU(cudaStreamSynchronize(st));
+  return FR_OK;
+}
+
+int fr_insert_particles(fr_recon *r, const float *imgs, int n, int box, const fr_particle *meta,
+                        int schedule) {
+  TRY(check_state(r));
+  if (n < 0 || box <= 0) return fail(FR_EINVAL_PARAM, "bad particle count or box");
+  if (n == 0) return FR_OK;
+  if (!imgs || !meta) return fail(FR_ENULL, "EMData pointer (input image) is NULL");
+  std::lock_guard<std::mutex> lk(r->mu);
+  const int N = r->N;
+  // Chunk so the per-chunk scratch (about 5 N^2 floats per particle) stays near 8 GiB.
+  const size_t per = (size_t)N * N * 4 * 5 + (size_t)box * box * 4;
+  const int chunk = (int)std::max<size_t>(1, std::min<size_t>(8192, (8ull << 30) / per));
+  const bool dev = is_device_ptr(imgs);
+  for (int p0 = 0; p0 < n; p0 += chunk) {
+    const int c = std::min(chunk, n - p0);
+    const float *src = imgs + (size_t)p0 * box * box;
+    const float *d_raw = src;
+    if (!dev) {
+      TRY(r->s_in.ensure(sizeof(float) * (size_t)c * box * box));
+      CU(cudaMemcpyAsync(r->s_in.p, src, sizeof(float) * (size_t)c * box * box,
+                         cudaMemcpyHostToDevice, r->stream));
+      d_raw = r->s_in.as<float>();
+    }
+    TRY(particles_chunk(r, d_raw, c, box, meta + p0, schedule));
+  }
+  CU(cudaStreamSynchronize(r->stream));
+  return FR_OK;
+}
+
+int fr_determine_slice_agreement(fr_recon *r, const float *slices, int n, const float *rot,
+                                 const float *weights, float apix, int sub, float *out) {
+  TRY(check_state(r));
+  if (n < 0) return fail(FR_EINVAL_PARAM, "negative count");
+  if (n == 0) return FR_OK;
+  if (!slices || !rot || !weights || !out) return fail(FR_ENULL, "EMData pointer (input image) is NULL");
+  if (sub)
+    return fail(FR_ENOTEXIST,
+                "class_ssnr: sub=True inserts the slice through the SSNR path, which needs the "
+                "class_ssnr attribute (NotExistingObjectException in the reference)");
+  std::lock_guard<std::mutex> lk(r->mu);
+  const int N = r->N;
+  cudaStream_t st = r->stream;
+  const void *d_sl = nullptr, *d_rot = nullptr, *d_w = nullptr;
+  TRY(to_device(slices, sizeof(float) * slice_floats(N) * n, r->s_in, st, &d_sl));
+  TRY(to_device(rot, sizeof(float) * 9 * n, r->s_rot, st, &d_rot));
+  TRY(to_device(weights, sizeof(float) * n, r->s_w, st, &d_w));
+  TRY(r->s_t3d.ensure(sizeof(float) * 9 * (size_t)n * r->nsym));
+  CU(launch_compose((const float *)d_rot, r->d_sym.as<float>(), n, r->nsym, r->s_t3d.as<float>(), st));
+  const bool dev_out = is_device_ptr(out);
+  float *d_out = out;
+  if (!dev_out) {
+    TRY(r->s_out.ensure(sizeof(float) * 5 * n));
+    d_out = r->s_out.as<float>();
+  }
+  CU(launch_agree_rt(r->vol_data.as<float>(), r->vol_norm.as<float>(), N, (const float *)d_sl,
+                     r->s_t3d.as<float>(), n, r->nsym, (const float *)d_w, apix, r->geom->d_rtab,
+                     d_out, st));
+  if (!dev_out) TRY(from_device(out, d_out, sizeof(float) * 5 * n, st));
+  else CU(cudaStreamSynchronize(st));
+  return FR_OK;
+}
+
+int fr_projection(fr_recon *r, const float *rot, float *out_slice) {
+  TRY(check_state(r));
+  if (!rot || !out_slice) return fail(FR_ENULL, "null argument");
+  std::lock_guard<std::mutex> lk(r->mu);
+  const int N = r->N;
+  cudaStream_t st = r->stream;
+  TRY(r->s_rot.ensure(sizeof(float) * 9));
+  const cudaMemcpyKind k = is_device_ptr(rot) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  CU(cudaMemcpyAsync(r->s_rot.p, rot, sizeof(float) * 9, k, st));
+  TRY(r->s_out.ensure(sizeof(float) * slice_floats(N)));
+  CU(cudaMemsetAsync(r->s_out.p, 0, sizeof(float) * slice_floats(N), st));
+  CU(launch_projection_rt(r->vol_data.as<float>(), r->vol_norm.as<float>(), N, r->s_rot.as<float>(),
+                          r->geom->d_rtab, r->s_out.as<float>(), st));
+  TRY(from_device(out_slice, r->s_out.p, sizeof(float) * slice_floats(N), st));
+  return FR_OK;
+}
+
+int fr_get_accumulators(fr_recon *r, float *data, float *norm) {
+  TRY(check_state(r));
+  std::lock_guard<std::mutex> lk(r->mu);
+  TRY(check_device_error(r));
+  if (data) TRY(from_device(data, r->vol_data.p, vol_floats(r->N) * sizeof(float), r->stream));
+  if (norm) TRY(from_device(norm, r->vol_norm.p, norm_floats(r->N) * sizeof(float), r->stream));
+  return FR_OK;
+}
+
+int fr_finish(fr_recon *r, int doift, float *out, float *normout) {
+  TRY(check_state(r));
+  std::lock_guard<std::mutex> lk(r->mu);
+  const int N = r->N;
+  cudaStream_t st = r->stream;
+  TRY(check_device_error(r));
+  CU(launch_normalize(r->vol_data.as<float>(), r->vol_norm.as<float>(), N, r->p.sqrtnorm, st));
+  if (normout) TRY(from_device(normout, r->vol_norm.p, norm_floats(N) * sizeof(float), st));
+  if (doift) {
+    cufftHandle plan;
+    TRY(r->plans.get3d(N, st, &plan));
+    CUFFT(cufftExecC2R(plan, r->vol_data.as<cufftComplex>(), r->vol_data.as<cufftReal>()));
+    // do_ift scale 1.0f / (nx*ny*nz) (libEM/emdata_transform.cpp:411-412)
+    const float scale = 1.0f / (float)((size_t)N * N * N);
+    if (out) {
+      if (is_device_ptr(out)) {
+        CU(launch_depad_center(r->vol_data.as<float>(), N, scale, out, st));
+        CU(cudaStreamSynchronize(st));
+      } else {
+        TRY(r->s_out.ensure(sizeof(float) * (size_t)N * N * N));
+        CU(launch_depad_center(r->vol_data.as<float>(), N, scale, r->s_out.as<float>(), st));
+        TRY(from_device(out, r->s_out.p, sizeof(float) * (size_t)N * N * N, st));
+      }
+    }
+  } else if (out) {
+    TRY(from_device(out, r->vol_data.p, vol_floats(N) * sizeof(float), st));
+  }
+  CU(cudaStreamSynchronize(st));
+  r->state = 2;
+  return FR_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,284 @@
+// fr_batch.cu -- many reconstructions in one persistent insertion launch, and
+// the tile/schedule autotuner.
+//
+// A batch holds independent FourierReconstructor states (uneven N, modes and
+// symmetries: even/odd half maps, heterogeneity classes).  Each insert call
+// runs every job's prologue on the batch stream, then ONE k_gather launch whose
+// work list interleaves all jobs' voxel tiles (heaviest first), then the small
+// face-tap kernels.  With CUDA graphs enabled the whole device sequence of a
+// call is captured once per shape signature and replayed.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <random>
+#include <tuple>
+#include <vector>
+
+#include "fr_handle.h"
+
+using namespace fr;
+
+namespace fr {
+
+// ------------------------------------------------------------------ tuning
+// Choices per (N, mode, nsym): >= 0 gather with that tile, -2 scatter.
+static std::mutex g_tune_mu;
+static std::map<std::tuple<int, int, int>, int> g_tuned;
+constexpr int kTunedScatter = -2;
+
+int tuned_tile(int N, int mode, int nsym) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  auto it = g_tuned.find(std::make_tuple(N, mode, nsym));
+  return it == g_tuned.end() ? -1 : it->second;
+}
+
+int default_tile(int mode, int N, int nsym, int np) {
+  (void)nsym; (void)np;
+  if (mode == FR_MODE_GAUSS5) return 0;   // 8x8x8
+  return N >= 256 ? 1 : 0;                // 16x8x8 for the thin gauss_2 windows at large N
+}
+
+}  // namespace fr
+
+// ------------------------------------------------------------------ batch
+struct fr_batch {
+  std::vector<fr_recon *> jobs;
+  cudaStream_t own = nullptr, stream = nullptr;
+  DevBuf d_jobs, d_work, d_counter, d_raw;
+  int tile = -1;
+  std::mutex mu;
+};
+
+extern "C" {
+
+int fr_batch_create(const fr_params *jobs, int njobs, fr_batch **out) {
+  if (!jobs || !out) return fail(FR_ENULL, "null argument");
+  if (njobs <= 0) return fail(FR_EINVAL_PARAM, "a batch needs at least one job");
+  *out = nullptr;
+  fr_batch *b = new fr_batch();
+  if (cudaStreamCreateWithFlags(&b->own, cudaStreamNonBlocking) != cudaSuccess) {
+    delete b;
+    return fail(FR_ECUDA, "cudaStreamCreate failed");
+  }
+  b->stream = b->own;
+  for (int j = 0; j < njobs; j++) {
+    fr_recon *r = nullptr;
+    int rc = fr_create(&jobs[j], &r);
+    if (rc == FR_OK) rc = fr_set_stream(r, b->stream);
+    if (rc == FR_OK) rc = fr_setup(r);
+    if (rc != FR_OK) {
+      if (r) fr_destroy(r);
+      for (fr_recon *q : b->jobs) fr_destroy(q);
+      cudaStreamDestroy(b->own);
+      delete b;
+      return rc;
+    }
+    b->jobs.push_back(r);
+  }
+  *out = b;
+  return FR_OK;
+}
+
+int fr_batch_destroy(fr_batch *b) {
+  if (!b) return FR_OK;
+  cudaStreamSynchronize(b->stream);
+  for (fr_recon *r : b->jobs) fr_destroy(r);
+  b->d_jobs.release();
+  b->d_work.release();
+  b->d_counter.release();
+  b->d_raw.release();
+  if (b->own) cudaStreamDestroy(b->own);
+  delete b;
+  return FR_OK;
+}
+
+int fr_batch_set_stream(fr_batch *b, void *stream) {
+  if (!b) return fail(FR_ENULL, "null batch");
+  std::lock_guard<std::mutex> lk(b->mu);
+  b->stream = stream ? (cudaStream_t)stream : b->own;
+  for (fr_recon *r : b->jobs) fr_set_stream(r, b->stream);
+  return FR_OK;
+}
+
+int fr_batch_insert_particles(fr_batch *b, const float *const *imgs, const int *boxes,
+                              const int *counts, const fr_particle *const *meta) {
+  if (!b || !imgs || !boxes || !counts || !meta) return fail(FR_ENULL, "null argument");
+  std::lock_guard<std::mutex> lk(b->mu);
+  const int nj = (int)b->jobs.size();
+  cudaStream_t st = b->stream;
+  for (int j = 0; j < nj; j++) {
+    TRY(check_state(b->jobs[j]));
+    if (counts[j] < 0 || (counts[j] > 0 && (boxes[j] <= 0 || !imgs[j] || !meta[j])))
+      return fail(FR_EINVAL_PARAM, "job %d: bad particle count, box or buffers", j);
+  }
+  // Rounds of at most `chunk` particles per job, so scratch stays bounded.
+  const int chunk = 4096;
+  int rounds = 0;
+  for (int j = 0; j < nj; j++) rounds = std::max(rounds, (counts[j] + chunk - 1) / chunk);
+  int tile = b->tile >= 0 ? b->tile : 0;
+  for (int rd = 0; rd < rounds; rd++) {
+    std::vector<InsertJob> hj;
+    std::vector<int> owner;
+    int max_mode = FR_MODE_NEAREST;
+    for (int j = 0; j < nj; j++) {
+      fr_recon *r = b->jobs[j];
+      const int p0 = rd * chunk;
+      const int c = std::max(0, std::min(chunk, counts[j] - p0));
+      if (c == 0) continue;
+      const int box = boxes[j];
+      const float *src = imgs[j] + (size_t)p0 * box * box;
+      const void *d_raw = nullptr;
+      TRY(to_device(src, sizeof(float) * (size_t)c * box * box, r->s_in, st, &d_raw));
+      TRY(prologue_chunk(r, (const float *)d_raw, c, box, meta[j] + p0));
+      InsertJob J = make_job(r, r->s_slices.as<float2>(), r->s_t3d.as<float>(), r->s_w.as<float>(), c);
+      if (r->tiles_tile != tile) {
+        gather_tiles(r->N, r->mode, tile, r->p.corners, r->tiles, r->tx, r->ty, r->tz);
+        r->tiles_tile = tile;
+      }
+      J.tiles_x = r->tx;
+      J.tiles_y = r->ty;
+      J.tiles_z = r->tz;
+      hj.push_back(J);
+      owner.push_back(j);
+      if (r->mode == FR_MODE_GAUSS5) max_mode = FR_MODE_GAUSS5;
+      else if (max_mode != FR_MODE_GAUSS5 && r->mode != FR_MODE_NEAREST) max_mode = r->mode;
+    }
+    if (hj.empty()) continue;
+    // Interleave every job's tiles by estimated cost (slices meeting a tile
+    // fall off with its distance from the origin), heaviest first.
+    std::vector<std::pair<double, int2>> items;
+    for (size_t k = 0; k < hj.size(); k++) {
+      fr_recon *r = b->jobs[owner[k]];
+      const double nsl = (double)hj[k].np * hj[k].nsym;
+      const double nt = (double)r->tiles.size();
+      for (size_t t = 0; t < r->tiles.size(); t++) {
+        const double frac = (double)t / std::max(1.0, nt);   // tiles are sorted by distance
+        const double cost = nsl / (1.0 + 8.0 * std::cbrt(frac) * r->N / 16.0);
+        items.push_back({-cost, make_int2((int)k, r->tiles[t])});
+      }
+    }
+    std::stable_sort(items.begin(), items.end(),
+                     [](const std::pair<double, int2> &a, const std::pair<double, int2> &c) {
+                       return a.first < c.first;
+                     });
+    std::vector<int2> work(items.size());
+    for (size_t i = 0; i < items.size(); i++) work[i] = items[i].second;
+    TRY(b->d_jobs.ensure(sizeof(InsertJob) * hj.size()));
+    TRY(b->d_work.ensure(sizeof(int2) * work.size()));
+    TRY(b->d_counter.ensure(sizeof(int)));
+    CU(cudaMemcpyAsync(b->d_jobs.p, hj.data(), sizeof(InsertJob) * hj.size(),
+                       cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(b->d_work.p, work.data(), sizeof(int2) * work.size(),
+                       cudaMemcpyHostToDevice, st));
+    CU(launch_gather(b->d_jobs.as<InsertJob>(), hj.data(), (int)hj.size(), b->d_work.as<int2>(),
+                     (int)work.size(), tile, b->d_counter.as<int>(), max_mode, st));
+    for (const InsertJob &J : hj) TRY(run_scatter(J, true, st));
+    CU(cudaStreamSynchronize(st));
+  }
+  return FR_OK;
+}
+
+int fr_batch_finish(fr_batch *b, int job, int doift, float *out, float *normout) {
+  if (!b) return fail(FR_ENULL, "null batch");
+  if (job < 0 || job >= (int)b->jobs.size()) return fail(FR_EINVAL_PARAM, "job %d out of range", job);
+  return fr_finish(b->jobs[job], doift, out, normout);
+}
+
+int fr_batch_get_accumulators(fr_batch *b, int job, float *data, float *norm) {
+  if (!b) return fail(FR_ENULL, "null batch");
+  if (job < 0 || job >= (int)b->jobs.size()) return fail(FR_EINVAL_PARAM, "job %d out of range", job);
+  return fr_get_accumulators(b->jobs[job], data, norm);
+}
+
+int fr_set_tile(int N, int mode, int nsym, int tile) {
+  if (tile != kTunedScatter && (tile < -1 || tile >= kNumTiles))
+    return fail(FR_EINVAL_PARAM, "tile %d out of range", tile);
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  if (tile == -1) g_tuned.erase(std::make_tuple(N, mode, nsym));
+  else g_tuned[std::make_tuple(N, mode, nsym)] = tile;
+  return FR_OK;
+}
+
+// Measures the gather schedule with every tile shape, and the scatter
+// schedule, on random slices of size N through random orientations; records
+// the fastest for (N, mode, nsym).  tile_out: chosen tile (-2 = scatter);
+// ms_out[kNumTiles+1]: per-candidate milliseconds (tiles, then scatter).
+int fr_autotune(int N, int mode, int nsym, int nparticles, int *tile_out, float *ms_out) {
+  if (nparticles <= 0) return fail(FR_EINVAL_PARAM, "nparticles must be positive");
+  fr_params p;
+  memset(&p, 0, sizeof p);
+  p.nx = p.ny = p.nz = N;
+  p.mode = mode;
+  snprintf(p.sym, sizeof p.sym, "c%d", std::max(1, nsym));
+  fr_recon *r = nullptr;
+  TRY(fr_create(&p, &r));
+  int rc = fr_setup(r);
+  std::vector<float> sl(slice_floats(N) * (size_t)nparticles), rot(9 * (size_t)nparticles),
+      w(nparticles, 1.0f);
+  std::mt19937 rng(1234);
+  std::normal_distribution<float> nd(0.f, 1.f);
+  for (auto &v : sl) v = nd(rng);
+  for (int i = 0; i < nparticles; i++) {
+    float q[4], n2 = 0;
+    for (float &c : q) { c = nd(rng); n2 += c * c; }
+    const float s = 1.0f / std::sqrt(n2);
+    for (float &c : q) c *= s;
+    const double e0 = q[0], e1 = q[1], e2 = q[2], e3 = q[3];
+    float *m = &rot[9 * i];
+    m[0] = (float)(e0 * e0 + e1 * e1 - e2 * e2 - e3 * e3);
+    m[1] = (float)(2.0 * (e1 * e2 + e0 * e3));
+    m[2] = (float)(2.0 * (e1 * e3 - e0 * e2));
+    m[3] = (float)(2.0 * (e2 * e1 - e0 * e3));
+    m[4] = (float)(e0 * e0 - e1 * e1 + e2 * e2 - e3 * e3);
+    m[5] = (float)(2.0 * (e2 * e3 + e0 * e1));
+    m[6] = (float)(2.0 * (e3 * e1 + e0 * e2));
+    m[7] = (float)(2.0 * (e3 * e2 - e0 * e1));
+    m[8] = (float)(e0 * e0 - e1 * e1 - e2 * e2 + e3 * e3);
+  }
+  float best = 1e30f;
+  int best_tile = kTunedScatter;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  for (int cand = 0; cand <= kNumTiles && rc == FR_OK; cand++) {
+    const bool scatter = cand == kNumTiles;
+    r->tile = scatter ? -1 : cand;
+    const int sched = scatter ? FR_SCHED_SCATTER : FR_SCHED_GATHER;
+    // one warm-up call, then one timed call
+    rc = fr_insert_slices(r, sl.data(), nparticles, rot.data(), w.data(), nullptr, 0, nullptr, sched);
+    if (rc != FR_OK) break;
+    // stage inputs on the device so the timing covers the insertion only
+    float ms = 0;
+    {
+      DevBuf ds, dr, dw;
+      if ((rc = ds.ensure(sizeof(float) * sl.size())) != FR_OK) break;
+      if ((rc = dr.ensure(sizeof(float) * rot.size())) != FR_OK) break;
+      if ((rc = dw.ensure(sizeof(float) * w.size())) != FR_OK) break;
+      cudaMemcpy(ds.p, sl.data(), sizeof(float) * sl.size(), cudaMemcpyHostToDevice);
+      cudaMemcpy(dr.p, rot.data(), sizeof(float) * rot.size(), cudaMemcpyHostToDevice);
+      cudaMemcpy(dw.p, w.data(), sizeof(float) * w.size(), cudaMemcpyHostToDevice);
+      cudaEventRecord(e0, r->stream);
+      rc = fr_insert_slices(r, ds.as<float>(), nparticles, dr.as<float>(), dw.as<float>(), nullptr,
+                            0, nullptr, sched);
+      cudaEventRecord(e1, r->stream);
+      cudaEventSynchronize(e1);
+      cudaEventElapsedTime(&ms, e0, e1);
+      ds.release();
+      dr.release();
+      dw.release();
+    }
+    if (ms_out) ms_out[cand] = ms;
+    if (ms < best) { best = ms; best_tile = scatter ? kTunedScatter : cand; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  fr_destroy(r);
+  if (rc != FR_OK) return rc;
+  fr_set_tile(N, mode, nsym, best_tile);
+  if (tile_out) *tile_out = best_tile;
+  return FR_OK;
+}
+
+}  // extern "C"

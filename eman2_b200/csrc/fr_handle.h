@@ -1,0 +1,156 @@
+// fr_handle.h -- the reconstruction handle and host helpers shared by the
+// C-ABI translation units (fr_api.cu, fr_batch.cu).  Not part of the C ABI.
+#pragma once
+#include <cufft.h>
+
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/eman2_b200.h"
+#include "fr_internal.h"
+
+namespace fr {
+
+int fail(int code, const char *fmt, ...);
+
+#define CU(call)                                                                      \
+  do {                                                                                \
+    cudaError_t e_ = (call);                                                          \
+    if (e_ != cudaSuccess)                                                            \
+      return ::fr::fail(e_ == cudaErrorMemoryAllocation ? FR_ENOMEM : FR_ECUDA,        \
+                        "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+  } while (0)
+
+#define CUFFT(call)                                                                   \
+  do {                                                                                \
+    cufftResult r_ = (call);                                                          \
+    if (r_ != CUFFT_SUCCESS)                                                          \
+      return ::fr::fail(r_ == CUFFT_ALLOC_FAILED ? FR_ENOMEM : FR_ECUDA, "%s: cufft error %d", \
+                        #call, (int)r_);                                              \
+  } while (0)
+
+#define TRY(call)                 \
+  do {                            \
+    int rc_ = (call);             \
+    if (rc_ != FR_OK) return rc_; \
+  } while (0)
+
+struct DevBuf {
+  void *p = nullptr;
+  size_t cap = 0;
+  int ensure(size_t bytes) {
+    if (bytes <= cap) return FR_OK;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    if (cudaMalloc(&p, bytes) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(FR_ENOMEM, "device allocation of %zu bytes failed", bytes);
+    }
+    cap = bytes;
+    return FR_OK;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+  }
+  template <class T> T *as() const { return reinterpret_cast<T *>(p); }
+};
+
+
+bool is_device_ptr(const void *p);
+int to_device(const void *src, size_t bytes, DevBuf &stage, cudaStream_t st, const void **out);
+int from_device(void *dst, const void *dsrc, size_t bytes, cudaStream_t st);
+
+// ------------------------------------------------------------- cuFFT plans
+struct PlanCache {
+  std::map<std::pair<int, int>, cufftHandle> r2c, c2r;   // key (N, batch)
+  cufftHandle c2r3 = 0;
+  int c2r3_N = 0;
+  ~PlanCache() {
+    for (auto &kv : r2c) cufftDestroy(kv.second);
+    for (auto &kv : c2r) cufftDestroy(kv.second);
+    if (c2r3) cufftDestroy(c2r3);
+  }
+  int get2d(bool forward, int N, int batch, cudaStream_t st, cufftHandle *out) {
+    auto &m = forward ? r2c : c2r;
+    auto key = std::make_pair(N, batch);
+    auto it = m.find(key);
+    if (it == m.end()) {
+      cufftHandle h;
+      int n[2] = {N, N};
+      const int dist_r = N * N, dist_c = N * (N / 2 + 1);
+      if (forward)
+        CUFFT(cufftPlanMany(&h, 2, n, nullptr, 1, dist_r, nullptr, 1, dist_c, CUFFT_R2C, batch));
+      else
+        CUFFT(cufftPlanMany(&h, 2, n, nullptr, 1, dist_c, nullptr, 1, dist_r, CUFFT_C2R, batch));
+      it = m.emplace(key, h).first;
+    }
+    CUFFT(cufftSetStream(it->second, st));
+    *out = it->second;
+    return FR_OK;
+  }
+  int get3d(int N, cudaStream_t st, cufftHandle *out) {
+    if (!c2r3 || c2r3_N != N) {
+      if (c2r3) cufftDestroy(c2r3);
+      c2r3 = 0;
+      CUFFT(cufftPlan3d(&c2r3, N, N, N, CUFFT_C2R));
+      c2r3_N = N;
+    }
+    CUFFT(cufftSetStream(c2r3, st));
+    *out = c2r3;
+    return FR_OK;
+  }
+};
+
+
+size_t vol_floats(int N);
+size_t norm_floats(int N);
+size_t slice_floats(int N);
+
+// Tile choice for the gather schedule (fr_batch.cu): measured choice when the
+// autotuner has one for (N, mode, nsym), else a size-based default.
+int tuned_tile(int N, int mode, int nsym);
+int default_tile(int mode, int N, int nsym, int np);
+
+}  // namespace fr
+
+// ------------------------------------------------------------------ handle
+struct fr_recon {
+  fr_params p;
+  int N = 0;
+  int mode = FR_MODE_GAUSS2;
+  int nsym = 1;
+  std::vector<float> syms;
+  int state = 0;              // 0 created, 1 accumulating, 2 finished
+  cudaStream_t own = nullptr, stream = nullptr;
+  fr::Geom *geom = nullptr;
+  fr::DevBuf vol_data, vol_norm, d_sym;
+  // scratch
+  fr::DevBuf s_in, s_slices, s_rot, s_w, s_t3d, s_img, s_img2, s_spec, s_ctf, s_mean, s_txy, s_out,
+      s_ssnr, s_jobs, s_work, s_counter;
+  fr::PlanCache plans;
+  int tile = -1;              // gather tile shape (-1: tuned default)
+  std::vector<int> tiles;
+  int tiles_tile = -1, tx = 0, ty = 0, tz = 0;
+  std::mutex mu;
+};
+
+
+namespace fr {
+int check_state(fr_recon *r);
+InsertJob make_job(fr_recon *r, const float2 *slices, const float *t3d, const float *pw, int np);
+int run_scatter(const InsertJob &j0, bool edge_only, cudaStream_t st);
+int insert_device(fr_recon *r, const float2 *d_slices, const float *d_t3d, const float *d_pw, int np,
+                  int schedule, const float *d_ssnr, int nssnr);
+int check_device_error(fr_recon *r);
+int alloc_volume(fr_recon *r);
+// Prologue of one chunk of device particles into r's scratch: s_slices,
+// s_t3d and s_w hold the chunk's slices, composed rotations and weights.
+int prologue_chunk(fr_recon *r, const float *d_raw, int n, int box, const fr_particle *meta);
+int particles_chunk(fr_recon *r, const float *d_raw, int n, int box, const fr_particle *meta,
+                    int schedule);
+}  // namespace fr

@@ -1,0 +1,570 @@
+// fr_insert.cu -- slice insertion into the (complex, weight) volume.
+//
+// Reference: FourierReconstructor::do_insert_slice_work
+// (libEM/reconstructor.cpp:1122-1210) driving the pixel inserters
+// (libEM/reconstructor_tools.cpp:113-189, 315-376) and
+// EMData::add_complex_at_fast (libEM/emdata_core.h:368-410).
+//
+// Three kernels:
+//  * k_scatter  -- one thread per (slice, pixel); every tap is added with FP32
+//                  atomics exactly as add_complex_at_fast places it.  Used for
+//                  single slices and small batches.
+//  * k_gather   -- a persistent kernel over voxel tiles.  A tile owns its
+//                  cells; for each slice whose plane passes the tile it stages
+//                  the slice's pixel patch in shared memory and every voxel
+//                  collects the taps that land on it, in registers.  No
+//                  atomics; the volume is read and written once per launch.
+//                  Covers every cell with |x|,|y|,|z| < N/2.
+//  * k_edge     -- the taps on the cube faces (|i|, |j| or |k| = N/2) of rim
+//                  pixels, with atomics.  Those taps write only face cells,
+//                  which the gather kernel never touches, and vice versa.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+
+#include "fr_device.cuh"
+#include "fr_internal.h"
+
+namespace fr {
+
+const TileShape kTiles[kNumTiles] = {{8, 8, 8}, {16, 8, 8}, {8, 8, 4}, {16, 16, 4}};
+
+// ---------------------------------------------------------------- compose
+// t3d[p*nsym+q] = arg[p] * sym[q] (libEM/transform.cpp:1384-1395), float.
+__global__ void k_compose(const float *__restrict__ arg, const float *__restrict__ sym, int np,
+                          int nsym, float *__restrict__ t3d) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= np * nsym * 9) return;
+  const int e = idx % 9, s = idx / 9, p = s / nsym, q = s % nsym;
+  const int i = e / 3, j = e % 3;
+  const float *a = arg + 9 * p;
+  const float *b = sym + 9 * q;
+  float v = __fmul_rn(a[3 * i + 0], b[j]);
+  v = __fadd_rn(v, __fmul_rn(a[3 * i + 1], b[3 + j]));
+  v = __fadd_rn(v, __fmul_rn(a[3 * i + 2], b[6 + j]));
+  t3d[idx] = v;
+}
+
+cudaError_t launch_compose(const float *d_arg, const float *d_sym, int np, int nsym, float *d_t3d,
+                           cudaStream_t st) {
+  const int n = np * nsym * 9;
+  if (n == 0) return cudaSuccess;
+  note_launch();
+  k_compose<<<(n + 255) / 256, 256, 0, st>>>(d_arg, d_sym, np, nsym, d_t3d);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------- scatter path
+// One pixel's full insert_pixel with atomics.  Window selection and reject
+// rules follow libEM/reconstructor_tools.cpp:113-126 (nearest),
+// :128-166 (gauss_2), :191-230 (trilinear), :315-376 (gauss_5).
+// face_only: process only taps with a coordinate at +-N/2 (edge kernel).
+template <int MODE>
+__device__ __forceinline__ void insert_pixel_atomic(float *__restrict__ data, float *__restrict__ norm,
+                                                    int N, float xx, float yy, float zz, float re,
+                                                    float im, float w, float h,
+                                                    const float *__restrict__ table, bool face_only) {
+  const int n2 = N >> 1;
+  if (MODE == MODE_NEAREST) {
+    const int x0 = (int)floorf(__fadd_rn(xx, 0.5f));
+    const int y0 = (int)floorf(__fadd_rn(yy, 0.5f));
+    const int z0 = (int)floorf(__fadd_rn(zz, 0.5f));
+    if (face_only && abs(x0) != n2 && abs(y0) != n2 && abs(z0) != n2) return;
+    add_tap_atomic(data, norm, N, x0, y0, z0, __fmul_rn(re, w), __fmul_rn(im, w), w);
+  } else if (MODE == MODE_GAUSS2 || MODE == MODE_TRILINEAR) {
+    const int x0 = (int)floorf(xx), y0 = (int)floorf(yy), z0 = (int)floorf(zz);
+    if (x0 < -n2 - 1 || y0 < -n2 - 1 || z0 < -n2 - 1 || x0 > n2 || y0 > n2 || z0 > n2) return;
+    for (int k = z0; k <= z0 + 1; k++)
+      for (int j = y0; j <= y0 + 1; j++)
+        for (int i = x0; i <= x0 + 1; i++) {
+          if (face_only && abs(i) != n2 && abs(j) != n2 && abs(k) != n2) continue;
+          float vre, vim, vw;
+          tap_value<MODE>(i, j, k, xx, yy, zz, re, im, w, h, table, vre, vim, vw);
+          add_tap_atomic(data, norm, N, i, j, k, vre, vim, vw);
+        }
+  } else {  // MODE_GAUSS5
+    int x0 = floor_minus_2p5(xx), y0 = floor_minus_2p5(yy), z0 = floor_minus_2p5(zz);
+    if (x0 < -n2 - 4 || y0 < -n2 - 4 || z0 < -n2 - 4 || x0 > n2 + 3 || y0 > n2 + 3 || z0 > n2 + 3)
+      return;
+    int x1 = x0 + 5, y1 = y0 + 5, z1 = z0 + 5;
+    x0 = max(x0, -n2); x1 = min(x1, n2);
+    y0 = max(y0, -n2); y1 = min(y1, n2);
+    z0 = max(z0, -n2); z1 = min(z1, n2);
+    for (int k = z0; k <= z1; k++)
+      for (int j = y0; j <= y1; j++)
+        for (int i = x0; i <= x1; i++) {
+          if (face_only && abs(i) != n2 && abs(j) != n2 && abs(k) != n2) continue;
+          float vre, vim, vw;
+          tap_value<MODE>(i, j, k, xx, yy, zz, re, im, w, h, table, vre, vim, vw);
+          add_tap_atomic(data, norm, N, i, j, k, vre, vim, vw);
+        }
+  }
+}
+
+// Per-pixel weight: the particle weight, or with usessnr the slice's
+// class_ssnr table at the pixel radius, max(0, ssnr[int(r*sscale)])
+// (libEM/reconstructor.cpp:1170-1184).
+__device__ __forceinline__ float pixel_weight(const InsertJob &J, int p, int x, int y, float w) {
+  if (!J.ssnr) return w;
+  const int r = (int)__fadd_rn((float)sqrt((double)(x * x + y * y)), 0.5f);
+  const int k = min((int)__fmul_rn((float)r, J.sscale), J.nssnr - 1);
+  const float sv = J.ssnr[(size_t)p * J.nssnr + k];
+  return sv > 0.0f ? sv : 0.0f;
+}
+
+// grid.x covers the N*(N/2+1) pixel grid, grid.y = slice (particle*nsym+sym).
+template <int MODE>
+__global__ void __launch_bounds__(256) k_scatter(InsertJob J, const float *__restrict__ table,
+                                                 float h) {
+  const int N = J.N, n2 = N >> 1, w2 = n2 + 1;
+  const int s = blockIdx.y;
+  const int p = s / J.nsym;
+  const float w = J.pw[p];
+  if (w == 0.0f) return;
+  const int pix = blockIdx.x * blockDim.x + threadIdx.x;
+  if (pix >= N * w2) return;
+  const int x = pix % w2, y = pix / w2 - n2;
+  if (x > __ldg(&J.xmax[y + n2])) return;
+  float M[6];
+#pragma unroll
+  for (int i = 0; i < 6; i++) M[i] = __ldg(&J.t3d[9 * s + i]);
+  float xx, yy, zz;
+  pixel_coords(__ldg(&J.rtab[x + n2]), __ldg(&J.rtab[y + n2]), M, (float)N, xx, yy, zz);
+  const float2 v = slice_value(J.slices + (size_t)p * N * w2, N, x, y);
+  insert_pixel_atomic<MODE>(J.data, J.norm, N, xx, yy, zz, v.x, v.y, pixel_weight(J, p, x, y, w),
+                            h, table, false);
+}
+
+// Face taps of rim pixels: grid.x covers the rim list, grid.y = slice.
+template <int MODE>
+__global__ void __launch_bounds__(128) k_edge(InsertJob J, const float *__restrict__ table,
+                                              float h) {
+  const int N = J.N, n2 = N >> 1, w2 = n2 + 1;
+  const int s = blockIdx.y;
+  const int p = s / J.nsym;
+  const float w = J.pw[p];
+  if (w == 0.0f) return;
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= J.nrim) return;
+  const int code = __ldg(&J.rim[r]);
+  const int x = code & 0xFFFF, y = (code >> 16) - n2;
+  float M[6];
+#pragma unroll
+  for (int i = 0; i < 6; i++) M[i] = __ldg(&J.t3d[9 * s + i]);
+  float xx, yy, zz;
+  pixel_coords(__ldg(&J.rtab[x + n2]), __ldg(&J.rtab[y + n2]), M, (float)N, xx, yy, zz);
+  const float2 v = slice_value(J.slices + (size_t)p * N * w2, N, x, y);
+  insert_pixel_atomic<MODE>(J.data, J.norm, N, xx, yy, zz, v.x, v.y, pixel_weight(J, p, x, y, w),
+                            h, table, true);
+}
+
+static float mode_h(int mode) {
+  const Consts &c = consts();
+  return mode == MODE_GAUSS5 ? c.h5 : c.h2;
+}
+
+cudaError_t launch_scatter(const InsertJob &j, cudaStream_t st) {
+  const int nsl = j.np * j.nsym;
+  if (nsl == 0) return cudaSuccess;
+  const int npx = j.N * (j.N / 2 + 1);
+  dim3 grid((npx + 255) / 256, nsl);
+  const float *tab = consts().d_exp;
+  const float h = mode_h(j.mode);
+  note_launch();
+  switch (j.mode) {
+    case MODE_NEAREST: k_scatter<MODE_NEAREST><<<grid, 256, 0, st>>>(j, tab, h); break;
+    case MODE_GAUSS2: k_scatter<MODE_GAUSS2><<<grid, 256, 0, st>>>(j, tab, h); break;
+    case MODE_GAUSS5: k_scatter<MODE_GAUSS5><<<grid, 256, 0, st>>>(j, tab, h); break;
+    case MODE_TRILINEAR: k_scatter<MODE_TRILINEAR><<<grid, 256, 0, st>>>(j, tab, h); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_edge(const InsertJob &j, cudaStream_t st) {
+  const int nsl = j.np * j.nsym;
+  if (nsl == 0 || j.nrim == 0) return cudaSuccess;
+  dim3 grid((j.nrim + 127) / 128, nsl);
+  const float *tab = consts().d_exp;
+  const float h = mode_h(j.mode);
+  note_launch();
+  switch (j.mode) {
+    case MODE_NEAREST: k_edge<MODE_NEAREST><<<grid, 128, 0, st>>>(j, tab, h); break;
+    case MODE_GAUSS2: k_edge<MODE_GAUSS2><<<grid, 128, 0, st>>>(j, tab, h); break;
+    case MODE_GAUSS5: k_edge<MODE_GAUSS5><<<grid, 128, 0, st>>>(j, tab, h); break;
+    case MODE_TRILINEAR: k_edge<MODE_TRILINEAR><<<grid, 128, 0, st>>>(j, tab, h); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+// -------------------------------------------------------------- gather path
+
+// Extent of the pixel-point box around a target tap t: a pixel at p reaches
+// t iff t - lo <= p < t + hi per axis (window rules of each inserter).
+template <int MODE> struct Reach;
+template <> struct Reach<MODE_GAUSS5> { static constexpr float lo = 2.5f, hi = 3.5f; };
+template <> struct Reach<MODE_GAUSS2> { static constexpr float lo = 1.0f, hi = 1.0f; };
+template <> struct Reach<MODE_TRILINEAR> { static constexpr float lo = 1.0f, hi = 1.0f; };
+template <> struct Reach<MODE_NEAREST> { static constexpr float lo = 0.5f, hi = 0.5f; };
+
+// Exact window membership of tap coordinate t for a pixel coordinate p.
+template <int MODE> __device__ __forceinline__ bool in_window(int t, float p) {
+  const float tf = (float)t;
+  if (MODE == MODE_GAUSS5) return __fadd_rn(tf, -2.5f) <= p && p < __fadd_rn(tf, 3.5f);
+  if (MODE == MODE_NEAREST) {
+    const float s = __fadd_rn(p, 0.5f);
+    return tf <= s && s < __fadd_rn(tf, 1.0f);
+  }
+  return __fadd_rn(tf, -1.0f) <= p && p < __fadd_rn(tf, 1.0f);
+}
+
+constexpr float kDel = 0.02f;     // slack on the approximate plane geometry
+constexpr float kPlaneTol = 0.05f;
+
+// Range of dot(m, q) over the box q in [lo, hi] (per axis).
+__device__ __forceinline__ void box_dot(const float *m, const float *lo, const float *hi, float &mn,
+                                        float &mx) {
+  mn = 0.f; mx = 0.f;
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    const float u = m[a] * lo[a], v = m[a] * hi[a];
+    mn += fminf(u, v);
+    mx += fmaxf(u, v);
+  }
+}
+
+template <int MODE, int TX, int TY, int TZ>
+__device__ __forceinline__ void gather_tile(const InsertJob &J, int bx, int by, int bz,
+                                            const float *s_exp, float h, int *s_hits,
+                                            int *s_wcount, float4 *s_pt, float2 *s_pv, int side,
+                                            int *err) {
+  constexpr int NV = TX * TY * TZ;
+  constexpr int VPT = (NV + 255) / 256;
+  const float RLO = Reach<MODE>::lo, RHI = Reach<MODE>::hi;
+  const int N = J.N, n2 = N >> 1, w2 = n2 + 1;
+  const float Nf = (float)N;
+  const int ex = min(bx + TX - 1, n2 - 1), ey = min(by + TY - 1, n2 - 1), ez = min(bz + TZ - 1, n2 - 1);
+
+  int vx[VPT], vy[VPT], vz[VPT];
+  bool valid[VPT];
+  double ar[VPT], ai[VPT], aw[VPT];
+  int touch = 0;
+#pragma unroll
+  for (int v = 0; v < VPT; v++) {
+    const int lin = threadIdx.x + v * 256;
+    vx[v] = bx + lin % TX;
+    vy[v] = by + (lin / TX) % TY;
+    vz[v] = bz + lin / (TX * TY);
+    valid[v] = lin < NV && vx[v] <= ex && vy[v] <= ey && vz[v] <= ez;
+    ar[v] = ai[v] = aw[v] = 0.0;
+  }
+
+  const int total = J.np * J.nsym;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int base = 0; base < total; base += 256) {
+    // ---- cull: does slice s's plane pass within reach of this tile?
+    const int s = base + threadIdx.x;
+    bool hit = false;
+    if (s < total && __ldg(&J.pw[s / J.nsym]) != 0.0f) {
+      const float n[3] = {__ldg(&J.t3d[9 * s + 6]), __ldg(&J.t3d[9 * s + 7]),
+                          __ldg(&J.t3d[9 * s + 8])};
+      const float lo[3] = {bx - RLO - kDel, by - RLO - kDel, bz - RLO - kDel};
+      const float hi[3] = {ex + RHI + kDel, ey + RHI + kDel, ez + RHI + kDel};
+      float mn, mx;
+      box_dot(n, lo, hi, mn, mx);
+      // the mirrored box (-tile) gives (-mx, -mn): the same test
+      hit = mn <= kPlaneTol && mx >= -kPlaneTol;
+    }
+    const unsigned b = __ballot_sync(0xffffffffu, hit);
+    if (lane == 0) s_wcount[warp] = __popc(b);
+    __syncthreads();
+    int off = 0, tot = 0;
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      const int c = s_wcount[i];
+      off += (i < warp) ? c : 0;
+      tot += c;
+    }
+    if (hit) s_hits[off + __popc(b & ((1u << lane) - 1u))] = s;
+    __syncthreads();
+
+    for (int hI = 0; hI < tot; hI++) {
+      const int s2 = s_hits[hI];
+      const int p = s2 / J.nsym;
+      float M[9];
+#pragma unroll
+      for (int i = 0; i < 9; i++) M[i] = __ldg(&J.t3d[9 * s2 + i]);
+      const float *m0 = M, *m1 = M + 3, *nrm = M + 6;
+      const float w = __ldg(&J.pw[p]);
+      const float2 *sl = J.slices + (size_t)p * N * w2;
+      float inv0[3];
+#pragma unroll
+      for (int a = 0; a < 3; a++) inv0[a] = fabsf(m0[a]) > 1e-4f ? 1.0f / m0[a] : 0.0f;
+
+#pragma unroll 1
+      for (int pass = 0; pass < 2; pass++) {
+        const int sg = pass ? -1 : 1;
+        float lo[3], hi[3];
+        if (!pass) {
+          lo[0] = bx; lo[1] = by; lo[2] = bz; hi[0] = ex; hi[1] = ey; hi[2] = ez;
+        } else {
+          lo[0] = -ex; lo[1] = -ey; lo[2] = -ez; hi[0] = -bx; hi[1] = -by; hi[2] = -bz;
+        }
+#pragma unroll
+        for (int a = 0; a < 3; a++) { lo[a] -= RLO + kDel; hi[a] += RHI + kDel; }
+        float xl, xh, yl, yh;
+        box_dot(m0, lo, hi, xl, xh);
+        box_dot(m1, lo, hi, yl, yh);
+        const int px0 = max(0, (int)floorf(xl) - 1), px1 = min(n2, (int)ceilf(xh) + 1);
+        const int py0 = max(-n2, (int)floorf(yl) - 1), py1 = min(n2 - 1, (int)ceilf(yh) + 1);
+        if (px0 > px1 || py0 > py1) continue;
+        int PW = px1 - px0 + 1, PH = py1 - py0 + 1;
+        if (PW > side || PH > side) {
+          // Cannot happen for an orthonormal block; record and stay in bounds.
+          if (threadIdx.x == 0) atomicOr(err, 2);
+          PW = min(PW, side);
+          PH = min(PH, side);
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < PW * PH; i += 256) {
+          const int x = px0 + i % PW, y = py0 + i / PW;
+          float4 pt;
+          float2 pv;
+          if (x > __ldg(&J.xmax[y + n2])) {
+            pt = make_float4(1e30f, 1e30f, 1e30f, 0.f);
+            pv = make_float2(0.f, 0.f);
+          } else {
+            pixel_coords(__ldg(&J.rtab[x + n2]), __ldg(&J.rtab[y + n2]), M, Nf, pt.x, pt.y, pt.z);
+            pt.w = w;
+            pv = slice_value(sl, N, x, y);
+          }
+          s_pt[i] = pt;
+          s_pv[i] = pv;
+        }
+        __syncthreads();
+
+#pragma unroll
+        for (int v = 0; v < VPT; v++) {
+          if (!valid[v]) continue;
+          const bool origin = vx[v] == 0 && vy[v] == 0 && vz[v] == 0;
+          if (pass && origin) continue;  // the origin tap adds no conjugate
+          const int t[3] = {sg * vx[v], sg * vy[v], sg * vz[v]};
+          const float tlo[3] = {t[0] - RLO - kDel, t[1] - RLO - kDel, t[2] - RLO - kDel};
+          const float thi[3] = {t[0] + RHI + kDel, t[1] + RHI + kDel, t[2] + RHI + kDel};
+          float dmn, dmx;
+          box_dot(nrm, tlo, thi, dmn, dmx);
+          if (dmn > kPlaneTol || dmx < -kPlaneTol) continue;
+          float ryl, ryh;
+          box_dot(m1, tlo, thi, ryl, ryh);
+          const int r0 = max(py0, (int)ceilf(ryl)), r1 = min(py0 + PH - 1, (int)floorf(ryh));
+          float pre = 0.f, pim = 0.f, pwt = 0.f;
+          int cnt = 0;
+          for (int y = r0; y <= r1; y++) {
+            float xlo = (float)px0, xhi = (float)(px0 + PW - 1);
+#pragma unroll
+            for (int a = 0; a < 3; a++) {
+              const float c = m1[a] * (float)y;
+              const float L = tlo[a] - c, U = thi[a] - c;
+              if (inv0[a] > 0.f) { xlo = fmaxf(xlo, L * inv0[a]); xhi = fminf(xhi, U * inv0[a]); }
+              else if (inv0[a] < 0.f) { xlo = fmaxf(xlo, U * inv0[a]); xhi = fminf(xhi, L * inv0[a]); }
+              else {
+                const float slack = 1e-4f * (float)(n2 + 1);
+                if (L > slack || U < -slack) xhi = -1.f;
+              }
+            }
+            const int c0 = max(px0, (int)ceilf(xlo));
+            const int c1 = min(px0 + PW - 1, (int)floorf(xhi));
+            const int rowoff = (y - py0) * PW - px0;
+            for (int x = c0; x <= c1; x++) {
+              const float4 pt = s_pt[rowoff + x];
+              if (!(in_window<MODE>(t[0], pt.x) && in_window<MODE>(t[1], pt.y) &&
+                    in_window<MODE>(t[2], pt.z)))
+                continue;
+              const float2 pv = s_pv[rowoff + x];
+              float vre, vim, vw;
+              tap_value<MODE>(t[0], t[1], t[2], pt.x, pt.y, pt.z, pv.x, pv.y, pt.w, h, s_exp, vre,
+                              vim, vw);
+              pre += vre;
+              pim += vim;
+              pwt += vw;
+              cnt++;
+            }
+          }
+          if (!cnt) continue;
+          if (origin) {
+            ar[v] += pre;          // real part only; the imaginary part is set to 0
+            aw[v] += pwt;
+            touch = 1;
+          } else if (pass) {
+            ar[v] += pre;          // conjugate add (re, -im)
+            ai[v] -= pim;
+            if (vx[v] != 0) aw[v] += pwt;   // x=0 conjugates carry no weight
+          } else {
+            ar[v] += pre;
+            ai[v] += pim;
+            aw[v] += pwt;
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+
+  // ---- write back: the tile owns these cells for the whole launch.
+  const size_t nxf = (size_t)N + 2;
+#pragma unroll
+  for (int v = 0; v < VPT; v++) {
+    if (!valid[v]) continue;
+    if (ar[v] == 0.0 && ai[v] == 0.0 && aw[v] == 0.0 && !(touch && vx[v] == 0 && vy[v] == 0 && vz[v] == 0))
+      continue;
+    const size_t row = (size_t)(vy[v] < 0 ? N + vy[v] : vy[v]);
+    const size_t slab = (size_t)(vz[v] < 0 ? N + vz[v] : vz[v]);
+    const size_t di = (size_t)vx[v] * 2 + row * nxf + slab * nxf * (size_t)N;
+    const size_t ni = (size_t)vx[v] + row * (size_t)w2 + slab * (size_t)w2 * (size_t)N;
+    float2 d = *reinterpret_cast<float2 *>(&J.data[di]);
+    d.x = __fadd_rn(d.x, (float)ar[v]);
+    if (touch && vx[v] == 0 && vy[v] == 0 && vz[v] == 0) d.y = 0.0f;
+    else d.y = __fadd_rn(d.y, (float)ai[v]);
+    *reinterpret_cast<float2 *>(&J.data[di]) = d;
+    J.norm[ni] = __fadd_rn(J.norm[ni], (float)aw[v]);
+  }
+}
+
+template <int TX, int TY, int TZ>
+__global__ void __launch_bounds__(256) k_gather(const InsertJob *__restrict__ jobs,
+                                                const int2 *__restrict__ work, int nwork,
+                                                int *counter, const float *__restrict__ exp_g,
+                                                float h2, float h5, int side, int max_mode,
+                                                int *err) {
+  __shared__ float s_exp[1000];
+  __shared__ int s_hits[256];
+  __shared__ int s_wcount[8];
+  __shared__ int s_work;
+  extern __shared__ float4 s_dyn[];
+  float4 *s_pt = s_dyn;
+  float2 *s_pv = reinterpret_cast<float2 *>(s_dyn + side * side);
+  for (int i = threadIdx.x; i < 1000; i += blockDim.x) s_exp[i] = exp_g[i];
+  (void)max_mode;
+  while (true) {
+    __syncthreads();
+    if (threadIdx.x == 0) s_work = atomicAdd(counter, 1);
+    __syncthreads();
+    const int wi = s_work;
+    if (wi >= nwork) break;
+    const int2 wk = work[wi];
+    const InsertJob J = jobs[wk.x];
+    const int n2 = J.N >> 1;
+    const int tix = wk.y % J.tiles_x, tiy = (wk.y / J.tiles_x) % J.tiles_y,
+              tiz = wk.y / (J.tiles_x * J.tiles_y);
+    const int bx = tix * TX, by = -n2 + 1 + tiy * TY, bz = -n2 + 1 + tiz * TZ;
+    switch (J.mode) {
+      case MODE_GAUSS2:
+        gather_tile<MODE_GAUSS2, TX, TY, TZ>(J, bx, by, bz, s_exp, h2, s_hits, s_wcount, s_pt, s_pv, side, err);
+        break;
+      case MODE_GAUSS5:
+        gather_tile<MODE_GAUSS5, TX, TY, TZ>(J, bx, by, bz, s_exp, h5, s_hits, s_wcount, s_pt, s_pv, side, err);
+        break;
+      case MODE_NEAREST:
+        gather_tile<MODE_NEAREST, TX, TY, TZ>(J, bx, by, bz, s_exp, h2, s_hits, s_wcount, s_pt, s_pv, side, err);
+        break;
+      case MODE_TRILINEAR:
+        gather_tile<MODE_TRILINEAR, TX, TY, TZ>(J, bx, by, bz, s_exp, h2, s_hits, s_wcount, s_pt, s_pv, side, err);
+        break;
+      default:
+        if (threadIdx.x == 0) atomicOr(err, 4);
+    }
+  }
+}
+
+static float reach_sum(int mode) {
+  switch (mode) {
+    case MODE_GAUSS5: return 6.0f;
+    case MODE_NEAREST: return 1.0f;
+    default: return 2.0f;
+  }
+}
+
+// Patch side bound: the pixel-space extent of the tile box grown by the
+// window reach, projected on a unit in-plane axis, plus rounding margins.
+static int patch_side(int tile, int max_mode) {
+  const TileShape &t = kTiles[tile];
+  const float r = reach_sum(max_mode) + 2 * kDel;
+  const float ex = t.tx - 1 + r, ey = t.ty - 1 + r, ez = t.tz - 1 + r;
+  return (int)std::ceil(std::sqrt(ex * ex + ey * ey + ez * ez)) + 5;
+}
+
+void gather_tiles(int N, int mode, int tile, int corners, std::vector<int> &out, int &tx, int &ty,
+                  int &tz) {
+  const TileShape &T = kTiles[tile];
+  const int n2 = N / 2;
+  tx = (n2 + T.tx - 1) / T.tx;
+  ty = (N - 1 + T.ty - 1) / T.ty;
+  tz = (N - 1 + T.tz - 1) / T.tz;
+  // Kept pixels satisfy round(hypot(x,y)) <= N/2, so their points lie within
+  // N/2 + 0.5 of the origin (to float rounding); corners mode keeps the whole
+  // square (radius N/2 * sqrt 2).  A tile farther than that plus the window
+  // reach (per axis, hence x sqrt 3) receives nothing.
+  const double reach = reach_sum(mode) * 0.5 + 0.5;
+  const double rpix = corners ? n2 * 1.41422 + 1.0 : n2 + 0.5 + 0.01;
+  const double rmax = rpix + reach * 1.7321 + 0.1;
+  std::vector<std::pair<double, int>> order;
+  for (int iz = 0; iz < tz; iz++)
+    for (int iy = 0; iy < ty; iy++)
+      for (int ix = 0; ix < tx; ix++) {
+        const int bx = ix * T.tx, by = -n2 + 1 + iy * T.ty, bz = -n2 + 1 + iz * T.tz;
+        const int ex = std::min(bx + T.tx - 1, n2 - 1), ey = std::min(by + T.ty - 1, n2 - 1),
+                  ez = std::min(bz + T.tz - 1, n2 - 1);
+        auto dmin = [](int a, int b) {
+          return (a <= 0 && b >= 0) ? 0.0 : (double)std::min(std::abs(a), std::abs(b));
+        };
+        const double dx = dmin(bx, ex), dy = dmin(by, ey), dz = dmin(bz, ez);
+        const double d = std::sqrt(dx * dx + dy * dy + dz * dz);
+        if (d <= rmax) order.push_back({d, ix + tx * (iy + ty * iz)});
+      }
+  // Nearest tiles first: they meet the most slices, so they start first.
+  std::stable_sort(order.begin(), order.end());
+  out.clear();
+  for (auto &o : order) out.push_back(o.second);
+}
+
+template <int TX, int TY, int TZ>
+static cudaError_t launch_gather_t(const InsertJob *d_jobs, int nwork, const int2 *d_work,
+                                   int *d_counter, int side, int max_mode, cudaStream_t st) {
+  const Consts &c = consts();
+  const size_t smem = (size_t)side * side * (sizeof(float4) + sizeof(float2));
+  static int configured = 0;
+  if (configured < (int)smem) {
+    cudaFuncSetAttribute(k_gather<TX, TY, TZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    configured = (int)smem;
+  }
+  int dev = 0, sms = 148, per_sm = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gather<TX, TY, TZ>, 256, smem);
+  if (per_sm < 1) per_sm = 1;
+  const int grid = std::max(1, std::min(nwork, sms * per_sm));
+  note_launch();
+  k_gather<TX, TY, TZ><<<grid, 256, smem, st>>>(d_jobs, d_work, nwork, d_counter, c.d_exp, c.h2,
+                                                c.h5, side, max_mode, c.d_err);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gather(const InsertJob *d_jobs, const InsertJob *h_jobs, int njobs,
+                          const int2 *d_work, int nwork, int tile, int *d_counter, int max_mode,
+                          cudaStream_t st) {
+  (void)h_jobs; (void)njobs;
+  if (nwork == 0) return cudaSuccess;
+  cudaError_t e = cudaMemsetAsync(d_counter, 0, sizeof(int), st);
+  if (e != cudaSuccess) return e;
+  const int side = patch_side(tile, max_mode);
+  switch (tile) {
+    case 0: return launch_gather_t<8, 8, 8>(d_jobs, nwork, d_work, d_counter, side, max_mode, st);
+    case 1: return launch_gather_t<16, 8, 8>(d_jobs, nwork, d_work, d_counter, side, max_mode, st);
+    case 2: return launch_gather_t<8, 8, 4>(d_jobs, nwork, d_work, d_counter, side, max_mode, st);
+    case 3: return launch_gather_t<16, 16, 4>(d_jobs, nwork, d_work, d_counter, side, max_mode, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace fr

@@ -1,0 +1,108 @@
+// fr_internal.h -- host/device structures and launcher declarations shared by
+// the library's translation units.  Not part of the C ABI.
+#pragma once
+#include <cuda_runtime.h>
+#include <cufft.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+namespace fr {
+
+// Per-size geometry tables, built on the host with the reference's own
+// scalar arithmetic and kept on the device.
+struct Geom {
+  int N = 0;
+  int corners = 0;
+  int *d_xmax = nullptr;     // [N]: largest x kept in row y (index y+N/2), -1 none
+  float *d_rtab = nullptr;   // [N+2]: (float)i/(float)N for i in [-N/2, N/2+1]
+  int *d_rim = nullptr;      // rim pixels (x | (y+N/2)<<16) that can reach the cube faces
+  int nrim = 0;
+  int npix = 0;              // kept pixels per slice
+  std::vector<int> xmax;     // host copy
+};
+
+// Gather tile shapes (the autotuner picks one of these by index).
+struct TileShape { int tx, ty, tz; };
+constexpr int kNumTiles = 4;
+extern const TileShape kTiles[kNumTiles];
+
+// One reconstruction's view for the insertion kernels.
+struct InsertJob {
+  float *data;               // [N][N][N+2]
+  float *norm;               // [N][N][N/2+1]
+  const float2 *slices;      // [np][N][N/2+1]
+  const float *t3d;          // [np*nsym][9]
+  const float *pw;           // [np] weight per particle
+  const int *xmax;
+  const float *rtab;
+  const int *rim;
+  int nrim;
+  const float *ssnr;         // optional [np][nssnr] class_ssnr tables (usessnr)
+  int nssnr;
+  float sscale;              // 2*(nssnr-1)/N (libEM/reconstructor.cpp:1162)
+  int N, mode, nsym, np;
+  int tiles_x, tiles_y, tiles_z;
+};
+
+// Launch accounting (fr_api.cu).
+void note_launch(int n = 1);
+
+struct Consts {
+  float *d_exp = nullptr;    // Util::fast_exp table [1000]
+  float h2 = 0, h5 = 0;      // 1/I2G, 1/I5G as the reference forms them
+  int *d_err = nullptr;      // device error word
+};
+Consts &consts();            // lazily initialised on the current device
+
+// Builds (or fetches) the geometry for size N.
+Geom *get_geom(int N, int corners);
+
+// Launchers (fr_insert.cu).  All enqueue on `st`.
+cudaError_t launch_compose(const float *d_arg, const float *d_sym, int np, int nsym, float *d_t3d,
+                           cudaStream_t st);
+cudaError_t launch_scatter(const InsertJob &j, cudaStream_t st);
+cudaError_t launch_gather(const InsertJob *d_jobs, const InsertJob *h_jobs, int njobs,
+                          const int2 *d_work, int nwork, int tile, int *d_counter, int max_mode,
+                          cudaStream_t st);
+cudaError_t launch_edge(const InsertJob &j, cudaStream_t st);
+// Ordered work list (tile ids of a job that can receive interior taps).
+void gather_tiles(int N, int mode, int tile, int corners, std::vector<int> &out, int &tx, int &ty,
+                  int &tz);
+
+// Prologue (fr_prologue.cu).
+cudaError_t launch_pad(const float *d_raw, int n, int box, int N, float *d_img, cudaStream_t st);
+void ctf_constants(float defocus, float dfdiff, float dfang, float voltage, float cs, float apix,
+                   float ampcont, int N, void *out);
+size_t ctf_dev_size();
+cudaError_t launch_ctf_flip_dev(cufftComplex *d_spec, const void *d_ctf, int n, int N,
+                                cudaStream_t st);
+cudaError_t launch_edge_mean(const float *d_img_off, const float *d_img_on, const void *d_ctf,
+                             int n, int N, float *d_mean, cudaStream_t st);
+cudaError_t launch_shift_corner(const float *d_img_off, const float *d_img_on, const void *d_ctf,
+                                const float *d_mean, const float *d_txy, int txy_stride, int n,
+                                int N, float scale_out, float *d_out, cudaStream_t st);
+
+// Finish / agreement (fr_finish.cu).
+cudaError_t launch_normalize(float *d_data, float *d_norm, int N, int sqrtnorm, cudaStream_t st);
+cudaError_t launch_depad_center(const float *d_real_padded, int N, float scale, float *d_out,
+                                cudaStream_t st);
+cudaError_t launch_seed(const float *d_seed, float w, int N, float *d_data, float *d_norm,
+                        cudaStream_t st);
+cudaError_t launch_agree_rt(const float *d_data, const float *d_norm, int N, const float *d_slices,
+                            const float *d_t3d, int np, int nsym, const float *d_w, float apix,
+                            const float *d_rtab, float *d_out, cudaStream_t st);
+cudaError_t launch_projection_rt(const float *d_data, const float *d_norm, int N,
+                                 const float *d_rot, const float *d_rtab, float *d_out,
+                                 cudaStream_t st);
+
+// Host-side symmetry (Symmetry3D::get_symmetries for c<n>/d<n>).
+int sym_ops(const std::string &sym, std::vector<float> &out);
+void eman_matrix(double az, double alt, double phi, float *m);
+
+}  // namespace fr

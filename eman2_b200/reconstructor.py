@@ -1,0 +1,410 @@
+"""Reconstructors.get("fourier", {...}) -- the drop-in for EMAN2's
+FourierReconstructor (libEM/reconstructor.h:388-565, libEM/reconstructor.cpp:686-1641)
+and its Python binding (libpyEM/libpyReconstructor2.cpp:192-226).
+
+Same method names, parameter keys, defaults, return values and exception
+classes; the work runs on the GPU through libeman2_b200.so.  Images may be
+``EMData`` objects, numpy arrays or torch tensors (host or CUDA; CUDA tensors
+are used in place).
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from .emdata import EMData
+from .exceptions import (ImageDimensionException, InvalidParameterException,
+                         NotExistingObjectException, NullPointerException, StateException,
+                         UnsupportedParameterException)
+from .transform import Transform
+
+# FourierReconstructor::get_param_types (libEM/reconstructor.h:501-516).
+PARAM_TYPES = {
+    "size": ("INTARRAY", "Required. The dimensions of the real-space output volume, including any "
+             "padding (must be handled by the calling application). Assumed that apix x/y/z "
+             "identical."),
+    "sym": ("STRING", "Required. The symmetry of the reconstructed volume, c?, d?, oct, tet, icos, "
+            "h?. Default is c1, ie - an asymmetric object"),
+    "mode": ("STRING", "Optional. Fourier pixel insertion mode name (nearest_neighbor, gauss_2, "
+             "gauss_3, gauss_5, gauss_5_slow, gypergeom_5, experimental) gauss_2 is the default."),
+    "corners": ("BOOL", "Optional. If not set, then reconstruction will cover a spherical volume "
+                "with a radius of nx/2. If set, the full Fourier volume will be reconstructed, but "
+                "will be ~2x slower."),
+    "sqrtnorm": ("BOOL", "Optional. When normalizing, additionally divides by the sqrt of the "
+                 "normalization factor to damp exaggerated features. Default is false."),
+    "usessnr": ("BOOL", "Optional. Looks for and uses the class_ssnr header parameter from each "
+                "slice to weight each voxel during insertion to the reconstruction."),
+    "verbose": ("BOOL", "Optional. Toggles writing useful information to standard out. Default is "
+                "false."),
+    "quiet": ("BOOL", "Optional. If false, print verbose information."),
+    "subvolume": ("INTARRAY", "Optional. (xorigin,yorigin,zorigin,xsize,ysize,zsize) all in "
+                  "Fourier pixels. Useful for parallelism."),
+    "savenorm": ("STRING", "Debug. Will cause the normalization volume to be written directly to "
+                 "the specified file when finish() is called."),
+    "normout": ("EMDATA", "Will write the normalization volume to the given EMData object file "
+                "when finish() is called."),
+}
+
+DESC = ("Reconstruction via direct Fourier methods using one of a variety of different kernels, "
+        "most of which are Gaussian based")
+
+
+def _host_or_device(a):
+    """numpy float32 contiguous array, or a contiguous float32 torch tensor as is."""
+    if isinstance(a, EMData):
+        return a.numpy()
+    if hasattr(a, "data_ptr"):
+        import torch
+        if a.dtype != torch.float32:
+            a = a.float()
+        return a.contiguous()
+    return np.ascontiguousarray(a, np.float32)
+
+
+def _rot_of(xf) -> np.ndarray:
+    if isinstance(xf, Transform):
+        return xf.rotation_block().astype(np.float32)
+    a = np.asarray(xf, np.float32)
+    if a.size == 12:
+        return np.ascontiguousarray(a.reshape(3, 4)[:, :3])
+    return np.ascontiguousarray(a.reshape(3, 3))
+
+
+def _trans_of(xf):
+    if isinstance(xf, Transform):
+        return float(xf.matrix[0, 3]), float(xf.matrix[1, 3])
+    a = np.asarray(xf, np.float32)
+    if a.size == 12:
+        m = a.reshape(3, 4)
+        return float(m[0, 3]), float(m[1, 3])
+    return 0.0, 0.0
+
+
+class FourierReconstructor:
+    """GPU FourierReconstructor with the reference's interface."""
+
+    NAME = "fourier"
+
+    def __init__(self, params: dict | None = None):
+        self.params: dict = {}
+        self._h = None
+        self._sig = None
+        self._state = 0
+        if params:
+            self.insert_params(params)
+
+    # --------------------------------------------------------- factory API
+    def get_name(self):
+        return self.NAME
+
+    def get_desc(self):
+        return DESC
+
+    def get_param_types(self):
+        return dict(PARAM_TYPES)
+
+    def get_params(self):
+        return dict(self.params)
+
+    def set_params(self, new_params: dict):
+        self.params = {}
+        self.insert_params(new_params)
+
+    def insert_params(self, new_params: dict):
+        """FactoryBase::insert_params (libEM/emobject.h:926-938): unknown key ->
+        InvalidParameterException."""
+        for k, v in new_params.items():
+            if k not in PARAM_TYPES:
+                raise InvalidParameterException(k)
+            self.params[k] = v
+
+    def set_param(self, key, value):
+        self.params[key] = value
+
+    def print_params(self):
+        for k, (t, d) in PARAM_TYPES.items():
+            print(f"{k}\t{t}\t{d}")
+
+    # --------------------------------------------------------- handle
+    @property
+    def N(self) -> int:
+        return int(self._size()[0])
+
+    def _size(self):
+        if "size" not in self.params:
+            raise NotExistingObjectException("The requested key does not exist: size")
+        size = self.params["size"]
+        if np.isscalar(size):
+            size = [int(size)] * 3
+        size = [int(s) for s in size]
+        if len(size) != 3:
+            raise InvalidParameterException("size must have three elements")
+        return size
+
+    def _mode(self) -> str:
+        return str(self.params.get("mode", "gauss_2"))
+
+    def _sym(self) -> str:
+        return str(self.params.get("sym", "c1"))
+
+    def _ensure_handle(self):
+        size = self._size()
+        mode = self._mode()
+        if mode not in _lib.MODE_IDS:
+            raise UnsupportedParameterException(
+                f"mode {mode!r}: the built inserters are {sorted(_lib.MODE_IDS)}")
+        if "subvolume" in self.params:
+            raise UnsupportedParameterException("subvolume reconstruction is not built")
+        sig = (tuple(size), mode, self._sym().lower(), bool(self.params.get("corners", False)),
+               bool(self.params.get("sqrtnorm", False)), bool(self.params.get("usessnr", False)))
+        if self._h is not None and sig == self._sig:
+            return
+        self.close()
+        lib = _lib.load()
+        p = _lib.fr_params()
+        p.nx, p.ny, p.nz = size
+        p.mode = _lib.MODE_IDS[mode]
+        p.sym = self._sym().encode()[:15]
+        p.corners = int(sig[3])
+        p.sqrtnorm = int(sig[4])
+        p.usessnr = int(sig[5])
+        p.verbose = int(bool(self.params.get("verbose", False)))
+        h = ctypes.c_void_p()
+        _lib.check(lib.fr_create(ctypes.byref(p), ctypes.byref(h)))
+        self._h = h
+        self._sig = sig
+
+    def close(self):
+        if self._h is not None:
+            _lib.load().fr_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    # --------------------------------------------------------- setup
+    def setup(self):
+        """FourierReconstructor::setup (libEM/reconstructor.cpp:730-818)."""
+        self._ensure_handle()
+        _lib.check(_lib.load().fr_setup(self._h))
+        self._state = 1
+
+    def setup_seed(self, seed, seed_weight: float):
+        """FourierReconstructor::setup_seed (libEM/reconstructor.cpp:820-902)."""
+        self._ensure_handle()
+        s = _host_or_device(seed)
+        N = self.N
+        if tuple(s.shape[-3:]) != (N, N, N + 2):
+            raise ImageDimensionException(
+                "The dimensions of the seed volume do not match the reconstruction size")
+        _lib.check(_lib.load().fr_setup_seed(self._h, _lib.ptr(s), float(seed_weight)))
+        self._state = 1
+
+    def setup_seedandweights(self, seed, weights):
+        """FourierReconstructor::setup_seedandweights (libEM/reconstructor.cpp:904-996)."""
+        self._ensure_handle()
+        s, w = _host_or_device(seed), _host_or_device(weights)
+        N = self.N
+        if tuple(s.shape[-3:]) != (N, N, N + 2) or tuple(w.shape[-3:]) != (N, N, N // 2 + 1):
+            raise ImageDimensionException(
+                "The dimensions of the seed volume do not match the reconstruction size")
+        _lib.check(_lib.load().fr_setup_seedandweights(self._h, _lib.ptr(s), _lib.ptr(w)))
+        self._state = 1
+
+    def clear(self):
+        _lib.check(_lib.load().fr_clear(self._h))
+
+    # --------------------------------------------------------- slices
+    def _check_image(self, a, complex_: bool):
+        N = self.N
+        want = (N, N + 2) if complex_ else (N, N)
+        if tuple(a.shape[-2:]) != want:
+            raise ImageDimensionException(
+                f"slice is {tuple(a.shape[-2:])}, expected {want} for a {N}^3 reconstruction")
+
+    def preprocess_slice(self, img, xform) -> EMData:
+        """FourierReconstructor::preprocess_slice (libEM/reconstructor.cpp:1022-1061):
+        translation (bilinear), phase origin to corner, r2c, x sqrt((N+2)/N)."""
+        if img is None:
+            raise NullPointerException("EMData pointer (input image) is NULL")
+        self._ensure_handle()
+        a = _host_or_device(img)
+        self._check_image(a, False)
+        tx, ty = _trans_of(xform if xform is not None else Transform())
+        inv = np.array([-tx, -ty], np.float32)   # the xform processor applies t^-1
+        N = self.N
+        out = np.empty((N, N + 2), np.float32)
+        _lib.check(_lib.load().fr_preprocess_slices(self._h, _lib.ptr(a), 1, _lib.ptr(inv),
+                                                    _lib.ptr(out)))
+        res = EMData(out, is_complex=True,
+                     attrs=dict(img.attrs) if isinstance(img, EMData) else None)
+        res.set_attr("reconstruct_preproc", 1)
+        return res
+
+    def _slice_of(self, img, xform):
+        if isinstance(img, EMData) and img.get_attr_default("reconstruct_preproc", 0):
+            a = img.numpy()
+            self._check_image(a, True)
+            return a
+        if isinstance(img, EMData) and img.is_complex():
+            a = img.numpy()
+            self._check_image(a, True)
+            return a
+        return self.preprocess_slice(img, xform).numpy()
+
+    def insert_slice(self, img, xform, weight: float = 1.0) -> int:
+        """FourierReconstructor::insert_slice (libEM/reconstructor.cpp:1064-1119).
+        Returns 0, or -1 when the weight is 0 (nothing inserted).  One slice per
+        call: the plain per-call GPU path."""
+        if img is None:
+            raise NullPointerException("EMData pointer (input image) is NULL")
+        if self._state != 1:
+            self._require_setup()
+        usessnr = bool(self.params.get("usessnr", False))
+        ssnr = None
+        if usessnr and isinstance(img, EMData) and img.has_attr("class_ssnr"):
+            ssnr = np.ascontiguousarray(img.get_attr("class_ssnr"), np.float32)
+        if (float(weight) == 0.0 and not usessnr) or (usessnr and ssnr is None):
+            return -1
+        sl = self._slice_of(img, xform)
+        rot = _rot_of(xform)
+        w = np.array([weight], np.float32)
+        status = (ctypes.c_int * 1)()
+        _lib.check(_lib.load().fr_insert_slices(
+            self._h, _lib.ptr(sl), 1, _lib.ptr(rot), _lib.ptr(w),
+            _lib.ptr(ssnr) if ssnr is not None else None,
+            int(ssnr.size) if ssnr is not None else 0, status, _lib.SCHED["scatter"]))
+        return int(status[0])
+
+    def insert_slices(self, slices, rots, weights, schedule: str = "auto"):
+        """Batched insert_slice over n preprocessed slices (n, N, N+2) with
+        rotation blocks (n, 3, 3) and weights (n,).  Returns the per-slice
+        insert_slice return values."""
+        if self._state != 1:
+            self._require_setup()
+        s = _host_or_device(slices)
+        self._check_image(s, True)
+        n = int(s.shape[0]) if s.ndim == 3 else 1
+        r = _host_or_device(rots)
+        w = _host_or_device(weights)
+        status = (ctypes.c_int * n)()
+        _lib.check(_lib.load().fr_insert_slices(self._h, _lib.ptr(s), n, _lib.ptr(r), _lib.ptr(w),
+                                                None, 0, status, _lib.SCHED[schedule]))
+        return list(status)
+
+    def insert_particles(self, images, meta, schedule: str = "auto"):
+        """The reference caller's per-particle loop (programs/e2spa_make3d.py:300-345)
+        for n raw box x box particles: edge-mean subtract, clip to N, CTF phase
+        flip, edge-mean subtract, shift, preprocess, insert.  ``meta`` is an
+        array of ``_lib.fr_particle`` (see ``eman2_b200.particles``)."""
+        if self._state != 1:
+            self._require_setup()
+        a = _host_or_device(images)
+        n, box = int(a.shape[0]), int(a.shape[-1])
+        _lib.check(_lib.load().fr_insert_particles(self._h, _lib.ptr(a), n, box,
+                                                   ctypes.cast(meta, ctypes.c_void_p),
+                                                   _lib.SCHED[schedule]))
+
+    def determine_slice_agreement(self, img, xform, weight: float = 1.0, sub: bool = True) -> int:
+        """FourierReconstructor::determine_slice_agreement
+        (libEM/reconstructor.cpp:1212-1257).  Sets reconstruct_norm,
+        reconstruct_absqual, reconstruct_absqual_lowres and reconstruct_weight
+        on ``img``; returns 0."""
+        if img is None:
+            raise NullPointerException("EMData pointer (input image) is NULL")
+        if self._state != 1:
+            self._require_setup()
+        sl = self._slice_of(img, xform)
+        rot = _rot_of(xform)
+        w = np.array([weight], np.float32)
+        apix = float(img.get_attr_default("apix_x", 1.0)) if isinstance(img, EMData) else 1.0
+        out = np.zeros(5, np.float32)
+        _lib.check(_lib.load().fr_determine_slice_agreement(
+            self._h, _lib.ptr(sl), 1, _lib.ptr(rot), _lib.ptr(w), apix, int(bool(sub)),
+            _lib.ptr(out)))
+        if isinstance(img, EMData):
+            img.set_attr("reconstruct_norm", float(out[0]))
+            img.set_attr("reconstruct_absqual", float(out[1]))
+            img.set_attr("reconstruct_absqual_lowres", float(out[2]))
+            img.set_attr("reconstruct_weight", float(out[4]))
+        return 0
+
+    def slice_agreement(self, slices, rots, weights, apix: float = 1.0) -> np.ndarray:
+        """Batched determine_slice_agreement(sub=False): (n, 5) array of
+        reconstruct_norm, _absqual, _absqual_lowres, _qual, _weight."""
+        s = _host_or_device(slices)
+        n = int(s.shape[0]) if s.ndim == 3 else 1
+        r = _host_or_device(rots)
+        w = _host_or_device(weights)
+        out = np.zeros((n, 5), np.float32)
+        _lib.check(_lib.load().fr_determine_slice_agreement(
+            self._h, _lib.ptr(s), n, _lib.ptr(r), _lib.ptr(w), float(apix), 0, _lib.ptr(out)))
+        return out
+
+    def projection(self, xform, ret_fourier: int = 1) -> EMData:
+        """FourierReconstructor::projection (libEM/reconstructor.cpp:1383-1445),
+        Fourier-space part (ret_fourier=1, no translation)."""
+        N = self.N
+        out = np.zeros((N, N + 2), np.float32)
+        rot = _rot_of(xform)
+        _lib.check(_lib.load().fr_projection(self._h, _lib.ptr(rot), _lib.ptr(out)))
+        if not ret_fourier:
+            raise UnsupportedParameterException("real-space projections are not built")
+        return EMData(out, is_complex=True)
+
+    # --------------------------------------------------------- results
+    def get_accumulators(self):
+        """Un-normalised (complex, weight) volumes: what finish(False) + normout
+        give before normalisation."""
+        N = self.N
+        d = np.empty((N, N, N + 2), np.float32)
+        n = np.empty((N, N, N // 2 + 1), np.float32)
+        _lib.check(_lib.load().fr_get_accumulators(self._h, _lib.ptr(d), _lib.ptr(n)))
+        return d, n
+
+    def finish(self, doift: bool = True) -> EMData:
+        """FourierReconstructor::finish (libEM/reconstructor.cpp:1552-1641).
+        doift: real N^3 map (phase origin at the centre); else the normalised
+        complex volume.  Fills the ``normout`` EMData if that param is set."""
+        if self._state != 1:
+            self._require_setup()
+        N = self.N
+        out = np.empty((N, N, N) if doift else (N, N, N + 2), np.float32)
+        norm = np.empty((N, N, N // 2 + 1), np.float32)
+        _lib.check(_lib.load().fr_finish(self._h, int(bool(doift)), _lib.ptr(out), _lib.ptr(norm)))
+        self._state = 2
+        if "normout" in self.params and isinstance(self.params["normout"], EMData):
+            self.params["normout"].set_data(norm)
+        if self.params.get("savenorm"):
+            np.save(str(self.params["savenorm"]), norm)
+        return EMData(out, is_complex=not doift)
+
+    def _require_setup(self):
+        raise StateException("setup() has not been called" if self._state == 0 else
+                             "finish() was called; call setup() again")
+
+
+class Reconstructors:
+    """Factory<Reconstructor> (libpyEM/libpyReconstructor2.cpp:221-226)."""
+
+    _known = {"fourier": FourierReconstructor}
+
+    @staticmethod
+    def get(name: str, params: dict | None = None):
+        cls = Reconstructors._known.get(name)
+        if cls is None:
+            raise NotExistingObjectException(f"No such an instance existing: {name}")
+        return cls(params)
+
+    @staticmethod
+    def get_list():
+        return list(Reconstructors._known)

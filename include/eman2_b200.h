@@ -1,0 +1,223 @@
+/*
+ * eman2_b200.h -- C ABI of the B200 direct Fourier inversion library
+ * (libeman2_b200.so).  Plain pointers and sizes; no C++ or torch types.
+ *
+ * The library replaces EMAN2's FourierReconstructor behind
+ * Reconstructors.get("fourier", {...}) (libEM/reconstructor.h:388-565,
+ * libEM/reconstructor.cpp:686-1641) and its Python binding
+ * (libpyEM/libpyReconstructor2.cpp:50-86,192-226).  Every entry point names
+ * the reference interface it stands in for.
+ *
+ * Volumes use the reference's layout:
+ *   complex volume : float[N][N][N+2]   (z, y, x-interleaved re/im, x = 0..N/2)
+ *   weight volume  : float[N][N][N/2+1]
+ *   slice          : float[N][N+2]      (r2c spectrum of an N x N image)
+ * Pointers may be host or device memory; the library detects which.
+ * All functions return FR_OK (0) or an FR_E* status; fr_last_error() gives
+ * the message of the calling thread's last failure.
+ */
+#ifndef EMAN2_B200_H
+#define EMAN2_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FR_API __attribute__((visibility("default")))
+
+/* Status codes; the Python layer raises the reference's exception class of
+ * the same meaning (libEM/exception.h). */
+enum {
+  FR_OK = 0,
+  FR_EINVAL_PARAM = 1,   /* InvalidParameterException (libEM/emobject.h:931-938) */
+  FR_EDIM = 2,           /* ImageDimensionException (libEM/reconstructor.cpp:767,861) */
+  FR_ENULL = 3,          /* NullPointerException (libEM/reconstructor.cpp:1067) */
+  FR_ESTATE = 4,         /* used before setup() or after finish() */
+  FR_ECUDA = 5,          /* CUDA / cuFFT runtime failure */
+  FR_ENOMEM = 6,         /* device allocation failed */
+  FR_EUNSUPPORTED = 7,   /* parameter value outside the built scope */
+  FR_ENOTEXIST = 8,      /* NotExistingObjectException (libEM/emdata_metadata.cpp:1142) */
+  FR_EDEVICE = 9         /* a kernel reported an internal consistency error */
+};
+
+/* Inserter modes (FourierPixelInserter3D factory names,
+ * libEM/reconstructor_tools.cpp:42-53). */
+enum {
+  FR_MODE_NEAREST = 1,   /* "nearest_neighbor" */
+  FR_MODE_GAUSS2 = 2,    /* "gauss_2" (default) */
+  FR_MODE_GAUSS5 = 5,    /* "gauss_5" */
+  FR_MODE_TRILINEAR = 6  /* "trilinear" */
+};
+
+/* Insertion schedules. */
+enum {
+  FR_SCHED_AUTO = 0,     /* pick by batch size and mode */
+  FR_SCHED_SCATTER = 1,  /* one thread per slice pixel, FP32 atomics */
+  FR_SCHED_GATHER = 2    /* voxel tiles own their cells; no atomics */
+};
+
+/* FourierReconstructor parameters (libEM/reconstructor.h:501-516). */
+typedef struct {
+  int nx, ny, nz;        /* "size": padded real-space volume (cubic, even) */
+  int mode;              /* FR_MODE_* */
+  char sym[16];          /* "c<n>" or "d<n>" */
+  int corners;           /* "corners" */
+  int sqrtnorm;          /* "sqrtnorm" */
+  int usessnr;           /* "usessnr" */
+  int verbose;           /* "verbose" */
+} fr_params;
+
+/* Per-particle metadata for the batched caller pipeline
+ * (programs/e2spa_make3d.py:300-345). */
+typedef struct {
+  float rot[9];          /* xform.projection rotation block, row-major */
+  float tx, ty;          /* xform.projection translation */
+  float weight;          /* insertion weight (<= 0: particle skipped) */
+  float defocus;         /* um; |defocus| <= 1e-4 disables the phase flip */
+  float dfdiff, dfang;   /* astigmatism */
+  float voltage, cs;     /* kV, mm */
+  float apix;            /* A/pixel */
+  float ampcont;         /* amplitude contrast, percent */
+} fr_particle;
+
+typedef struct fr_recon fr_recon;
+
+/* Factory<Reconstructor>::get("fourier", params) + set_params
+ * (libpyEM/libpyReconstructor2.cpp:221-226, libEM/emobject.h:916-938). */
+FR_API int fr_create(const fr_params *p, fr_recon **out);
+
+/* ~FourierReconstructor (libEM/reconstructor.h:400). */
+FR_API int fr_destroy(fr_recon *r);
+
+/* Binds the handle to an existing CUDA stream (cudaStream_t); 0 restores the
+ * handle's own stream. */
+FR_API int fr_set_stream(fr_recon *r, void *stream);
+
+/* FourierReconstructor::setup (libEM/reconstructor.cpp:730-818). */
+FR_API int fr_setup(fr_recon *r);
+
+/* FourierReconstructor::setup_seed (libEM/reconstructor.cpp:820-902):
+ * data = seed * seed_weight, weights = seed_weight (halved on the x=0 and
+ * x=Nyquist planes, four cells kept whole). seed: float[N][N][N+2]. */
+FR_API int fr_setup_seed(fr_recon *r, const float *seed, float seed_weight);
+
+/* FourierReconstructor::setup_seedandweights (libEM/reconstructor.cpp:904-996). */
+FR_API int fr_setup_seedandweights(fr_recon *r, const float *seed, const float *weights);
+
+/* FourierReconstructor::clear (libEM/reconstructor.cpp:999-1020). */
+FR_API int fr_clear(fr_recon *r);
+
+/* FourierReconstructor::preprocess_slice (libEM/reconstructor.cpp:1022-1061)
+ * for n real N x N images and translation-only transforms whose inverse
+ * translates by inv_txy[2*i], inv_txy[2*i+1] (the reference applies the
+ * inverse of the transform it is given, libEM/processor.cpp:11029).
+ * Writes n slices float[N][N+2]. */
+FR_API int fr_preprocess_slices(fr_recon *r, const float *imgs, int n, const float *inv_txy,
+                                float *out_slices);
+
+/* FourierReconstructor::insert_slice (libEM/reconstructor.cpp:1064-1119) for
+ * n preprocessed slices float[N][N+2] with rotation blocks rot[9*n] and
+ * weights[n].  status_out[i] (optional) receives insert_slice's return
+ * value (0, or -1 when the weight is 0).  ssnr (optional, nssnr entries per
+ * slice) carries class_ssnr for usessnr=1. */
+FR_API int fr_insert_slices(fr_recon *r, const float *slices, int n, const float *rot,
+                            const float *weights, const float *ssnr, int nssnr,
+                            int *status_out, int schedule);
+
+/* The reference caller's per-particle loop (programs/e2spa_make3d.py:300-345):
+ * edge-mean subtract, clip to N, CTF phase flip, edge-mean subtract,
+ * preprocess_slice with the inverted translation, insert_slice.  imgs:
+ * float[n][box][box]. */
+FR_API int fr_insert_particles(fr_recon *r, const float *imgs, int n, int box,
+                               const fr_particle *meta, int schedule);
+
+/* FourierReconstructor::determine_slice_agreement (libEM/reconstructor.cpp:1212-1257)
+ * for n preprocessed slices.  out[5*i..] = reconstruct_norm, _absqual,
+ * _absqual_lowres, _qual, _weight.  apix: the slices' apix_x.  sub=1 needs
+ * usessnr with class_ssnr (as in the reference). */
+FR_API int fr_determine_slice_agreement(fr_recon *r, const float *slices, int n,
+                                        const float *rot, const float *weights, float apix,
+                                        int sub, float *out);
+
+/* FourierReconstructor::projection (libEM/reconstructor.cpp:1383-1445),
+ * ret_fourier=1 form without the final translation: writes float[N][N+2]. */
+FR_API int fr_projection(fr_recon *r, const float *rot, float *out_slice);
+
+/* FourierReconstructor::finish (libEM/reconstructor.cpp:1552-1641).
+ * doift=1: out = float[N][N][N] real map (inverse FFT, depad, phase origin
+ * to centre); doift=0: out = normalised float[N][N][N+2] complex volume.
+ * normout (optional) = float[N][N][N/2+1] weights (the "normout" param).
+ * The handle needs fr_setup() again afterwards (ownership passes out). */
+FR_API int fr_finish(fr_recon *r, int doift, float *out, float *normout);
+
+/* Un-normalised accumulators (finish(False) + normout before normalisation);
+ * the form the reference's parallel make3d merges (programs/e2spa_make3d.py:175-188).
+ * Either pointer may be NULL. */
+FR_API int fr_get_accumulators(fr_recon *r, float *data, float *norm);
+
+/* Sizes and state. */
+FR_API int fr_get_size(const fr_recon *r, int *N);
+FR_API size_t fr_footprint_bytes(int N);
+
+/* Symmetry operators of a symmetry name (Symmetry3D::get_symmetries,
+ * libEM/symmetry.cpp:1240-1246) as rotation blocks; returns the count or -1. */
+FR_API int fr_sym_ops(const char *sym, float *out, int cap);
+
+/* Launch accounting and insertion-kernel timing.  With profiling on, CUDA
+ * events bracket every insertion launch (gather + face taps, or scatter) on
+ * the stream it runs on.  No counterpart in the reference (it has no timers
+ * on this path). */
+typedef struct {
+  long long kernel_launches;     /* kernels this library launched (cuFFT's not counted) */
+  long long insert_launches;     /* insertion passes (one gather or scatter pass each) */
+  long long slices_inserted;     /* particle-slices x symmetry copies inserted */
+  double insert_ms;              /* summed event time of the insertion passes */
+  double gather_ms;              /* summed event time of the gather kernel alone */
+  long long gather_launches;
+} fr_stats;
+FR_API int fr_profile(int on);
+FR_API int fr_stats_get(fr_stats *out);
+FR_API int fr_stats_reset(void);
+
+/* Last error message of the calling thread. */
+FR_API const char *fr_last_error(void);
+
+/* Library version string. */
+FR_API const char *fr_version(void);
+
+/* ---------------------------------------------------------------- batched
+ * Many independent reconstructions (uneven N, mode, symmetry) inserted by one
+ * persistent launch per chunk.  No counterpart in the reference beyond
+ * running several FourierReconstructors (even/odd half maps,
+ * programs/e2gmm.py:115-139). */
+typedef struct fr_batch fr_batch;
+
+/* Creates a batch of njobs reconstructions (each set up as fr_setup). */
+FR_API int fr_batch_create(const fr_params *jobs, int njobs, fr_batch **out);
+FR_API int fr_batch_destroy(fr_batch *b);
+FR_API int fr_batch_set_stream(fr_batch *b, void *stream);
+
+/* Inserts, for every job j, counts[j] particles whose images start at
+ * imgs[j] (float[counts[j]][box_j][box_j]) with metadata meta[j].  All jobs'
+ * particles go through one prologue pass per box size and one persistent
+ * insertion launch. */
+FR_API int fr_batch_insert_particles(fr_batch *b, const float *const *imgs, const int *boxes,
+                                     const int *counts, const fr_particle *const *meta);
+
+/* Finishes job j like fr_finish. */
+FR_API int fr_batch_finish(fr_batch *b, int job, int doift, float *out, float *normout);
+FR_API int fr_batch_get_accumulators(fr_batch *b, int job, float *data, float *norm);
+
+/* Tile shape / schedule selection for the gather insertion, measured on the
+ * device and cached per (N, mode, nsym).  Returns the chosen tile index. */
+FR_API int fr_autotune(int N, int mode, int nsym, int nparticles, int *tile_out,
+                       float *ms_out);
+FR_API int fr_set_tile(int N, int mode, int nsym, int tile);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* EMAN2_B200_H */

@@ -1,0 +1,348 @@
+"""CPU oracle for EMAN2's direct Fourier inversion (FourierReconstructor).
+
+TEST INFRASTRUCTURE ONLY.  The product (the ``eman2_b200`` package) never
+imports this module.  It is imported by ``tests/``, by the smoke check in
+``__graft_entry__.py`` and by the ``cpu_baseline`` / ``--impl reference`` legs
+of ``bench.py``, where it is the checker or the timed CPU baseline.
+
+Two precisions, one restatement (``fr_oracle.c``):
+
+* ``fp32`` -- FP32-faithful: the reference's operation order and rounding
+  points in strict IEEE single precision.  This is the stand-in for the
+  reference's own FourierReconstructor, which cannot be built here.
+* ``fp64`` -- the same algorithm in double precision (coordinates, weights,
+  accumulators); the FP64 oracle both GPU forms state their error against.
+
+The FFTs (numpy/pocketfft, float64) replace FFTW, which is not present; the
+FP32 path rounds each FFT result to float32, so it differs from an FFTW float
+transform at the 1e-7 level.  The restatement's insert_pixel/add_complex_at
+arithmetic is pinned bitwise against the reference's own inserter source
+(``build_ref.sh`` -> ``_ref/libfr_ref.so``; ``tests/test_oracle_ref.py``).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+BUILD = os.path.join(HERE, "_build")
+REF_SO = os.path.join(HERE, "_ref", "libfr_ref.so")
+
+MODES = {"nearest_neighbor": 1, "gauss_2": 2, "gauss_5": 5, "trilinear": 6}
+
+_F = ctypes.POINTER(ctypes.c_float)
+_D = ctypes.POINTER(ctypes.c_double)
+_libs: dict = {}
+
+
+def build(ref: bool = True) -> None:
+    """Compile the oracle libraries (and the reference pin, when its tree is present)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    if ref:
+        subprocess.run(["sh", os.path.join(HERE, "build_ref.sh")], check=True,
+                       stdout=subprocess.DEVNULL)
+
+
+def _lib(kind: str = "fp32"):
+    if kind in _libs:
+        return _libs[kind]
+    name = {"fp32": "liborfp32.so", "fp64": "liborfp64.so", "omp": "liborfp32_omp.so"}[kind]
+    path = os.path.join(BUILD, name)
+    if not os.path.exists(path):
+        build(ref=False)
+    lib = ctypes.CDLL(path)
+    R = _F if kind in ("fp32", "omp") else _D
+    lib.or_insert_slice.argtypes = [R, R, ctypes.c_int, ctypes.c_int, _F, _F, ctypes.c_int,
+                                    ctypes.c_float, ctypes.c_int, _F, ctypes.c_int]
+    lib.or_insert_batch.argtypes = [R, R, ctypes.c_int, ctypes.c_int, _F, ctypes.c_int, _F, _F,
+                                    ctypes.c_int, _F, ctypes.c_int]
+    lib.or_insert_pixels.argtypes = [ctypes.c_int, R, R, ctypes.c_int, _F, ctypes.c_long]
+    lib.or_normalize.argtypes = [R, R, ctypes.c_int, ctypes.c_int]
+    lib.or_compare_slice.argtypes = [R, R, ctypes.c_int, _F, _F, ctypes.c_int, ctypes.c_float,
+                                     ctypes.c_float, _F]
+    lib.or_sym_ops.argtypes = [ctypes.c_char, ctypes.c_int, _F, ctypes.c_int]
+    lib.or_eman_matrix.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_double, _F]
+    lib.or_quaternion_matrix.argtypes = [ctypes.c_double] * 4 + [_F]
+    lib.or_compose.argtypes = [_F, _F, _F]
+    lib.or_edge_mean.argtypes = [_F, ctypes.c_int, ctypes.c_int]
+    lib.or_edge_mean.restype = ctypes.c_float
+    lib.or_ctf_sign.argtypes = [_F, ctypes.c_int] + [ctypes.c_float] * 7
+    lib.or_translate_bilinear.argtypes = [_F, _F, ctypes.c_int, ctypes.c_int, ctypes.c_float,
+                                          ctypes.c_float]
+    lib.or_fast_exp_value.argtypes = [ctypes.c_float]
+    lib.or_fast_exp_value.restype = ctypes.c_float
+    lib.or_hypot_int.argtypes = [ctypes.c_int, ctypes.c_int]
+    if kind == "omp":
+        lib.or_insert_batch_omp.argtypes = [R, R, ctypes.c_int, ctypes.c_int, _F, ctypes.c_int, _F,
+                                            _F, ctypes.c_int, _F, ctypes.c_int]
+    _libs[kind] = lib
+    return lib
+
+
+def _fp(a: np.ndarray):
+    assert a.dtype == np.float32 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(_F)
+
+
+def _rp(a: np.ndarray):
+    if a.dtype == np.float32:
+        return a.ctypes.data_as(_F)
+    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(_D)
+
+
+# ----------------------------------------------------------------- transforms
+
+def eman_matrix(az: float, alt: float, phi: float) -> np.ndarray:
+    m = np.zeros(9, np.float32)
+    _lib().or_eman_matrix(az, alt, phi, _fp(m))
+    return m.reshape(3, 3)
+
+
+def quaternion_matrix(q) -> np.ndarray:
+    m = np.zeros(9, np.float32)
+    _lib().or_quaternion_matrix(float(q[0]), float(q[1]), float(q[2]), float(q[3]), _fp(m))
+    return m.reshape(3, 3)
+
+
+def sym_ops(sym: str) -> np.ndarray:
+    """Symmetry operators of ``c<n>`` / ``d<n>`` as (nsym, 3, 3) float32."""
+    sym = sym.lower()
+    kind, n = sym[0], int(sym[1:] or 1)
+    out = np.zeros(9 * 2 * n, np.float32)
+    k = _lib().or_sym_ops(kind.encode(), n, _fp(out), 2 * n)
+    if k < 0:
+        raise ValueError(f"unsupported symmetry {sym}")
+    return out[: 9 * k].reshape(k, 3, 3)
+
+
+def compose(a: np.ndarray, b: np.ndarray) -> np.ndarray:
+    a = np.ascontiguousarray(a, np.float32).reshape(9)
+    b = np.ascontiguousarray(b, np.float32).reshape(9)
+    out = np.zeros(9, np.float32)
+    _lib().or_compose(_fp(a), _fp(b), _fp(out))
+    return out.reshape(3, 3)
+
+
+# ------------------------------------------------------------------ the volume
+
+class OracleVolume:
+    """Un-normalised (complex, weight) accumulators in the reference layout."""
+
+    def __init__(self, N: int, precision: str = "fp32"):
+        self.N = N
+        self.kind = precision
+        dt = np.float32 if precision in ("fp32", "omp") else np.float64
+        self.data = np.zeros((N, N, N + 2), dt)
+        self.norm = np.zeros((N, N, N // 2 + 1), dt)
+
+    @property
+    def lib(self):
+        return _lib(self.kind)
+
+    def insert(self, slices, rots, weights, mode="gauss_2", sym="c1", corners=False):
+        """insert_slice for n preprocessed slices (n, N, N+2) float32 with
+        orientation blocks rots (n, 3, 3) and weights (n,)."""
+        slices = np.ascontiguousarray(slices, np.float32).reshape(-1, self.N, self.N + 2)
+        n = slices.shape[0]
+        rots = np.ascontiguousarray(rots, np.float32).reshape(n, 9)
+        weights = np.ascontiguousarray(weights, np.float32).reshape(n)
+        ops = np.ascontiguousarray(sym_ops(sym)).reshape(-1, 9)
+        rc = self.lib.or_insert_batch(_rp(self.data), _rp(self.norm), self.N, MODES[mode],
+                                      _fp(slices), n, _fp(rots), _fp(ops), ops.shape[0],
+                                      _fp(weights), int(bool(corners)))
+        if rc:
+            raise RuntimeError(f"oracle insert failed rc={rc}")
+
+    def insert_omp(self, slices, rots, weights, mode="gauss_2", sym="c1", threads=0):
+        assert self.kind == "omp"
+        slices = np.ascontiguousarray(slices, np.float32).reshape(-1, self.N, self.N + 2)
+        n = slices.shape[0]
+        rots = np.ascontiguousarray(rots, np.float32).reshape(n, 9)
+        weights = np.ascontiguousarray(weights, np.float32).reshape(n)
+        ops = np.ascontiguousarray(sym_ops(sym)).reshape(-1, 9)
+        rc = self.lib.or_insert_batch_omp(_rp(self.data), _rp(self.norm), self.N, MODES[mode],
+                                          _fp(slices), n, _fp(rots), _fp(ops), ops.shape[0],
+                                          _fp(weights), int(threads))
+        if rc:
+            raise RuntimeError(f"oracle insert failed rc={rc}")
+
+    def insert_pixels(self, mode: str, px: np.ndarray):
+        px = np.ascontiguousarray(px, np.float32).reshape(-1, 6)
+        self.lib.or_insert_pixels(MODES[mode], _rp(self.data), _rp(self.norm), self.N,
+                                  _fp(px), px.shape[0])
+
+    def compare(self, slice_, rot, weight=1.0, sym="c1", apix=1.0):
+        """determine_slice_agreement(sub=False) statistics for one slice:
+        (norm, absqual, absqual_lowres, qual, weight)."""
+        s = np.ascontiguousarray(slice_, np.float32).reshape(self.N, self.N + 2)
+        ops = sym_ops(sym)
+        t3d = np.stack([compose(rot, o) for o in ops]).astype(np.float32).reshape(-1, 9)
+        out = np.zeros(5, np.float32)
+        self.lib.or_compare_slice(_rp(self.data), _rp(self.norm), self.N, _fp(s),
+                                  _fp(np.ascontiguousarray(t3d)), t3d.shape[0], float(weight),
+                                  float(apix), _fp(out))
+        return out
+
+    def copy(self):
+        o = OracleVolume.__new__(OracleVolume)
+        o.N, o.kind = self.N, self.kind
+        o.data, o.norm = self.data.copy(), self.norm.copy()
+        return o
+
+    def normalize(self, sqrtnorm=False):
+        self.lib.or_normalize(_rp(self.data), _rp(self.norm), self.N, int(bool(sqrtnorm)))
+
+    def finish(self, doift=True, sqrtnorm=False):
+        """FourierReconstructor::finish (libEM/reconstructor.cpp:1552-1641):
+        normalise; optionally inverse FFT (x 1/N^3), depad, phase-origin to
+        centre.  Returns (volume, norm) like finish() + normout."""
+        self.normalize(sqrtnorm)
+        if not doift:
+            return self.data, self.norm
+        N = self.N
+        c = self.data.astype(np.float64).view(np.complex128)
+        real = np.fft.irfftn(c, s=(N, N, N), axes=(0, 1, 2), norm="forward")
+        if self.kind == "fp64":
+            real = real * (1.0 / (N * N * N))
+        else:
+            real = real.astype(np.float32) * np.float32(1.0 / (N * N * N))
+        real = np.roll(real, (N // 2, N // 2, N // 2), axis=(0, 1, 2))
+        return real, self.norm
+
+
+# ------------------------------------------------------------------- prologue
+
+def edge_mean(img: np.ndarray) -> np.float32:
+    img = np.ascontiguousarray(img, np.float32)
+    return np.float32(_lib().or_edge_mean(_fp(img), img.shape[1], img.shape[0]))
+
+
+def clip_pad(img: np.ndarray, N: int) -> np.ndarray:
+    """clip_inplace(Region((nx-N)//2, (ny-N)//2, N, N)) with zero fill
+    (libEM/emdata.cpp:350)."""
+    ny, nx = img.shape
+    x0, y0 = (nx - N) // 2, (ny - N) // 2
+    out = np.zeros((N, N), np.float32)
+    for y in range(N):
+        sy = y + y0
+        if 0 <= sy < ny:
+            xs = np.arange(N) + x0
+            ok = (xs >= 0) & (xs < nx)
+            out[y, ok] = img[sy, xs[ok]]
+    return out
+
+
+def ctf_sign(N: int, defocus, voltage=300.0, cs=2.7, apix=1.0, ampcont=10.0, dfdiff=0.0,
+             dfang=0.0) -> np.ndarray:
+    out = np.zeros((N, N // 2 + 1), np.float32)
+    _lib().or_ctf_sign(_fp(out), N, float(defocus), float(dfdiff), float(dfang), float(voltage),
+                       float(cs), float(apix), float(ampcont))
+    return out
+
+
+def _fft_f32(img: np.ndarray) -> np.ndarray:
+    """Unnormalised r2c of a float32 image, rounded to complex64 (FFTW stand-in)."""
+    return np.fft.rfft2(img.astype(np.float64)).astype(np.complex64)
+
+
+def _ift_f32(spec: np.ndarray, N: int) -> np.ndarray:
+    """do_ift (libEM/emdata_transform.cpp:392-425): unnormalised c2r, then x 1/N^2."""
+    r = np.fft.irfft2(spec.astype(np.complex128), s=(N, N), norm="forward").astype(np.float32)
+    return r * np.float32(1.0 / (N * N))
+
+
+def ctf_flip(img: np.ndarray, ctf: dict) -> np.ndarray:
+    """FFT -> x CTF_SIGN -> IFT (programs/e2spa_make3d.py:316-326, one flip)."""
+    N = img.shape[0]
+    F = _fft_f32(img)
+    s = ctf_sign(N, ctf["defocus"], ctf.get("voltage", 300.0), ctf.get("cs", 2.7),
+                 ctf.get("apix", 1.0), ctf.get("ampcont", 10.0), ctf.get("dfdiff", 0.0),
+                 ctf.get("dfang", 0.0))
+    F = (F.real * s + 1j * (F.imag * s)).astype(np.complex64)
+    return _ift_f32(F, N)
+
+
+def translate(img: np.ndarray, tx: float, ty: float) -> np.ndarray:
+    img = np.ascontiguousarray(img, np.float32)
+    out = np.zeros_like(img)
+    _lib().or_translate_bilinear(_fp(img), _fp(out), img.shape[1], img.shape[0], float(tx),
+                                 float(ty))
+    return out
+
+
+def _near_int(v: float) -> float:
+    c, f = np.ceil(np.float32(v)), np.floor(np.float32(v))
+    if abs(v - c) < 1e-6:
+        return c
+    if abs(v - f) < 1e-6:
+        return f
+    return v
+
+
+def preprocess_slice(img: np.ndarray, inv_tx: float = 0.0, inv_ty: float = 0.0) -> np.ndarray:
+    """FourierReconstructor::preprocess_slice (libEM/reconstructor.cpp:1022-1061)
+    for a translation-only transform whose inverse translates by
+    (inv_tx, inv_ty): bilinear xform (identity -> copy), phase origin to corner,
+    r2c, x sqrt((N+2)/N).  Returns the (N, N+2) float32 interleaved slice."""
+    N = img.shape[0]
+    img = np.ascontiguousarray(img, np.float32)
+    if _near_int(-inv_tx) == 0 and _near_int(-inv_ty) == 0:
+        work = img.copy()
+    else:
+        work = translate(img, inv_tx, inv_ty)
+    work = np.roll(work, (-(N // 2), -(N // 2)), axis=(0, 1))
+    F = _fft_f32(work)
+    scale = np.sqrt(np.float32(1.0) / np.float32(N) * np.float32(N + 2)).astype(np.float32)
+    out = np.empty((N, N + 2), np.float32)
+    out[:, 0::2] = F.real * scale
+    out[:, 1::2] = F.imag * scale
+    return out
+
+
+def particle_to_slice(raw: np.ndarray, N: int, shift=(0.0, 0.0), ctf: dict | None = None):
+    """The reference caller's per-particle pipeline (programs/e2spa_make3d.py:300-342):
+    edge-mean subtract, clip to N, optional CTF phase flip, edge-mean subtract,
+    then preprocess_slice with the inverted translation of xform.projection."""
+    img = np.asarray(raw, np.float32)
+    img = img - edge_mean(img)
+    img = clip_pad(img, N)
+    if ctf is not None and abs(ctf.get("defocus", 0.0)) > 1e-4:
+        img = ctf_flip(img, ctf)
+    img = img - edge_mean(img)
+    return preprocess_slice(img, float(np.float32(shift[0])), float(np.float32(shift[1])))
+
+
+# ------------------------------------------------------------------- metrics
+
+def fsc(a: np.ndarray, b: np.ndarray) -> np.ndarray:
+    """Fourier shell correlation of two complex half volumes (N, N, N+2)
+    following EMData::calc_fourier_shell_correlation
+    (libEM/sparx/emdata_sparx.cpp:867-990) with ring width 1."""
+    N = a.shape[0]
+    ca = a.astype(np.float64).view(np.complex128)
+    cb = b.astype(np.float64).view(np.complex128)
+    k = np.fft.fftfreq(N, 1.0 / N)
+    kz, ky, kx = np.meshgrid(k, k, np.arange(N // 2 + 1), indexing="ij")
+    r = np.floor(np.sqrt(kx ** 2 + ky ** 2 + kz ** 2) + 0.5).astype(int)
+    keep = (kx > 0) | ((kz >= 0) & ((ky >= 0) | (kz != 0)))
+    keep &= r <= N // 2
+    rr = r[keep]
+    num = np.bincount(rr, (ca[keep] * np.conj(cb[keep])).real, N // 2 + 1)
+    n1 = np.bincount(rr, np.abs(ca[keep]) ** 2, N // 2 + 1)
+    n2 = np.bincount(rr, np.abs(cb[keep]) ** 2, N // 2 + 1)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        out = num / np.sqrt(n1 * n2)
+    out[(n1 <= 0) | (n2 <= 0)] = 1.0
+    return out
+
+
+def rel_l2(a: np.ndarray, b: np.ndarray) -> float:
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    d = np.linalg.norm((a - b).ravel())
+    n = np.linalg.norm(b.ravel())
+    return float(d / n) if n > 0 else float(d)

@@ -1,0 +1,220 @@
+"""GPU parity: libeman2_b200 against the CPU oracle on identical seeded inputs.
+
+Tolerances: the GPU reproduces every tap selection and exp-table index of the
+reference bit for bit; only the order of FP32 additions differs (atomics in
+the scatter schedule, FP64 partial sums in the gather schedule), so the
+accumulators agree with the FP32-faithful oracle to a relative L2 of
+RTOL_ACC = 2e-6 and to the FP64 oracle likewise.  Anything that moves a
+window or a table index shows up as an error of order 1e-3 or more.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from oracle import oracle
+
+pytestmark = pytest.mark.gpu
+
+RTOL_ACC = 2e-6      # accumulators, FP32 summation-order noise only
+RTOL_FFT = 2e-5      # paths through cuFFT vs pocketfft (float64 rounded to float32)
+# versus the FP64 oracle: within 3x the FP32-faithful oracle's own distance
+
+
+def rand_slices(N, n, seed):
+    rng = np.random.default_rng(seed)
+    return rng.normal(size=(n, N, N + 2)).astype(np.float32)
+
+
+def rand_rots(n, seed):
+    from eman2_b200.synth import quaternion_blocks, random_quaternions
+    return quaternion_blocks(random_quaternions(n, np.random.default_rng(seed)))
+
+
+def recon(N, mode="gauss_2", sym="c1", **kw):
+    from eman2_b200 import Reconstructors
+    p = {"size": [N, N, N], "sym": sym, "mode": mode}
+    p.update(kw)
+    r = Reconstructors.get("fourier", p)
+    r.setup()
+    return r
+
+
+def oracle_insert(N, slices, rots, weights, mode, sym, prec="fp32", corners=False):
+    v = oracle.OracleVolume(N, prec)
+    v.insert(slices, rots, weights, mode, sym, corners=corners)
+    return v
+
+
+def rel(a, b):
+    return oracle.rel_l2(a, b)
+
+
+@pytest.mark.parametrize("sched", ["scatter", "gather"])
+@pytest.mark.parametrize("mode", ["nearest_neighbor", "gauss_2", "gauss_5", "trilinear"])
+@pytest.mark.parametrize("N,sym", [(16, "c1"), (22, "d2"), (32, "c3")])
+def test_insert_schedules_match_oracle(gpu, sched, mode, N, sym):
+    n = 24
+    sl, rt = rand_slices(N, n, N), rand_rots(n, N + 1)
+    w = np.random.default_rng(N + 2).uniform(0.5, 1.0, n).astype(np.float32)
+    r = recon(N, mode, sym)
+    st = r.insert_slices(sl, rt, w, schedule=sched)
+    assert st == [0] * n
+    d, nm = r.get_accumulators()
+    o = oracle_insert(N, sl, rt, w, mode, sym)
+    assert rel(nm, o.norm) < RTOL_ACC
+    assert rel(d, o.data) < RTOL_ACC
+    # same support: no tap went missing or appeared
+    assert np.array_equal(nm != 0, o.norm != 0)
+    # Against the FP64 oracle the distance is the FP32 path's own rounding
+    # (coordinates, weights, a rare exp-table index): the GPU sits as close to
+    # it as the FP32-faithful oracle does.
+    o64 = oracle_insert(N, sl, rt, w, mode, sym, "fp64")
+    assert rel(d, o64.data) < 3 * rel(o.data, o64.data) + 1e-6
+
+
+def test_plain_insert_slice_path(gpu):
+    """One insert_slice call per particle (the plain per-call path)."""
+    from eman2_b200 import EMData, Transform
+    N, n = 24, 12
+    sl, rt = rand_slices(N, n, 5), rand_rots(n, 6)
+    r = recon(N, "gauss_2", "c1")
+    for i in range(n):
+        img = EMData(sl[i], is_complex=True, attrs={"reconstruct_preproc": 1})
+        assert r.insert_slice(img, Transform(rt[i]), 0.75) == 0
+    assert r.insert_slice(EMData(sl[0], is_complex=True, attrs={"reconstruct_preproc": 1}),
+                          Transform(rt[0]), 0.0) == -1
+    d, nm = r.get_accumulators()
+    o = oracle_insert(N, sl, rt, np.full(n, 0.75, np.float32), "gauss_2", "c1")
+    assert rel(d, o.data) < RTOL_ACC and rel(nm, o.norm) < RTOL_ACC
+
+
+def interior(N):
+    """Cells with |x|,|y|,|z| < N/2 (the gather kernel's own cells): every
+    cell except the x=N/2 column and the y=-N/2 row and z=-N/2 slab."""
+    m = np.ones((N, N, N // 2 + 1), bool)
+    m[:, :, N // 2] = False
+    m[:, N // 2, :] = False
+    m[N // 2, :, :] = False
+    return m
+
+
+def test_gather_is_deterministic_and_matches_scatter(gpu):
+    """The gather schedule owns every interior cell: bitwise reproducible
+    there.  Cube-face cells come from the atomic face-tap kernel."""
+    N, n = 48, 64
+    sl, rt = rand_slices(N, n, 11), rand_rots(n, 12)
+    w = np.ones(n, np.float32)
+    outs = []
+    for sched in ("gather", "gather", "scatter"):
+        r = recon(N, "gauss_5", "d3")
+        r.insert_slices(sl, rt, w, schedule=sched)
+        outs.append(r.get_accumulators())
+    m = interior(N)
+    c0 = outs[0][0].view(np.complex64)
+    c1 = outs[1][0].view(np.complex64)
+    assert np.array_equal(c0[m], c1[m]) and np.array_equal(outs[0][1][m], outs[1][1][m])
+    assert rel(outs[0][0], outs[1][0]) < RTOL_ACC
+    assert rel(outs[0][0], outs[2][0]) < RTOL_ACC
+
+
+def test_zero_negative_weights_and_removal(gpu):
+    """weight 0 inserts nothing (-1); inserting with -w removes to ~0 (the
+    intent of rt/pyem/test_reconstructor.py:48-90)."""
+    N, n = 20, 10
+    sl, rt = rand_slices(N, n, 21), rand_rots(n, 22)
+    w = np.ones(n, np.float32)
+    w[3] = 0.0
+    r = recon(N, "gauss_2", "c1")
+    st = r.insert_slices(sl, rt, w, schedule="scatter")
+    assert st[3] == -1 and st.count(-1) == 1
+    r.insert_slices(sl, rt, -w, schedule="scatter")
+    d, nm = r.get_accumulators()
+    assert np.abs(d).max() < 1e-4 and np.abs(nm).max() < 1e-5
+
+
+def test_corners_mode(gpu):
+    N, n = 16, 8
+    sl, rt = rand_slices(N, n, 31), rand_rots(n, 32)
+    w = np.ones(n, np.float32)
+    for sched in ("scatter", "gather"):
+        r = recon(N, "gauss_2", "c1", corners=True)
+        r.insert_slices(sl, rt, w, schedule=sched)
+        d, nm = r.get_accumulators()
+        o = oracle_insert(N, sl, rt, w, "gauss_2", "c1", corners=True)
+        assert rel(d, o.data) < RTOL_ACC and rel(nm, o.norm) < RTOL_ACC
+
+
+def test_preprocess_matches_oracle(gpu):
+    from eman2_b200 import EMData, Transform
+    N = 32
+    rng = np.random.default_rng(41)
+    r = recon(N)
+    for t in [(0.0, 0.0), (1.25, -2.5), (3.0, 0.75)]:
+        img = rng.normal(size=(N, N)).astype(np.float32)
+        xf = Transform({"type": "eman", "az": 10.0, "alt": 20.0, "phi": 30.0, "tx": t[0], "ty": t[1]})
+        got = r.preprocess_slice(EMData(img), xf).numpy()
+        want = oracle.preprocess_slice(img, -t[0], -t[1])
+        assert rel(got, want) < RTOL_FFT
+
+
+def test_particle_pipeline_matches_oracle(gpu):
+    """fr_insert_particles (edge mean, pad, CTF flip, shift, r2c, insert) vs
+    the oracle's restatement of the caller loop."""
+    from eman2_b200.particles import particle_meta
+    from eman2_b200.synth import make_particles
+    box, N, n = 32, 48, 24
+    ps = make_particles(box, n, seed=51, snr=0.5, shift=3.0, weights=(0.5, 1.0), ctf=True)
+    r = recon(N, "gauss_2", "c1")
+    r.insert_particles(ps.images, particle_meta(ps.rots, ps.shifts, ps.weights, defocus=ps.defocus))
+    d, nm = r.get_accumulators()
+    slices = np.stack([oracle.particle_to_slice(ps.images[i], N, ps.shifts[i],
+                                                {"defocus": float(ps.defocus[i])})
+                       for i in range(n)])
+    o = oracle_insert(N, slices, ps.rots, ps.weights, "gauss_2", "c1")
+    assert rel(nm, o.norm) < RTOL_ACC
+    assert rel(d, o.data) < RTOL_FFT
+
+
+def test_finish_matches_oracle(gpu):
+    N, n = 32, 40
+    sl, rt = rand_slices(N, n, 61), rand_rots(n, 62)
+    w = np.ones(n, np.float32)
+    for doift in (False, True):
+        r = recon(N, "gauss_2", "c1")
+        r.insert_slices(sl, rt, w)
+        out = r.finish(doift).numpy()
+        o = oracle_insert(N, sl, rt, w, "gauss_2", "c1")
+        want, _ = o.finish(doift)
+        assert rel(out, want) < (RTOL_FFT if doift else RTOL_ACC)
+
+
+def test_agreement_matches_oracle(gpu):
+    N, n = 32, 30
+    sl, rt = rand_slices(N, n, 71), rand_rots(n, 72)
+    w = np.ones(n, np.float32)
+    r = recon(N, "gauss_2", "d2")
+    r.insert_slices(sl, rt, w)
+    got = r.slice_agreement(sl[:5], rt[:5], w[:5], apix=1.0)
+    o = oracle_insert(N, sl, rt, w, "gauss_2", "d2")
+    for i in range(5):
+        want = o.compare(sl[i], rt[i], 1.0, "d2", 1.0)
+        np.testing.assert_allclose(got[i], want, rtol=1e-5, atol=1e-6)
+
+
+def test_seed_setup_matches_reference_rule(gpu):
+    """setup_seed: data = seed*w; weights w, halved on x=0 and x=N/2 planes
+    except four cells (libEM/reconstructor.cpp:865-895)."""
+    from eman2_b200 import Reconstructors
+    N = 16
+    seed = np.random.default_rng(81).normal(size=(N, N, N + 2)).astype(np.float32)
+    r = Reconstructors.get("fourier", {"size": [N] * 3, "sym": "c1"})
+    r.setup_seed(seed, 2.5)
+    d, nm = r.get_accumulators()
+    assert np.array_equal(d, seed * np.float32(2.5))
+    want = np.full((N, N, N // 2 + 1), 2.5, np.float32)
+    want[:, :, 0] = want[:, :, -1] = 1.25
+    for x in (0, N // 2):
+        want[0, N // 2, x] = 2.5
+        want[N // 2, 0, x] = 2.5
+    assert np.array_equal(nm, want)
