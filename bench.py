@@ -315,8 +315,10 @@ def main():
     e2e = ws * args.steps * args.batch / (e2e_ms / 1e3)
     V = (N // 2 + 1) * N * N
     alg_bytes = args.batch * (8 * (N // 2 + 1) * N + 64) + 24 * V
-    glaunch = max(1, st["gather_launches"])
-    gms = st["gather_ms"] / glaunch
+    if st["gather_launches"] > 0:
+        kname, gms = "k_column (gather schedule)", st["gather_ms"] / st["gather_launches"]
+    else:
+        kname, gms = "k_scatter", st["insert_ms"] / max(1, st["insert_launches"])
     achieved = alg_bytes / (gms / 1e3) / 1e9
     peak, peak_kind = load_peaks()
     traffic = load_traffic(args.workload, args.batch)
@@ -334,7 +336,7 @@ def main():
         "gpu_launches": int(st["kernel_launches"]),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
-                     "kernel": "k_gather",
+                     "kernel": kname,
                      "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": gms},
         "taps": {"per_particle_upper": taps_per,
                  "per_s_upper": taps_per * args.batch / (gms / 1e3)},

@@ -305,24 +305,53 @@ int insert_device(fr_recon *r, const float2 *d_slices, const float *d_t3d, const
   }
   int tile = r->tile >= 0 ? r->tile : (tuned >= 0 ? tuned : default_tile(r->mode, r->N, r->nsym, np));
   if (r->tiles_tile != tile) {
-    gather_tiles(r->N, r->mode, tile, r->p.corners, r->tiles, r->tx, r->ty, r->tz);
+    if (tile == kColumnTile)
+      column_tiles(r->N, r->mode, r->p.corners, r->tiles, r->tx, r->ty, r->tz, &r->tile_dist);
+    else gather_tiles(r->N, r->mode, tile, r->p.corners, r->tiles, r->tx, r->ty, r->tz);
     r->tiles_tile = tile;
+    r->work_np = -1;
+  }
+  j.tiles_x = r->tx;
+  j.tiles_y = r->ty;
+  j.tiles_z = r->tz;
+  const int nsl = np * r->nsym;
+  int nwork = 0;
+  if (tile == kColumnTile) {
+    // work items (job 0, tile, first slice of the block)
+    if (r->work_np != nsl) {
+      std::vector<int4> work;
+      for (size_t ti = 0; ti < r->tiles.size(); ti++) {
+        const int blk = column_block(r->tile_dist[ti]);
+        for (int s0 = 0; s0 < nsl; s0 += blk)
+          work.push_back(make_int4(0, r->tiles[ti], s0, std::min(nsl, s0 + blk)));
+      }
+      TRY(r->s_work.ensure(sizeof(int4) * std::max<size_t>(1, work.size())));
+      CU(cudaMemcpyAsync(r->s_work.p, work.data(), sizeof(int4) * work.size(),
+                         cudaMemcpyHostToDevice, st));
+      CU(cudaStreamSynchronize(st));
+      r->work_np = nsl;
+      r->nwork = (int)work.size();
+    }
+    nwork = r->nwork;
+  } else if (r->work_np != -2) {
     std::vector<int2> work(r->tiles.size());
     for (size_t i = 0; i < work.size(); i++) work[i] = make_int2(0, r->tiles[i]);
     TRY(r->s_work.ensure(sizeof(int2) * std::max<size_t>(1, work.size())));
     CU(cudaMemcpyAsync(r->s_work.p, work.data(), sizeof(int2) * work.size(),
                        cudaMemcpyHostToDevice, st));
     CU(cudaStreamSynchronize(st));
+    r->work_np = -2;
   }
-  j.tiles_x = r->tx;
-  j.tiles_y = r->ty;
-  j.tiles_z = r->tz;
   TRY(r->s_jobs.ensure(sizeof(InsertJob)));
   TRY(r->s_counter.ensure(sizeof(int)));
   CU(cudaMemcpyAsync(r->s_jobs.p, &j, sizeof(InsertJob), cudaMemcpyHostToDevice, st));
   if (prof) CU(cudaEventRecord(ev[0], st));
-  CU(launch_gather(r->s_jobs.as<InsertJob>(), &j, 1, r->s_work.as<int2>(), (int)r->tiles.size(),
-                   tile, r->s_counter.as<int>(), r->mode, st));
+  if (tile == kColumnTile)
+    CU(launch_column(r->s_jobs.as<InsertJob>(), r->s_work.as<int4>(), nwork, kColumnBlock,
+                     r->s_counter.as<int>(), r->mode, st));
+  else
+    CU(launch_gather(r->s_jobs.as<InsertJob>(), &j, 1, r->s_work.as<int2>(), (int)r->tiles.size(),
+                     tile, r->s_counter.as<int>(), r->mode, st));
   if (prof) CU(cudaEventRecord(ev[1], st));
   TRY(run_scatter(j, true, st));
   g_gather_launches++;

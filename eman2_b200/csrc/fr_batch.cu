@@ -3,10 +3,9 @@
 //
 // A batch holds independent FourierReconstructor states (uneven N, modes and
 // symmetries: even/odd half maps, heterogeneity classes).  Each insert call
-// runs every job's prologue on the batch stream, then ONE k_gather launch whose
-// work list interleaves all jobs' voxel tiles (heaviest first), then the small
-// face-tap kernels.  With CUDA graphs enabled the whole device sequence of a
-// call is captured once per shape signature and replayed.
+// runs every job's prologue on the batch stream, then ONE persistent insertion
+// launch (k_column) whose work list interleaves all jobs' (tile, slice block)
+// items, heaviest first, then the small face-tap kernels.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -35,9 +34,8 @@ int tuned_tile(int N, int mode, int nsym) {
 }
 
 int default_tile(int mode, int N, int nsym, int np) {
-  (void)nsym; (void)np;
-  if (mode == FR_MODE_GAUSS5) return 0;   // 8x8x8
-  return N >= 256 ? 1 : 0;                // 16x8x8 for the thin gauss_2 windows at large N
+  (void)nsym; (void)np; (void)N; (void)mode;
+  return kColumnTile;   // the column-owner kernel unless the autotuner measured otherwise
 }
 
 }  // namespace fr
@@ -117,7 +115,8 @@ int fr_batch_insert_particles(fr_batch *b, const float *const *imgs, const int *
   const int chunk = 4096;
   int rounds = 0;
   for (int j = 0; j < nj; j++) rounds = std::max(rounds, (counts[j] + chunk - 1) / chunk);
-  int tile = b->tile >= 0 ? b->tile : 0;
+  const int tile = b->tile >= 0 ? b->tile : kColumnTile;
+  const bool column = tile == kColumnTile;
   for (int rd = 0; rd < rounds; rd++) {
     std::vector<InsertJob> hj;
     std::vector<int> owner;
@@ -134,7 +133,9 @@ int fr_batch_insert_particles(fr_batch *b, const float *const *imgs, const int *
       TRY(prologue_chunk(r, (const float *)d_raw, c, box, meta[j] + p0));
       InsertJob J = make_job(r, r->s_slices.as<float2>(), r->s_t3d.as<float>(), r->s_w.as<float>(), c);
       if (r->tiles_tile != tile) {
-        gather_tiles(r->N, r->mode, tile, r->p.corners, r->tiles, r->tx, r->ty, r->tz);
+        if (column)
+          column_tiles(r->N, r->mode, r->p.corners, r->tiles, r->tx, r->ty, r->tz, &r->tile_dist);
+        else gather_tiles(r->N, r->mode, tile, r->p.corners, r->tiles, r->tx, r->ty, r->tz);
         r->tiles_tile = tile;
       }
       J.tiles_x = r->tx;
@@ -146,34 +147,53 @@ int fr_batch_insert_particles(fr_batch *b, const float *const *imgs, const int *
       else if (max_mode != FR_MODE_GAUSS5 && r->mode != FR_MODE_NEAREST) max_mode = r->mode;
     }
     if (hj.empty()) continue;
-    // Interleave every job's tiles by estimated cost (slices meeting a tile
-    // fall off with its distance from the origin), heaviest first.
-    std::vector<std::pair<double, int2>> items;
+    // Interleave every job's work items by estimated cost, heaviest first: the
+    // slices meeting a tile fall off with its distance from the origin (tiles
+    // are sorted by distance), times the slices in the item's block.
+    std::vector<std::pair<double, int4>> items;
     for (size_t k = 0; k < hj.size(); k++) {
       fr_recon *r = b->jobs[owner[k]];
-      const double nsl = (double)hj[k].np * hj[k].nsym;
+      const int nsl = hj[k].np * hj[k].nsym;
       const double nt = (double)r->tiles.size();
       for (size_t t = 0; t < r->tiles.size(); t++) {
-        const double frac = (double)t / std::max(1.0, nt);   // tiles are sorted by distance
-        const double cost = nsl / (1.0 + 8.0 * std::cbrt(frac) * r->N / 16.0);
-        items.push_back({-cost, make_int2((int)k, r->tiles[t])});
+        const double frac = (double)t / std::max(1.0, nt);
+        const double fall = 1.0 / (1.0 + 8.0 * std::cbrt(frac) * r->N / 16.0);
+        if (column) {
+          const int blk = column_block(r->tile_dist[t]);
+          for (int s0 = 0; s0 < nsl; s0 += blk) {
+            const int len = std::min(blk, nsl - s0);
+            items.push_back({-len * fall, make_int4((int)k, r->tiles[t], s0, s0 + len)});
+          }
+        } else {
+          items.push_back({-nsl * fall, make_int4((int)k, r->tiles[t], 0, 0)});
+        }
       }
     }
     std::stable_sort(items.begin(), items.end(),
-                     [](const std::pair<double, int2> &a, const std::pair<double, int2> &c) {
+                     [](const std::pair<double, int4> &a, const std::pair<double, int4> &c) {
                        return a.first < c.first;
                      });
-    std::vector<int2> work(items.size());
-    for (size_t i = 0; i < items.size(); i++) work[i] = items[i].second;
     TRY(b->d_jobs.ensure(sizeof(InsertJob) * hj.size()));
-    TRY(b->d_work.ensure(sizeof(int2) * work.size()));
     TRY(b->d_counter.ensure(sizeof(int)));
     CU(cudaMemcpyAsync(b->d_jobs.p, hj.data(), sizeof(InsertJob) * hj.size(),
                        cudaMemcpyHostToDevice, st));
-    CU(cudaMemcpyAsync(b->d_work.p, work.data(), sizeof(int2) * work.size(),
-                       cudaMemcpyHostToDevice, st));
-    CU(launch_gather(b->d_jobs.as<InsertJob>(), hj.data(), (int)hj.size(), b->d_work.as<int2>(),
-                     (int)work.size(), tile, b->d_counter.as<int>(), max_mode, st));
+    if (column) {
+      std::vector<int4> work(items.size());
+      for (size_t i = 0; i < items.size(); i++) work[i] = items[i].second;
+      TRY(b->d_work.ensure(sizeof(int4) * work.size()));
+      CU(cudaMemcpyAsync(b->d_work.p, work.data(), sizeof(int4) * work.size(),
+                         cudaMemcpyHostToDevice, st));
+      CU(launch_column(b->d_jobs.as<InsertJob>(), b->d_work.as<int4>(), (int)work.size(),
+                       kColumnBlock, b->d_counter.as<int>(), max_mode, st));
+    } else {
+      std::vector<int2> work(items.size());
+      for (size_t i = 0; i < items.size(); i++) work[i] = make_int2(items[i].second.x, items[i].second.y);
+      TRY(b->d_work.ensure(sizeof(int2) * work.size()));
+      CU(cudaMemcpyAsync(b->d_work.p, work.data(), sizeof(int2) * work.size(),
+                         cudaMemcpyHostToDevice, st));
+      CU(launch_gather(b->d_jobs.as<InsertJob>(), hj.data(), (int)hj.size(), b->d_work.as<int2>(),
+                       (int)work.size(), tile, b->d_counter.as<int>(), max_mode, st));
+    }
     for (const InsertJob &J : hj) TRY(run_scatter(J, true, st));
     CU(cudaStreamSynchronize(st));
   }
@@ -193,7 +213,7 @@ int fr_batch_get_accumulators(fr_batch *b, int job, float *data, float *norm) {
 }
 
 int fr_set_tile(int N, int mode, int nsym, int tile) {
-  if (tile != kTunedScatter && (tile < -1 || tile >= kNumTiles))
+  if (tile != kTunedScatter && (tile < -1 || tile > kColumnTile))
     return fail(FR_EINVAL_PARAM, "tile %d out of range", tile);
   std::lock_guard<std::mutex> lk(g_tune_mu);
   if (tile == -1) g_tuned.erase(std::make_tuple(N, mode, nsym));

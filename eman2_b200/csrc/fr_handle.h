@@ -135,7 +135,9 @@ struct fr_recon {
   fr::PlanCache plans;
   int tile = -1;              // gather tile shape (-1: tuned default)
   std::vector<int> tiles;
+  std::vector<float> tile_dist;   // nearest-cell distance of each tile (column kernel)
   int tiles_tile = -1, tx = 0, ty = 0, tz = 0;
+  int work_np = -1, nwork = 0;   // cached work list signature (slices) and size
   std::mutex mu;
 };
 

@@ -71,6 +71,20 @@ cudaError_t launch_gather(const InsertJob *d_jobs, const InsertJob *h_jobs, int 
                           const int2 *d_work, int nwork, int tile, int *d_counter, int max_mode,
                           cudaStream_t st);
 cudaError_t launch_edge(const InsertJob &j, cudaStream_t st);
+// Column-owner kernel (fr_column.cu): 16^3 tiles, work items (job, tile,
+// first slice, end slice) over slice blocks of at most kColumnBlock.
+constexpr int kColumnTile = kNumTiles;   // tile id selecting the column kernel
+constexpr int kColumnBlock = 1024;       // largest slice block (shared-memory hit list)
+// Slices per work item for a tile whose nearest cell is `dist` voxels from the
+// origin: every slice meets the centre tiles, so their FP32 chains in shared
+// memory are kept short; far tiles meet few slices and take long blocks.
+inline int column_block(double dist) {
+  return dist < 16 ? 64 : dist < 32 ? 128 : dist < 64 ? 256 : kColumnBlock;
+}
+cudaError_t launch_column(const InsertJob *d_jobs, const int4 *d_work, int nwork, int block,
+                          int *d_counter, int max_mode, cudaStream_t st);
+void column_tiles(int N, int mode, int corners, std::vector<int> &out, int &tx, int &ty, int &tz,
+                  std::vector<float> *dist = nullptr);
 // Ordered work list (tile ids of a job that can receive interior taps).
 void gather_tiles(int N, int mode, int tile, int corners, std::vector<int> &out, int &tx, int &ty,
                   int &tz);

@@ -13,11 +13,15 @@
  * the reference's own inserter and Hermitian-add source compiled from where it
  * lies (oracle/build_ref.sh -> oracle/_ref/), see tests/test_oracle_ref.py.
  *
- * One source, two builds:
+ * One source, three builds:
  *   OR_REAL=float  -> the FP32-faithful oracle: the same operation order and
  *                     rounding points as the reference source, evaluated with
  *                     strict IEEE single precision (no contraction, no
  *                     reassociation, divisions as written).
+ *   OR_REAL=float, OR_ACC=double
+ *                  -> FP32 tap arithmetic (identical tap selection, exp-table
+ *                     indices and products) summed in double: isolates the
+ *                     FP32 summation-order noise of any schedule.
  *   OR_REAL=double -> the FP64 oracle: the same algorithm (table exp, the same
  *                     Hermitian bookkeeping) with double coordinates, weights
  *                     and accumulators.
@@ -35,6 +39,10 @@
 #define OR_REAL float
 #endif
 typedef OR_REAL real;
+#ifndef OR_ACC
+#define OR_ACC OR_REAL
+#endif
+typedef OR_ACC acc_t;   /* volume accumulators */
 #define IS_F32 (sizeof(real) == sizeof(float))
 
 #define OR_EXPORT __attribute__((visibility("default")))
@@ -152,8 +160,8 @@ OR_EXPORT void or_compose(const float *a, const float *b, float *out) {
 /* ------------------------------------------------------------- the volume */
 
 typedef struct {
-  real *data;   /* complex volume, [nz][ny][nx] floats, nx = N+2 */
-  real *norm;   /* weights, [nz][ny][nx/2] */
+  acc_t *data;  /* complex volume, [nz][ny][nx] floats, nx = N+2 */
+  acc_t *norm;  /* weights, [nz][ny][nx/2] */
   int nx, ny, nz;
   long nxyz;
 } or_vol;
@@ -163,7 +171,7 @@ typedef struct {
 static inline long or_add_complex_at(or_vol *v, int x, int y, int z, real re, real im) {
   const int nx = v->nx, ny = v->ny, nz = v->nz;
   const long nxy = (long)nx * ny;
-  real *rdata = v->data;
+  acc_t *rdata = v->data;
   if (abs(x) >= nx / 2 || abs(y) > ny / 2 || abs(z) > nz / 2) return v->nxyz;
   long idx;
   if (x == 0) {
@@ -275,7 +283,7 @@ static inline void or_slice_at(const float *s, int nx, int ny, int x, int y, rea
  * blocks t3d[nsym*9] (arg*sym, libEM/transform.cpp:1384).
  * vol_data [N][N][N+2], vol_norm [N][N][N/2+1]; slice [N][N+2] (complex).
  * weight < 0 selects the SSNR path (ssnr table of nssnr entries). */
-OR_EXPORT int or_insert_slice(real *vol_data, real *vol_norm, int N, int mode,
+OR_EXPORT int or_insert_slice(acc_t *vol_data, acc_t *vol_norm, int N, int mode,
                               const float *slice, const float *t3d, int nsym,
                               float weight, int corners, const float *ssnr, int nssnr) {
   or_init_tables();
@@ -341,7 +349,7 @@ OR_EXPORT int or_insert_slice(real *vol_data, real *vol_norm, int N, int mode,
 
 /* Convenience for tests: insert n slices with per-slice orientation blocks
  * arg[n*9] composed with the symmetry operators sym[nsym*9]. */
-OR_EXPORT int or_insert_batch(real *vol_data, real *vol_norm, int N, int mode,
+OR_EXPORT int or_insert_batch(acc_t *vol_data, acc_t *vol_norm, int N, int mode,
                               const float *slices, int n, const float *arg,
                               const float *sym, int nsym, const float *weights, int corners) {
   float *t3d = (float *)malloc(sizeof(float) * 9 * nsym);
@@ -359,7 +367,7 @@ OR_EXPORT int or_insert_batch(real *vol_data, real *vol_norm, int N, int mode,
 
 /* ReconstructorVolumeData::normalize_threed (libEM/reconstructor.cpp:315-390),
  * full-volume case, wiener off. */
-OR_EXPORT void or_normalize(real *rdata, real *norm, int N, int sqrtnorm) {
+OR_EXPORT void or_normalize(acc_t *rdata, acc_t *norm, int N, int sqrtnorm) {
   const int nx = N + 2, ny = N, nz = N;
   const long nnx = nx / 2, nnxy = (long)ny * nnx;
   for (int z = -nz / 2; z < nz / 2; z++) {
@@ -368,7 +376,7 @@ OR_EXPORT void or_normalize(real *rdata, real *norm, int N, int sqrtnorm) {
       long idx1 = (long)(y == 0 ? 0 : ny - y) * nnx + (long)(z <= 0 ? -z : nz - z) * nnxy;
       long idx2 = (long)y * nnx + (long)(z < 0 ? nz + z : z) * nnxy;
       if (idx1 == idx2) continue;
-      real snorm = norm[idx1] + norm[idx2];
+      acc_t snorm = norm[idx1] + norm[idx2];
       norm[idx1] = norm[idx2] = snorm;
       idx1 += nnx - 1;
       idx2 += nnx - 1;
@@ -383,8 +391,8 @@ OR_EXPORT void or_normalize(real *rdata, real *norm, int N, int sqrtnorm) {
   norm[nx / 2 - 1 + (ny / 2) * nnx + 0 * nnxy] *= 2;
   const long total = (long)nx * ny * nz;
   for (long i = 0; i < total; i += 2) {
-    real d = norm[i / 2];
-    if (sqrtnorm) d = IS_F32 ? (real)sqrtf((float)d) : (real)sqrt((double)d);
+    acc_t d = norm[i / 2];
+    if (sqrtnorm) d = (sizeof(acc_t) == sizeof(float)) ? (acc_t)sqrtf((float)d) : (acc_t)sqrt((double)d);
     if (d == 0) { rdata[i] = 0; rdata[i + 1] = 0; }
     else { rdata[i] /= d; rdata[i + 1] /= d; }
   }
@@ -393,7 +401,7 @@ OR_EXPORT void or_normalize(real *rdata, real *norm, int N, int sqrtnorm) {
 /* FourierReconstructor::pixel_at (libEM/reconstructor.cpp:1448-1462) with
  * EMData::get_complex_at(x,y,z) (libEM/emdata_core.cpp:134-145) and
  * get_complex_index_fast (libEM/emdata_core.h:302-308). */
-static inline void or_pixel_at(const real *rdata, const real *norm, int N, real xx, real yy, real zz, real *dt) {
+static inline void or_pixel_at(const acc_t *rdata, const acc_t *norm, int N, real xx, real yy, real zz, real *dt) {
   const int nx = N + 2, ny = N, nz = N;
   const long nxy = (long)nx * ny;
   int x0 = or_round(xx), y0 = or_round(yy), z0 = or_round(zz);
@@ -421,7 +429,7 @@ static inline void or_pixel_at(const real *rdata, const real *norm, int N, real 
  * The loop reads one column past Nyquist (x = N/2+1), i.e. the first element
  * of the next row; on the last row that is past the end of the slice buffer
  * in the reference, and reads 0 here. */
-OR_EXPORT void or_compare_slice(const real *rdata, const real *norm, int N, const float *slice,
+OR_EXPORT void or_compare_slice(const acc_t *rdata, const acc_t *norm, int N, const float *slice,
                                 const float *t3d, int nsym, float weight, float apix, float *out) {
   const int nx = N + 2, ny = N, nz = N;
   const float inx = (float)(N + 2), iny = (float)N;
@@ -549,6 +557,7 @@ OR_EXPORT void or_translate_bilinear(const float *src, float *dst, int nx, int n
 }
 
 OR_EXPORT int or_real_size(void) { return (int)sizeof(real); }
+OR_EXPORT int or_acc_size(void) { return (int)sizeof(acc_t); }
 OR_EXPORT float or_fast_exp_value(float f) { or_init_tables(); return (float)or_fast_exp((real)f); }
 OR_EXPORT int or_hypot_int(int x, int y) { return or_hypot_fast_int(x, y); }
 
@@ -559,7 +568,7 @@ OR_EXPORT int or_hypot_int(int x, int y) { return or_hypot_fast_int(x, y); }
  * plain addition of the un-normalised accumulators, as the reference's own
  * parallel make3d merges per-task volumes (programs/e2spa_make3d.py:175-188).
  * The reference's shared-volume threading races on the += and is not used. */
-OR_EXPORT int or_insert_batch_omp(real *vol_data, real *vol_norm, int N, int mode,
+OR_EXPORT int or_insert_batch_omp(acc_t *vol_data, acc_t *vol_norm, int N, int mode,
                                   const float *slices, int n, const float *arg,
                                   const float *sym, int nsym, const float *weights, int nthreads) {
   if (nthreads < 1) nthreads = omp_get_max_threads();
@@ -570,8 +579,8 @@ OR_EXPORT int or_insert_batch_omp(real *vol_data, real *vol_norm, int N, int mod
 #pragma omp parallel num_threads(nthreads)
   {
     int tid = omp_get_thread_num(), nt = omp_get_num_threads();
-    real *pd = (tid == 0) ? vol_data : (real *)calloc(vd, sizeof(real));
-    real *pn = (tid == 0) ? vol_norm : (real *)calloc(vn, sizeof(real));
+    acc_t *pd = (tid == 0) ? vol_data : (acc_t *)calloc(vd, sizeof(acc_t));
+    acc_t *pn = (tid == 0) ? vol_norm : (acc_t *)calloc(vn, sizeof(acc_t));
     float *t3d = (float *)malloc(sizeof(float) * 9 * nsym);
     if (!pd || !pn || !t3d) {
 #pragma omp atomic write
@@ -601,7 +610,7 @@ OR_EXPORT int or_insert_batch_omp(real *vol_data, real *vol_norm, int N, int mod
 /* Per-pixel entry with the same contract as the reference inserter driver in
  * ref_driver.cpp: n calls of insert_pixel with px[n*6] =
  * (xx, yy, zz, re, im, weight).  Used only to pin this restatement. */
-OR_EXPORT int or_insert_pixels(int mode, real *data, real *norm, int N, const float *px, long n) {
+OR_EXPORT int or_insert_pixels(int mode, acc_t *data, acc_t *norm, int N, const float *px, long n) {
   or_init_tables();
   or_vol v;
   v.data = data; v.norm = norm;

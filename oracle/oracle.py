@@ -5,11 +5,13 @@ imports this module.  It is imported by ``tests/``, by the smoke check in
 ``__graft_entry__.py`` and by the ``cpu_baseline`` / ``--impl reference`` legs
 of ``bench.py``, where it is the checker or the timed CPU baseline.
 
-Two precisions, one restatement (``fr_oracle.c``):
+Three builds of one restatement (``fr_oracle.c``):
 
 * ``fp32`` -- FP32-faithful: the reference's operation order and rounding
   points in strict IEEE single precision.  This is the stand-in for the
   reference's own FourierReconstructor, which cannot be built here.
+* ``fp32acc64`` -- FP32 tap arithmetic (identical taps) with FP64 sums: the
+  yardstick for summation-order noise.
 * ``fp64`` -- the same algorithm in double precision (coordinates, weights,
   accumulators); the FP64 oracle both GPU forms state their error against.
 
@@ -49,12 +51,13 @@ def build(ref: bool = True) -> None:
 def _lib(kind: str = "fp32"):
     if kind in _libs:
         return _libs[kind]
-    name = {"fp32": "liborfp32.so", "fp64": "liborfp64.so", "omp": "liborfp32_omp.so"}[kind]
+    name = {"fp32": "liborfp32.so", "fp64": "liborfp64.so", "omp": "liborfp32_omp.so",
+            "fp32acc64": "liborfp32acc64.so"}[kind]
     path = os.path.join(BUILD, name)
     if not os.path.exists(path):
         build(ref=False)
     lib = ctypes.CDLL(path)
-    R = _F if kind in ("fp32", "omp") else _D
+    R = _F if kind in ("fp32", "omp") else _D   # accumulator pointer type
     lib.or_insert_slice.argtypes = [R, R, ctypes.c_int, ctypes.c_int, _F, _F, ctypes.c_int,
                                     ctypes.c_float, ctypes.c_int, _F, ctypes.c_int]
     lib.or_insert_batch.argtypes = [R, R, ctypes.c_int, ctypes.c_int, _F, ctypes.c_int, _F, _F,
@@ -135,7 +138,7 @@ class OracleVolume:
     def __init__(self, N: int, precision: str = "fp32"):
         self.N = N
         self.kind = precision
-        dt = np.float32 if precision in ("fp32", "omp") else np.float64
+        dt = np.float32 if precision in ("fp32", "omp") else np.float64   # accumulators
         self.data = np.zeros((N, N, N + 2), dt)
         self.norm = np.zeros((N, N, N // 2 + 1), dt)
 
@@ -206,7 +209,7 @@ class OracleVolume:
         N = self.N
         c = self.data.astype(np.float64).view(np.complex128)
         real = np.fft.irfftn(c, s=(N, N, N), axes=(0, 1, 2), norm="forward")
-        if self.kind == "fp64":
+        if self.data.dtype == np.float64:
             real = real * (1.0 / (N * N * N))
         else:
             real = real.astype(np.float32) * np.float32(1.0 / (N * N * N))
