@@ -80,6 +80,8 @@ SIGNATURES = {
     "fr_autotune": ([ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _I, _F],
                     ctypes.c_int),
     "fr_set_tile": ([ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+    "fr_insert_slices_noalloc": ([_P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_char_p,
+                                  _P, _P, _P, _P, _P], ctypes.c_int),
 }
 
 _lib = None

@@ -181,6 +181,25 @@ cudaError_t launch_scatter(const InsertJob &j, cudaStream_t st) {
   return cudaGetLastError();
 }
 
+// The scatter launch with caller-supplied exp table and Gaussian factor
+// (no use of the lazily allocated per-device constants).
+cudaError_t launch_scatter_tables(const InsertJob &j, const float *table, float h,
+                                  cudaStream_t st) {
+  const int nsl = j.np * j.nsym;
+  if (nsl == 0) return cudaSuccess;
+  const int npx = j.N * (j.N / 2 + 1);
+  dim3 grid((npx + 255) / 256, nsl);
+  note_launch();
+  switch (j.mode) {
+    case MODE_NEAREST: k_scatter<MODE_NEAREST><<<grid, 256, 0, st>>>(j, table, h); break;
+    case MODE_GAUSS2: k_scatter<MODE_GAUSS2><<<grid, 256, 0, st>>>(j, table, h); break;
+    case MODE_GAUSS5: k_scatter<MODE_GAUSS5><<<grid, 256, 0, st>>>(j, table, h); break;
+    case MODE_TRILINEAR: k_scatter<MODE_TRILINEAR><<<grid, 256, 0, st>>>(j, table, h); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
 cudaError_t launch_edge(const InsertJob &j, cudaStream_t st) {
   const int nsl = j.np * j.nsym;
   if (nsl == 0 || j.nrim == 0) return cudaSuccess;

@@ -71,6 +71,8 @@ cudaError_t launch_gather(const InsertJob *d_jobs, const InsertJob *h_jobs, int 
                           const int2 *d_work, int nwork, int tile, int *d_counter, int max_mode,
                           cudaStream_t st);
 cudaError_t launch_edge(const InsertJob &j, cudaStream_t st);
+cudaError_t launch_scatter_tables(const InsertJob &j, const float *table, float h,
+                                  cudaStream_t st);
 // Column-owner kernel (fr_column.cu): 16^3 tiles, work items (job, tile,
 // first slice, end slice) over slice blocks of at most kColumnBlock.
 constexpr int kColumnTile = kNumTiles;   // tile id selecting the column kernel

@@ -182,6 +182,26 @@ FR_API int fr_profile(int on);
 FR_API int fr_stats_get(fr_stats *out);
 FR_API int fr_stats_reset(void);
 
+/* Insertion that allocates no device memory, for callers that cannot let a
+ * library call cudaMalloc: processes that reserve all of their HBM for their
+ * own pool allocator, or paths where an allocation's stall or implicit device
+ * synchronisation is not acceptable.  No counterpart in the reference.
+ * The caller passes device buffers: n preprocessed slices float[N][N+2],
+ * rotation blocks rot[9*n], weights[n], and the accumulators it owns,
+ * data float[N][N][N+2] and norm float[N][N][N/2+1], to which the slices'
+ * taps are added (atomic scatter, same arithmetic as fr_insert_slices).
+ * Scratch (tables, symmetry operators, composed rotations) lives in a static
+ * __device__ array of 596 KiB (152,696 floats) inside the library, held by
+ * every GPU that loads it until exit.  Limits: even N <= 1024, at most 240 symmetry operators and
+ * n * nsym <= 16384 per call; larger requests fail with FR_EINVAL_PARAM.
+ * The first call on a device looks up the array's address (with that device
+ * current) and uploads the exp table: make that first call before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU race. */
+FR_API int fr_insert_slices_noalloc(const float *d_slices, int n, int N, int mode,
+                                    const char *sym, const float *d_rot,
+                                    const float *d_weights, float *d_data, float *d_norm,
+                                    void *stream);
+
 /* Last error message of the calling thread. */
 FR_API const char *fr_last_error(void);
 
