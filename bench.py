@@ -107,31 +107,18 @@ class ClockSampler:
 
 # ------------------------------------------------------------------ helpers
 def dist_setup():
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if ws > 1:
-        import datetime
-
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    return ws, rank, local
+    from eman2_b200 import replicas
+    return replicas.init("nccl")
 
 
 def barrier(ws):
-    if ws > 1:
-        import torch.distributed as dist
-        dist.barrier()
+    from eman2_b200 import replicas
+    replicas.barrier(ws)
 
 
 def max_over_ranks(v: float, ws: int) -> float:
-    if ws == 1:
-        return v
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([v], device="cuda", dtype=torch.float64)
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    from eman2_b200 import replicas
+    return replicas.max_over_ranks(v, ws)
 
 
 def load_peaks():

@@ -76,6 +76,8 @@ SIGNATURES = {
     "fr_batch_insert_particles": ([_P, ctypes.POINTER(_P), _I, _I, ctypes.POINTER(_P)],
                                   ctypes.c_int),
     "fr_batch_finish": ([_P, ctypes.c_int, ctypes.c_int, _P, _P], ctypes.c_int),
+    "fr_insert_particles_multi": ([ctypes.POINTER(_P), ctypes.c_int, ctypes.POINTER(_P), _I, _I,
+                                   ctypes.POINTER(_P), _P], ctypes.c_int),
     "fr_batch_get_accumulators": ([_P, ctypes.c_int, _P, _P], ctypes.c_int),
     "fr_autotune": ([ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _I, _F],
                     ctypes.c_int),

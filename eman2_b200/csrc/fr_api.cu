@@ -687,16 +687,25 @@ int fr_insert_slices(fr_recon *r, const float *slices, int n, const float *rot, 
   const bool wdev = is_device_ptr(weights);
   if (wdev) CU(cudaMemcpy(w.data(), weights, sizeof(float) * n, cudaMemcpyDeviceToHost));
   else memcpy(w.data(), weights, sizeof(float) * n);
-  const bool use_ssnr = r->p.usessnr != 0;
-  if (use_ssnr) {
-    for (int i = 0; i < n; i++) w[i] = (ssnr && nssnr > 0) ? -1.0f : 0.0f;
+  const bool have_ssnr = ssnr && nssnr > 0;
+  if (r->p.usessnr) {
+    for (int i = 0; i < n; i++) w[i] = have_ssnr ? -1.0f : 0.0f;
   }
+  // A negative weight selects the SSNR path (libEM/reconstructor.cpp:1158-1162),
+  // which reads the slice's class_ssnr attribute; without it the reference
+  // throws NotExistingObjectException (libEM/emdata_metadata.cpp:1142).
+  bool any_neg = false;
+  for (int i = 0; i < n; i++) any_neg |= w[i] < 0.0f;
+  if (any_neg && !have_ssnr)
+    return fail(FR_ENOTEXIST, "The requested key does not exist: class_ssnr (a negative weight "
+                "selects the SSNR insertion path)");
   for (int i = 0; i < n; i++)
     if (status_out) status_out[i] = (w[i] == 0.0f) ? -1 : 0;
+  const bool use_ssnr = any_neg;
   const void *d_sl = nullptr, *d_rot = nullptr, *d_ss = nullptr;
   TRY(to_device(slices, sizeof(float) * slice_floats(N) * n, r->s_in, st, &d_sl));
   TRY(to_device(rot, sizeof(float) * 9 * n, r->s_rot, st, &d_rot));
-  if (use_ssnr && ssnr && nssnr > 0)
+  if (use_ssnr)
     TRY(to_device(ssnr, sizeof(float) * (size_t)nssnr * n, r->s_ssnr, st, &d_ss));
   TRY(r->s_w.ensure(sizeof(float) * n));
   CU(cudaMemcpyAsync(r->s_w.p, w.data(), sizeof(float) * n, cudaMemcpyHostToDevice, st));

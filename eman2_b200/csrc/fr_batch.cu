@@ -44,7 +44,6 @@ int default_tile(int mode, int N, int nsym, int np) {
 struct fr_batch {
   std::vector<fr_recon *> jobs;
   cudaStream_t own = nullptr, stream = nullptr;
-  DevBuf d_jobs, d_work, d_counter, d_raw;
   int tile = -1;
   std::mutex mu;
 };
@@ -83,10 +82,6 @@ int fr_batch_destroy(fr_batch *b) {
   if (!b) return FR_OK;
   cudaStreamSynchronize(b->stream);
   for (fr_recon *r : b->jobs) fr_destroy(r);
-  b->d_jobs.release();
-  b->d_work.release();
-  b->d_counter.release();
-  b->d_raw.release();
   if (b->own) cudaStreamDestroy(b->own);
   delete b;
   return FR_OK;
@@ -100,14 +95,31 @@ int fr_batch_set_stream(fr_batch *b, void *stream) {
   return FR_OK;
 }
 
-int fr_batch_insert_particles(fr_batch *b, const float *const *imgs, const int *boxes,
-                              const int *counts, const fr_particle *const *meta) {
-  if (!b || !imgs || !boxes || !counts || !meta) return fail(FR_ENULL, "null argument");
-  std::lock_guard<std::mutex> lk(b->mu);
-  const int nj = (int)b->jobs.size();
-  cudaStream_t st = b->stream;
+}  // extern "C"
+
+namespace fr {
+
+struct BatchScratch {
+  DevBuf d_jobs, d_work, d_counter;
+};
+
+// Inserts, for every job, counts[j] particles through the caller pipeline;
+// all jobs' insertion work goes through one persistent launch per round.
+// Every job runs on `st` for the duration of the call.
+static int batch_insert(std::vector<fr_recon *> &jobs, BatchScratch &bs, int tile_pref,
+                        cudaStream_t st, const float *const *imgs, const int *boxes,
+                        const int *counts, const fr_particle *const *meta) {
+  const int nj = (int)jobs.size();
+  struct StreamSwap {
+    std::vector<fr_recon *> &j;
+    std::vector<cudaStream_t> saved;
+    StreamSwap(std::vector<fr_recon *> &jj, cudaStream_t s) : j(jj) {
+      for (fr_recon *r : j) { saved.push_back(r->stream); r->stream = s; }
+    }
+    ~StreamSwap() { for (size_t i = 0; i < j.size(); i++) j[i]->stream = saved[i]; }
+  } swap(jobs, st);
   for (int j = 0; j < nj; j++) {
-    TRY(check_state(b->jobs[j]));
+    TRY(check_state(jobs[j]));
     if (counts[j] < 0 || (counts[j] > 0 && (boxes[j] <= 0 || !imgs[j] || !meta[j])))
       return fail(FR_EINVAL_PARAM, "job %d: bad particle count, box or buffers", j);
   }
@@ -115,14 +127,14 @@ int fr_batch_insert_particles(fr_batch *b, const float *const *imgs, const int *
   const int chunk = 4096;
   int rounds = 0;
   for (int j = 0; j < nj; j++) rounds = std::max(rounds, (counts[j] + chunk - 1) / chunk);
-  const int tile = b->tile >= 0 ? b->tile : kColumnTile;
+  const int tile = tile_pref >= 0 ? tile_pref : kColumnTile;
   const bool column = tile == kColumnTile;
   for (int rd = 0; rd < rounds; rd++) {
     std::vector<InsertJob> hj;
     std::vector<int> owner;
     int max_mode = FR_MODE_NEAREST;
     for (int j = 0; j < nj; j++) {
-      fr_recon *r = b->jobs[j];
+      fr_recon *r = jobs[j];
       const int p0 = rd * chunk;
       const int c = std::max(0, std::min(chunk, counts[j] - p0));
       if (c == 0) continue;
@@ -152,7 +164,7 @@ int fr_batch_insert_particles(fr_batch *b, const float *const *imgs, const int *
     // are sorted by distance), times the slices in the item's block.
     std::vector<std::pair<double, int4>> items;
     for (size_t k = 0; k < hj.size(); k++) {
-      fr_recon *r = b->jobs[owner[k]];
+      fr_recon *r = jobs[owner[k]];
       const int nsl = hj[k].np * hj[k].nsym;
       const double nt = (double)r->tiles.size();
       for (size_t t = 0; t < r->tiles.size(); t++) {
@@ -173,31 +185,65 @@ int fr_batch_insert_particles(fr_batch *b, const float *const *imgs, const int *
                      [](const std::pair<double, int4> &a, const std::pair<double, int4> &c) {
                        return a.first < c.first;
                      });
-    TRY(b->d_jobs.ensure(sizeof(InsertJob) * hj.size()));
-    TRY(b->d_counter.ensure(sizeof(int)));
-    CU(cudaMemcpyAsync(b->d_jobs.p, hj.data(), sizeof(InsertJob) * hj.size(),
+    TRY(bs.d_jobs.ensure(sizeof(InsertJob) * hj.size()));
+    TRY(bs.d_counter.ensure(sizeof(int)));
+    CU(cudaMemcpyAsync(bs.d_jobs.p, hj.data(), sizeof(InsertJob) * hj.size(),
                        cudaMemcpyHostToDevice, st));
     if (column) {
       std::vector<int4> work(items.size());
       for (size_t i = 0; i < items.size(); i++) work[i] = items[i].second;
-      TRY(b->d_work.ensure(sizeof(int4) * work.size()));
-      CU(cudaMemcpyAsync(b->d_work.p, work.data(), sizeof(int4) * work.size(),
+      TRY(bs.d_work.ensure(sizeof(int4) * work.size()));
+      CU(cudaMemcpyAsync(bs.d_work.p, work.data(), sizeof(int4) * work.size(),
                          cudaMemcpyHostToDevice, st));
-      CU(launch_column(b->d_jobs.as<InsertJob>(), b->d_work.as<int4>(), (int)work.size(),
-                       kColumnBlock, b->d_counter.as<int>(), max_mode, st));
+      CU(launch_column(bs.d_jobs.as<InsertJob>(), bs.d_work.as<int4>(), (int)work.size(),
+                       kColumnBlock, bs.d_counter.as<int>(), max_mode, st));
     } else {
       std::vector<int2> work(items.size());
       for (size_t i = 0; i < items.size(); i++) work[i] = make_int2(items[i].second.x, items[i].second.y);
-      TRY(b->d_work.ensure(sizeof(int2) * work.size()));
-      CU(cudaMemcpyAsync(b->d_work.p, work.data(), sizeof(int2) * work.size(),
+      TRY(bs.d_work.ensure(sizeof(int2) * work.size()));
+      CU(cudaMemcpyAsync(bs.d_work.p, work.data(), sizeof(int2) * work.size(),
                          cudaMemcpyHostToDevice, st));
-      CU(launch_gather(b->d_jobs.as<InsertJob>(), hj.data(), (int)hj.size(), b->d_work.as<int2>(),
-                       (int)work.size(), tile, b->d_counter.as<int>(), max_mode, st));
+      CU(launch_gather(bs.d_jobs.as<InsertJob>(), hj.data(), (int)hj.size(), bs.d_work.as<int2>(),
+                       (int)work.size(), tile, bs.d_counter.as<int>(), max_mode, st));
     }
     for (const InsertJob &J : hj) TRY(run_scatter(J, true, st));
     CU(cudaStreamSynchronize(st));
   }
   return FR_OK;
+}
+
+}  // namespace fr
+
+extern "C" {
+
+int fr_batch_insert_particles(fr_batch *b, const float *const *imgs, const int *boxes,
+                              const int *counts, const fr_particle *const *meta) {
+  if (!b || !imgs || !boxes || !counts || !meta) return fail(FR_ENULL, "null argument");
+  std::lock_guard<std::mutex> lk(b->mu);
+  BatchScratch bs;
+  int rc = batch_insert(b->jobs, bs, b->tile, b->stream, imgs, boxes, counts, meta);
+  bs.d_jobs.release(); bs.d_work.release(); bs.d_counter.release();
+  return rc;
+}
+
+int fr_insert_particles_multi(fr_recon *const *handles, int nh, const float *const *imgs,
+                              const int *boxes, const int *counts,
+                              const fr_particle *const *meta, void *stream) {
+  if (!handles || nh <= 0 || !imgs || !boxes || !counts || !meta)
+    return fail(FR_ENULL, "null argument");
+  std::vector<fr_recon *> jobs(handles, handles + nh);
+  for (fr_recon *r : jobs)
+    if (!r) return fail(FR_ENULL, "null reconstructor handle");
+  // One caller at a time per handle: lock them in address order.
+  std::vector<fr_recon *> order(jobs);
+  std::sort(order.begin(), order.end());
+  order.erase(std::unique(order.begin(), order.end()), order.end());
+  if (order.size() != jobs.size()) return fail(FR_EINVAL_PARAM, "a handle appears twice");
+  std::vector<std::unique_lock<std::mutex>> locks;
+  for (fr_recon *r : order) locks.emplace_back(r->mu);
+  static thread_local BatchScratch bs;
+  cudaStream_t st = stream ? (cudaStream_t)stream : jobs[0]->stream;
+  return batch_insert(jobs, bs, -1, st, imgs, boxes, counts, meta);
 }
 
 int fr_batch_finish(fr_batch *b, int job, int doift, float *out, float *normout) {

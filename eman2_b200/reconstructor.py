@@ -271,10 +271,17 @@ class FourierReconstructor:
             self._require_setup()
         usessnr = bool(self.params.get("usessnr", False))
         ssnr = None
-        if usessnr and isinstance(img, EMData) and img.has_attr("class_ssnr"):
+        if isinstance(img, EMData) and img.has_attr("class_ssnr"):
             ssnr = np.ascontiguousarray(img.get_attr("class_ssnr"), np.float32)
-        if (float(weight) == 0.0 and not usessnr) or (usessnr and ssnr is None):
+        if usessnr:
+            weight = -1.0 if ssnr is not None else 0.0
+        if float(weight) == 0.0:
             return -1
+        if float(weight) < 0.0 and ssnr is None:
+            # the SSNR path reads class_ssnr (libEM/reconstructor.cpp:1160-1162)
+            raise NotExistingObjectException("The requested key does not exist: class_ssnr")
+        if float(weight) > 0.0:
+            ssnr = None
         sl = self._slice_of(img, xform)
         rot = _rot_of(xform)
         w = np.array([weight], np.float32)

@@ -1,0 +1,201 @@
+"""Served form: a request loop that admits reconstruction jobs by HBM
+footprint, keeps their accumulating volumes resident on the device across
+insertion ticks, and batches the chunks of every active job into one
+persistent insertion launch per tick (continuous batching: a request that
+arrives while others are on the GPU joins at the next tick once a slot and
+its memory are free).
+
+The scheduler is plain Python (testable without a GPU through any executor
+with the same three methods); ``GpuExecutor`` runs it on the device.
+"""
+from __future__ import annotations
+
+import math
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+
+@dataclass
+class Request:
+    """A reconstruction request: parameters plus particle chunks."""
+    rid: int
+    params: dict                   # {"size": [N]*3, "sym": ..., "mode": ...}
+    chunks: list                   # [(images (n, box, box), meta fr_particle array), ...]
+    arrival: float = 0.0           # seconds, on the server clock
+    particles: int = 0
+
+    def __post_init__(self):
+        if not self.particles:
+            self.particles = sum(int(np.shape(c[0])[0]) for c in self.chunks)
+
+
+@dataclass
+class Job:
+    req: Request
+    handle: object = None
+    next_chunk: int = 0
+    admitted: float = 0.0
+    done: float = 0.0
+    footprint: int = 0
+    result: object = None
+
+    @property
+    def finished_inserting(self) -> bool:
+        return self.next_chunk >= len(self.req.chunks)
+
+
+def footprint_bytes(params: dict, box: int, chunk: int) -> int:
+    """Device bytes a job holds: the (complex, weight) accumulators
+    (12*(N/2+1)*N^2 bytes, as libEM/reconstructor.cpp:782,800 allocate) plus
+    the per-chunk prologue and slice scratch (~5 N^2 floats per particle and
+    the raw images)."""
+    N = int(params["size"][0]) if not np.isscalar(params["size"]) else int(params["size"])
+    vol = 4 * (N * N * (N + 2) + N * N * (N // 2 + 1))
+    return vol + chunk * (20 * N * N + 4 * box * box)
+
+
+class Scheduler:
+    """FIFO admission by HBM footprint and slot count; one chunk per active job
+    per tick."""
+
+    def __init__(self, hbm_budget: int, max_active: int = 16, chunks_per_tick: int = 1):
+        self.budget = int(hbm_budget)
+        self.max_active = max_active
+        self.chunks_per_tick = chunks_per_tick
+        self.waiting: list[Request] = []
+        self.active: list[Job] = []
+        self.done: list[Job] = []
+        self.used = 0
+        self.rejected: list[Request] = []
+
+    def submit(self, req: Request):
+        self.waiting.append(req)
+
+    def _need(self, req: Request) -> int:
+        box = int(np.shape(req.chunks[0][0])[-1]) if req.chunks else 0
+        chunk = max((int(np.shape(c[0])[0]) for c in req.chunks), default=0)
+        return footprint_bytes(req.params, box, chunk)
+
+    def admit(self, now: float, executor) -> list[Job]:
+        out = []
+        while self.waiting and self.waiting[0].arrival <= now and len(self.active) < self.max_active:
+            req = self.waiting[0]
+            need = self._need(req)
+            if need > self.budget:          # can never fit: refuse instead of blocking the queue
+                self.rejected.append(self.waiting.pop(0))
+                continue
+            if self.used + need > self.budget:
+                break                       # wait for memory to free up
+            self.waiting.pop(0)
+            job = Job(req, footprint=need, admitted=now)
+            job.handle = executor.create(req.params)
+            self.used += need
+            self.active.append(job)
+            out.append(job)
+        return out
+
+    def tick_work(self) -> list[tuple[Job, object]]:
+        """The chunks of this tick: up to chunks_per_tick from every active job."""
+        work = []
+        for job in self.active:
+            for _ in range(self.chunks_per_tick):
+                if job.finished_inserting:
+                    break
+                work.append((job, job.req.chunks[job.next_chunk]))
+                job.next_chunk += 1
+        return work
+
+    def retire(self, now: float, executor) -> list[Job]:
+        out = []
+        for job in list(self.active):
+            if job.finished_inserting:
+                job.result = executor.finish(job.handle)
+                job.done = now
+                self.active.remove(job)
+                self.used -= job.footprint
+                self.done.append(job)
+                out.append(job)
+        return out
+
+    def idle(self) -> bool:
+        return not self.waiting and not self.active
+
+
+def percentile(v, q):
+    if not v:
+        return None
+    return float(np.percentile(np.asarray(v, np.float64), q))
+
+
+class Server:
+    """Runs a scheduler against an executor on a wall clock.  Requests with
+    arrival times in the future are held until their time comes."""
+
+    def __init__(self, scheduler: Scheduler, executor, clock=time.perf_counter):
+        self.sched = scheduler
+        self.exe = executor
+        self.clock = clock
+
+    def run(self, requests: list[Request], timeout: float = 3600.0) -> dict:
+        for r in sorted(requests, key=lambda r: r.arrival):
+            self.sched.submit(r)
+        t0 = self.clock()
+        ticks = 0
+        while not self.sched.idle():
+            now = self.clock() - t0
+            if now > timeout:
+                raise TimeoutError("server did not drain its queue")
+            self.sched.admit(now, self.exe)
+            work = self.sched.tick_work()
+            if work:
+                self.exe.insert([(job.handle, chunk) for job, chunk in work])
+                ticks += 1
+            self.sched.retire(self.clock() - t0, self.exe)
+            if not work and not self.sched.active and self.sched.waiting:
+                nxt = self.sched.waiting[0].arrival
+                wait = nxt - (self.clock() - t0)
+                if wait > 0:
+                    time.sleep(min(wait, 0.05))
+        wall = self.clock() - t0
+        lat = [j.done - j.req.arrival for j in self.sched.done]
+        parts = sum(j.req.particles for j in self.sched.done)
+        return {"requests": len(self.sched.done), "rejected": len(self.sched.rejected),
+                "ticks": ticks, "wall_s": wall, "p50_s": percentile(lat, 50),
+                "p99_s": percentile(lat, 99), "particles": parts,
+                "particles_per_s": parts / wall if wall > 0 else math.nan}
+
+
+class GpuExecutor:
+    """Device execution for the scheduler: a resident FourierReconstructor per
+    job; each tick's chunks go through one fr_insert_particles_multi call."""
+
+    def __init__(self, doift: bool = False, stream=None):
+        self.doift = doift
+        self.stream = stream
+
+    def create(self, params: dict):
+        from .reconstructor import FourierReconstructor
+        r = FourierReconstructor(params)
+        r.setup()
+        return r
+
+    def insert(self, items):
+        from .batch import insert_particles_multi
+        recons = [h for h, _ in items]
+        # a handle may appear once per call: group repeated jobs into rounds
+        while items:
+            seen, now, later = set(), [], []
+            for h, c in items:
+                (later if id(h) in seen else now).append((h, c))
+                seen.add(id(h))
+            insert_particles_multi([h for h, _ in now], [c[0] for _, c in now],
+                                   [c[1] for _, c in now], self.stream)
+            items = later
+        del recons
+
+    def finish(self, handle):
+        out = handle.finish(self.doift)
+        handle.close()
+        return out

@@ -227,6 +227,14 @@ FR_API int fr_batch_set_stream(fr_batch *b, void *stream);
 FR_API int fr_batch_insert_particles(fr_batch *b, const float *const *imgs, const int *boxes,
                                      const int *counts, const fr_particle *const *meta);
 
+/* The same batched insertion over independent, already set-up handles (each
+ * keeps its resident volume): imgs[j], boxes[j], counts[j], meta[j] go to
+ * handles[j].  One persistent insertion launch per round of chunks; runs on
+ * `stream` (NULL: the first handle's stream).  The serving loop's tick. */
+FR_API int fr_insert_particles_multi(fr_recon *const *handles, int nh, const float *const *imgs,
+                                     const int *boxes, const int *counts,
+                                     const fr_particle *const *meta, void *stream);
+
 /* Finishes job j like fr_finish. */
 FR_API int fr_batch_finish(fr_batch *b, int job, int doift, float *out, float *normout);
 FR_API int fr_batch_get_accumulators(fr_batch *b, int job, float *data, float *norm);

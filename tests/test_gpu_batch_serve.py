@@ -1,0 +1,84 @@
+"""Batched and served forms change execution, not arithmetic: every job's
+volume equals the one the plain per-job path gives it (alone vs in the mix),
+within the FP32 summation-order tolerance."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from oracle import oracle
+
+pytestmark = pytest.mark.gpu
+
+RTOL = 2e-6
+
+
+def _jobs():
+    from eman2_b200.particles import particle_meta
+    from eman2_b200.synth import make_particles
+    specs = [(32, 48, "gauss_2", "c1", 40), (40, 60, "gauss_5", "d2", 25),
+             (32, 48, "gauss_5", "c1", 30), (24, 36, "nearest_neighbor", "c3", 50)]
+    jobs = []
+    for k, (box, N, mode, sym, n) in enumerate(specs):
+        ps = make_particles(box, n, seed=300 + k, snr=0.5, shift=2.0, weights=(0.5, 1.0),
+                            ctf=(k % 2 == 0))
+        meta = particle_meta(ps.rots, ps.shifts, ps.weights, defocus=ps.defocus)
+        jobs.append(({"size": [N] * 3, "sym": sym, "mode": mode}, ps, meta))
+    return jobs
+
+
+def _alone(params, images, meta):
+    from eman2_b200 import FourierReconstructor
+    r = FourierReconstructor(params)
+    r.setup()
+    r.insert_particles(images, meta)
+    return r.get_accumulators()
+
+
+def test_batch_equals_each_job_alone(gpu):
+    from eman2_b200.batch import BatchReconstructor
+    jobs = _jobs()
+    b = BatchReconstructor([p for p, _, _ in jobs])
+    b.insert_particles([ps.images for _, ps, _ in jobs], [m for _, _, m in jobs])
+    for j, (params, ps, meta) in enumerate(jobs):
+        d, n = b.get_accumulators(j)
+        d0, n0 = _alone(params, ps.images, meta)
+        assert oracle.rel_l2(d, d0) < RTOL and oracle.rel_l2(n, n0) < RTOL
+    # one job against the oracle's restatement of the whole caller loop
+    params, ps, meta = jobs[1]
+    N = params["size"][0]
+    sl = np.stack([oracle.particle_to_slice(ps.images[i], N, ps.shifts[i],
+                                            {"defocus": float(ps.defocus[i])})
+                   for i in range(len(ps.images))])
+    o = oracle.OracleVolume(N, "fp32")
+    o.insert(sl, ps.rots, ps.weights, params["mode"], params["sym"])
+    d, n = b.get_accumulators(1)
+    assert oracle.rel_l2(n, o.norm) < RTOL and oracle.rel_l2(d, o.data) < 2e-5
+
+
+def test_served_result_equals_alone(gpu):
+    """Requests arriving at different times, split into chunks, admitted by
+    footprint and batched together: each result equals the job run alone."""
+    from eman2_b200.server import GpuExecutor, Request, Scheduler, Server
+    from eman2_b200.particles import particle_meta
+    jobs = _jobs()
+    reqs = []
+    for k, (params, ps, meta) in enumerate(jobs):
+        n = len(ps.images)
+        cut = list(range(0, n, 12)) + [n]
+        chunks = [(ps.images[a:b], particle_meta(ps.rots[a:b], ps.shifts[a:b], ps.weights[a:b],
+                                                  defocus=ps.defocus[a:b]))
+                  for a, b in zip(cut[:-1], cut[1:])]
+        reqs.append(Request(k, params, chunks, arrival=0.02 * k))
+    sched = Scheduler(hbm_budget=8 << 30, max_active=3)
+    res = Server(sched, GpuExecutor(doift=False)).run(reqs)
+    assert res["requests"] == 4 and res["p99_s"] >= res["p50_s"] > 0
+    by_id = {j.req.rid: j for j in sched.done}
+    for k, (params, ps, meta) in enumerate(jobs):
+        want = _alone(params, ps.images, meta)
+        from eman2_b200 import FourierReconstructor
+        r = FourierReconstructor(params)
+        r.setup_seedandweights(*want)
+        want_final = r.finish(False).numpy()
+        got = by_id[k].result.numpy()
+        assert oracle.rel_l2(got, want_final) < 1e-5

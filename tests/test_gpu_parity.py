@@ -138,9 +138,10 @@ def test_gather_is_deterministic_and_matches_scatter(gpu):
     assert rel(outs[0][0], outs[2][0]) < RTOL_ACC
 
 
-def test_zero_negative_weights_and_removal(gpu):
-    """weight 0 inserts nothing (-1); inserting with -w removes to ~0 (the
-    intent of rt/pyem/test_reconstructor.py:48-90)."""
+def test_zero_and_negative_weights(gpu):
+    """weight 0 inserts nothing (-1); a negative weight selects the SSNR path,
+    which needs class_ssnr (NotExistingObjectException without it)."""
+    from eman2_b200 import EMData, NotExistingObjectException, Transform
     N, n = 20, 10
     sl, rt = rand_slices(N, n, 21), rand_rots(n, 22)
     w = np.ones(n, np.float32)
@@ -148,9 +149,34 @@ def test_zero_negative_weights_and_removal(gpu):
     r = recon(N, "gauss_2", "c1")
     st = r.insert_slices(sl, rt, w, schedule="scatter")
     assert st[3] == -1 and st.count(-1) == 1
-    r.insert_slices(sl, rt, -w, schedule="scatter")
+    img = EMData(sl[0], is_complex=True, attrs={"reconstruct_preproc": 1})
+    with pytest.raises(NotExistingObjectException):
+        r.insert_slice(img, Transform(rt[0]), -1.0)
+
+
+def test_ssnr_weighted_insertion(gpu):
+    """usessnr: per-pixel weights max(0, ssnr[int(r*sscale)]) from class_ssnr
+    (libEM/reconstructor.cpp:1158-1184), against the oracle fed the same
+    per-pixel weights through its inserter."""
+    from eman2_b200 import EMData, Transform
+    N = 16
+    sl, rt = rand_slices(N, 1, 23), rand_rots(1, 24)
+    ssnr = np.linspace(2.0, -0.5, 12).astype(np.float32)
+    r = recon(N, "gauss_2", "c1", usessnr=True)
+    img = EMData(sl[0], is_complex=True, attrs={"reconstruct_preproc": 1, "class_ssnr": ssnr})
+    assert r.insert_slice(img, Transform(rt[0]), 1.0) == 0
     d, nm = r.get_accumulators()
-    assert np.abs(d).max() < 1e-4 and np.abs(nm).max() < 1e-5
+    # oracle: the same loop with the SSNR weight per pixel
+    import ctypes
+    v = oracle.OracleVolume(N, "fp32")
+    lib = v.lib
+    F = ctypes.POINTER(ctypes.c_float)
+    rc = lib.or_insert_slice(v.data.ctypes.data_as(F), v.norm.ctypes.data_as(F), N, 2,
+                             np.ascontiguousarray(sl[0]).ctypes.data_as(F),
+                             np.ascontiguousarray(rt[0]).ctypes.data_as(F), 1, -1.0, 0,
+                             ssnr.ctypes.data_as(F), ssnr.size)
+    assert rc == 0
+    assert rel(d, v.data) < RTOL_ACC and rel(nm, v.norm) < RTOL_ACC
 
 
 def test_corners_mode(gpu):

@@ -1,0 +1,185 @@
+"""Host-side logic without a GPU: the C ABI loads and exports every declared
+entry point, parameter validation and exception mapping, Transform and
+symmetry conventions against the oracle, particle metadata layout, the
+serving scheduler (fake executor) and the bench's pixel counts."""
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from oracle import oracle
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from eman2_b200 import _lib
+    from eman2_b200 import build as b
+    b.build()
+    return _lib.load()
+
+
+def declared_symbols():
+    src = open(os.path.join(ROOT, "include", "eman2_b200.h")).read()
+    return sorted(set(re.findall(r"FR_API\s+[\w\s\*]*?\b(fr_\w+)\s*\(", src)))
+
+
+def test_library_exports_every_declared_symbol(lib):
+    names = declared_symbols()
+    assert len(names) >= 30
+    for n in names:
+        assert hasattr(lib, n), n
+    from eman2_b200 import _lib
+    assert set(names) <= set(_lib.SIGNATURES), set(names) - set(_lib.SIGNATURES)
+
+
+def test_abi_errors_without_touching_the_device(lib):
+    from eman2_b200 import _lib
+    h = ctypes.c_void_p()
+    assert lib.fr_create(None, ctypes.byref(h)) == 3          # FR_ENULL
+    p = _lib.fr_params()
+    p.nx = p.ny = p.nz = 33
+    p.mode = 2
+    p.sym = b"c1"
+    assert lib.fr_create(ctypes.byref(p), ctypes.byref(h)) == 7   # odd size unsupported
+    assert b"odd" in lib.fr_last_error()
+    p.nx = p.ny = p.nz = 32
+    p.mode = 3
+    assert lib.fr_create(ctypes.byref(p), ctypes.byref(h)) == 7   # gauss_3 not built
+    p.mode = 2
+    p.sym = b"icos"
+    assert lib.fr_create(ctypes.byref(p), ctypes.byref(h)) == 7
+    assert lib.fr_version().startswith(b"eman2_b200")
+
+
+@pytest.mark.parametrize("sym", ["c1", "c4", "c7", "d1", "d2", "d7", "D3", "C2"])
+def test_library_symmetry_matches_oracle(lib, sym):
+    out = np.zeros(9 * 64, np.float32)
+    n = lib.fr_sym_ops(sym.encode(), out.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), 64)
+    want = oracle.sym_ops(sym)
+    assert n == len(want)
+    assert np.array_equal(out[: 9 * n].reshape(n, 3, 3), want)
+
+
+def test_params_and_exceptions():
+    from eman2_b200 import (InvalidParameterException, NotExistingObjectException,
+                            Reconstructors, UnsupportedParameterException)
+    assert Reconstructors.get_list() == ["fourier"]
+    with pytest.raises(NotExistingObjectException):
+        Reconstructors.get("wiener_fourier")
+    with pytest.raises(InvalidParameterException):
+        Reconstructors.get("fourier", {"size": [32] * 3, "bogus": 1})
+    r = Reconstructors.get("fourier", {"size": [32] * 3, "sym": "d7"})
+    # the reference's TypeDict keys (libEM/reconstructor.h:501-516)
+    assert sorted(r.get_param_types()) == sorted(
+        ["size", "sym", "mode", "corners", "sqrtnorm", "usessnr", "verbose", "quiet",
+         "subvolume", "savenorm", "normout"])
+    assert r.get_name() == "fourier" and "direct Fourier" in r.get_desc()
+    r.insert_params({"mode": "gauss_5"})
+    assert r.get_params()["sym"] == "d7" and r.get_params()["mode"] == "gauss_5"
+    r.set_params({"size": [16] * 3})
+    assert "sym" not in r.get_params()
+    r.set_params({"size": [16] * 3, "mode": "gauss_3"})
+    with pytest.raises(UnsupportedParameterException):
+        r.setup()
+
+
+def test_transform_conventions_match_oracle():
+    from eman2_b200 import Transform
+    rng = np.random.default_rng(1)
+    for _ in range(20):
+        az, alt, phi = rng.uniform(-360, 360, 3)
+        t = Transform({"type": "eman", "az": az, "alt": alt, "phi": phi})
+        assert np.array_equal(t.rotation_block(), oracle.eman_matrix(az, alt, phi))
+        q = rng.normal(size=4)
+        q /= np.linalg.norm(q)
+        tq = Transform({"type": "quaternion", "e0": q[0], "e1": q[1], "e2": q[2], "e3": q[3]})
+        assert np.array_equal(tq.rotation_block(), oracle.quaternion_matrix(q))
+        # product in float, the reference's order
+        assert np.array_equal((t * tq).rotation_block(),
+                              oracle.compose(t.rotation_block(), tq.rotation_block()))
+    tr = Transform({"type": "eman", "az": 10, "alt": 20, "phi": 30, "tx": 1.5, "ty": -2.25})
+    inv = tr.inverse()
+    assert np.allclose((tr * inv).matrix, np.eye(3, 4), atol=1e-6)
+    e = Transform({"type": "eman", "az": 10, "alt": 20, "phi": 30}).get_rotation("eman")
+    assert np.allclose([e["az"], e["alt"], e["phi"]], [10, 20, 30], atol=1e-4)
+
+
+def test_synth_quaternion_blocks_match_oracle():
+    from eman2_b200.synth import quaternion_blocks, random_quaternions
+    q = random_quaternions(10, np.random.default_rng(4))
+    m = quaternion_blocks(q)
+    for i in range(10):
+        assert np.array_equal(m[i], oracle.quaternion_matrix(q[i]))
+
+
+def test_particle_meta_layout():
+    from eman2_b200 import _lib
+    from eman2_b200.particles import particle_meta
+    assert ctypes.sizeof(_lib.fr_particle) == 19 * 4
+    m = particle_meta(np.eye(3, dtype=np.float32)[None].repeat(2, 0), [[1, 2], [3, 4]],
+                      [0.5, 1.0], defocus=[1.5, 0.0])
+    assert m[1].tx == 3 and m[0].weight == 0.5 and m[0].defocus == 1.5 and m[1].voltage == 300
+
+
+def test_bench_pixel_counts():
+    import bench
+    assert [bench.pixels_per_slice(N) for N in (96, 192)] == [3738, 14711]
+    assert bench.nsym_of("d7") == 14 and bench.nsym_of("c4") == 4
+
+
+class FakeExecutor:
+    def __init__(self):
+        self.created, self.inserted, self.finished = 0, [], 0
+
+    def create(self, params):
+        self.created += 1
+        return {"params": params, "chunks": 0}
+
+    def insert(self, items):
+        self.inserted.append(len(items))
+        for h, _ in items:
+            h["chunks"] += 1
+
+    def finish(self, h):
+        self.finished += 1
+        return h["chunks"]
+
+
+def _req(rid, N, nchunks, arrival=0.0, chunk=8, box=None):
+    from eman2_b200.server import Request
+    box = box or N * 2 // 3
+    return Request(rid, {"size": [N] * 3, "sym": "c1", "mode": "gauss_2"},
+                   [(np.zeros((chunk, box, box), np.float32), None)] * nchunks, arrival)
+
+
+def test_scheduler_admits_by_footprint_and_batches_continuously():
+    from eman2_b200.server import Scheduler, Server, footprint_bytes
+    one = footprint_bytes({"size": [96] * 3}, 64, 8)
+    sched = Scheduler(hbm_budget=int(2.5 * one), max_active=8)
+    exe = FakeExecutor()
+    reqs = [_req(i, 96, 3 + i % 2) for i in range(5)] + [_req(9, 400, 1)]   # last never fits
+    res = Server(sched, exe).run(reqs)
+    assert res["requests"] == 5 and res["rejected"] == 1
+    # never more than two 96^3 jobs resident: batches of at most 2 chunks
+    assert max(exe.inserted) == 2
+    # every job got all its chunks, each exactly once
+    assert sorted(j.result for j in sched.done) == sorted(len(r.chunks) for r in reqs[:5])
+    assert sched.used == 0 and res["p99_s"] >= res["p50_s"] >= 0
+
+
+def test_scheduler_joins_late_arrivals_at_next_tick():
+    from eman2_b200.server import Scheduler
+    sched = Scheduler(hbm_budget=1 << 40, max_active=4)
+    exe = FakeExecutor()
+    sched.submit(_req(0, 64, 4, arrival=0.0))
+    sched.submit(_req(1, 64, 2, arrival=0.5))
+    sched.admit(0.0, exe)
+    assert len(sched.tick_work()) == 1
+    sched.admit(0.6, exe)                  # arrived while job 0 was on the GPU
+    assert len(sched.tick_work()) == 2     # both in the same tick now
