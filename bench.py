@@ -173,6 +173,62 @@ def cpu_sample(wl: dict, seed: int, budget_s: float = 15.0, max_n: int = 64, thr
     return total_n / total_t, total_n, threads, total_t
 
 
+# ------------------------------------------------------------------ serving
+def run_serving(dev, seed: int = 4242, nreq: int = 12, rate: float = 4.0, max_particles: int = 4000):
+    """A short Poisson stream of reconstruction requests (the served form):
+    boxes {64, 128, 192} padded x1.5, particle counts log-uniform over
+    [500, max_particles], sym c1/c4/d7, chunks of 512, arrivals at `rate`/s.
+    Returns p50/p99 latency and particle-slices/s, and the same requests run
+    one after another through the plain per-job path for comparison."""
+    import torch
+
+    from eman2_b200 import FourierReconstructor
+    from eman2_b200.particles import particle_meta
+    from eman2_b200.server import GpuExecutor, Request, Scheduler, Server
+    from eman2_b200.synth import make_particles
+    rng = np.random.default_rng(seed)
+    pools = {}
+    for box in (64, 128, 192):
+        ps = make_particles(box, 1024, seed=seed + box, snr=0.05, shift=4.0, weights=(0.5, 1.0),
+                            ctf=True, device=dev)
+        pools[box] = ps
+    reqs, t = [], 0.0
+    for k in range(nreq):
+        box = int(rng.choice([64, 128, 192]))
+        N = box * 3 // 2
+        n = int(np.exp(rng.uniform(np.log(500), np.log(max_particles))))
+        sym = str(rng.choice(["c1", "c4", "d7"]))
+        ps = pools[box]
+        chunks = []
+        for a in range(0, n, 512):
+            b = min(n, a + 512)
+            idx = np.arange(a, b) % 1024
+            chunks.append((ps.images[idx], particle_meta(ps.rots[idx], ps.shifts[idx],
+                                                         ps.weights[idx], defocus=ps.defocus[idx])))
+        t += float(rng.exponential(1.0 / rate))
+        reqs.append(Request(k, {"size": [N] * 3, "sym": sym, "mode": "gauss_2"}, chunks, arrival=t))
+    torch.cuda.synchronize()
+    sched = Scheduler(hbm_budget=int(torch.cuda.mem_get_info()[0] * 0.6), max_active=16)
+    res = Server(sched, GpuExecutor(doift=False)).run(reqs)
+    slices = sum(r.particles for r in reqs)
+    # plain per-job path: each request alone, one insert call per chunk
+    t0 = time.perf_counter()
+    for r in reqs:
+        rec = FourierReconstructor(r.params)
+        rec.setup()
+        for img, meta in r.chunks:
+            rec.insert_particles(img, meta, schedule="scatter")
+        rec.finish(False)
+        rec.close()
+    torch.cuda.synchronize()
+    plain_s = time.perf_counter() - t0
+    return {"requests": res["requests"], "p50_s": res["p50_s"], "p99_s": res["p99_s"],
+            "particle_slices_per_s": slices / res["wall_s"], "wall_s": res["wall_s"],
+            "plain_per_job_particle_slices_per_s": slices / plain_s,
+            "stream": f"{nreq} requests, Poisson {rate}/s, boxes 64/128/192 x1.5, "
+                      f"500-{max_particles} particles, c1/c4/d7, gauss_2, chunks of 512"}
+
+
 # ------------------------------------------------------------------ GPU run
 def run_gpu(args, wl, ws, rank, local):
     import torch
@@ -261,6 +317,7 @@ def main():
     ap.add_argument("--batch", type=int, default=2048, help="particles per step")
     ap.add_argument("--plain", type=int, default=64, help="particles timed on the plain path")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving latency leg")
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]
     ws, rank, local = dist_setup()
@@ -332,6 +389,9 @@ def main():
     if plain is not None:
         line["plain_gpu"] = {"value": plain, "unit": "particle-slices/s", "sample": args.plain,
                              "speedup_batched_vs_plain": value / plain}
+    if not args.no_serve and ws == 1:
+        import torch
+        line["latency"] = run_serving(torch.device("cuda", local))
     if not args.no_cpu and ws == 1:
         v, n, thr, secs = cpu_sample(wl, seed=7000)
         line["cpu_baseline"] = {"value": v, "unit": "particle-slices/s", "cores": thr,
