@@ -247,6 +247,8 @@ def run_gpu(args, wl, ws, rank, local):
     meta = particle_meta(ps.rots, ps.shifts, ps.weights, defocus=ps.defocus)
     r = Reconstructors.get("fourier", {"size": [N] * 3, "sym": wl["sym"], "mode": wl["mode"]})
     r.setup()
+    if args.tile != -1:
+        _lib.check(lib.fr_set_tile(N, _lib.MODE_IDS[wl["mode"]], nsym_of(wl["sym"]), args.tile))
     stream = torch.cuda.Stream(device=dev)
     _lib.check(lib.fr_set_stream(r.handle, ctypes.c_void_p(stream.cuda_stream)))
 
@@ -318,6 +320,9 @@ def main():
     ap.add_argument("--plain", type=int, default=64, help="particles timed on the plain path")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving latency leg")
+    ap.add_argument("--tile", type=int, default=-1,
+                    help="pin the insertion kernel (0-3 register tiles, 4 staged column, "
+                         "5 barrier-free column, -2 scatter); default: library choice")
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]
     ws, rank, local = dist_setup()

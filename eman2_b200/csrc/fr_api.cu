@@ -3,6 +3,7 @@
 // prologue / insertion / agreement / finish kernels.
 #include <algorithm>
 #include <atomic>
+#include <cstdint>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -43,6 +44,69 @@ static std::mutex g_mu;
 static std::map<int, Consts> g_consts;
 static std::map<std::pair<int, int>, Geom *> g_geoms[64];
 
+// Table index of Util::fast_exp(-r*h) for a float r >= 0, evaluated with the
+// reference's rounding points (f = -r*h in float; (int)(-f*50.0+0.5) in
+// double); -1 when f < -19.98 (the exp() branch).
+static int exp_index(float r, float h) {
+  volatile float rv = r, hv = h;
+  const float f = -(rv * hv);
+  if ((double)f > 0 || (double)f < -19.98) return -1;
+  return (int)(-(double)f * 50.0 + 0.5);
+}
+
+// Smallest float r >= 0 with pred(r) true, for pred monotone in r.
+template <class P> static float min_float_where(P pred, float hi) {
+  uint32_t lo_b = 0, hi_b;
+  memcpy(&hi_b, &hi, 4);
+  while (lo_b < hi_b) {
+    const uint32_t mid = lo_b + (hi_b - lo_b) / 2;
+    float m;
+    memcpy(&m, &mid, 4);
+    if (pred(m)) hi_b = mid;
+    else lo_b = mid + 1;
+  }
+  float out;
+  memcpy(&out, &lo_b, 4);
+  return out;
+}
+
+// Builds the step table of fast_exp(-r*h) over r in [0, rmax).
+static void build_steps(float h, float K, float rmax, const float *tab, ExpSteps &out) {
+  const float rout = min_float_where([&](float r) { return exp_index(r, h) < 0 && r > 0; }, 1e4f);
+  const float rend = std::min(rmax, rout);
+  const int nb = (int)std::ceil(rend * K) + 1;
+  std::vector<float4> bins(nb);
+  for (int b = 0; b < nb; b++) {
+    const float r0 = (float)b / K, r1 = (float)(b + 1) / K;
+    int g0 = exp_index(r0, h);
+    float4 e;
+    if (g0 < 0) {   // the whole bin is past the table: entries unused
+      e = make_float4(0.f, 0.f, 0.f, 0.f);
+    } else {
+      float thr = INFINITY;
+      if (g0 + 1 <= 999) {
+        const float t = min_float_where([&](float r) { int g = exp_index(r, h); return g < 0 || g >= g0 + 1; }, 1e4f);
+        if (t < r1) thr = t;
+      }
+      const int g1 = std::min(g0 + 1, 999);
+      e = make_float4(thr, tab[g0], tab[g1], 0.f);
+    }
+    bins[b] = e;
+    // at most one threshold per bin (thresholds are 1/(50h) apart in r)
+    if (g0 >= 0) {
+      const float below_r1 = std::nextafter(r1, 0.0f);
+      const int g1 = exp_index(below_r1, h);
+      if (g1 >= 0 && g1 > g0 + 1)
+        fprintf(stderr, "eman2_b200: exp step table bin %d holds two thresholds\n", b);
+    }
+  }
+  out.K = K;
+  out.rout = rout;
+  out.nbins = nb;
+  cudaMalloc(&out.d_bins, sizeof(float4) * nb);
+  cudaMemcpy(out.d_bins, bins.data(), sizeof(float4) * nb, cudaMemcpyHostToDevice);
+}
+
 Consts &consts() {
   int dev = 0;
   cudaGetDevice(&dev);
@@ -63,6 +127,8 @@ Consts &consts() {
   volatile float i5g = (float)(10.4 / (M_PI * M_PI));
   c.h2 = 1.0f / i2g;
   c.h5 = 1.0f / i5g;
+  build_steps(c.h2, 256.0f, 3.01f, tab, c.steps2);   // gauss_2 taps: |d| <= 1 per axis, r <= 3
+  build_steps(c.h5, 64.0f, 40.0f, tab, c.steps5);
   return g_consts[dev] = c;
 }
 
@@ -305,7 +371,7 @@ int insert_device(fr_recon *r, const float2 *d_slices, const float *d_t3d, const
   }
   int tile = r->tile >= 0 ? r->tile : (tuned >= 0 ? tuned : default_tile(r->mode, r->N, r->nsym, np));
   if (r->tiles_tile != tile) {
-    if (tile == kColumnTile)
+    if (tile == kColumnTile || tile == kColumn3Tile)
       column_tiles(r->N, r->mode, r->p.corners, r->tiles, r->tx, r->ty, r->tz, &r->tile_dist);
     else gather_tiles(r->N, r->mode, tile, r->p.corners, r->tiles, r->tx, r->ty, r->tz);
     r->tiles_tile = tile;
@@ -316,7 +382,8 @@ int insert_device(fr_recon *r, const float2 *d_slices, const float *d_t3d, const
   j.tiles_z = r->tz;
   const int nsl = np * r->nsym;
   int nwork = 0;
-  if (tile == kColumnTile) {
+  const bool column = tile == kColumnTile || tile == kColumn3Tile;
+  if (column) {
     // work items (job 0, tile, first slice of the block)
     if (r->work_np != nsl) {
       std::vector<int4> work;
@@ -346,7 +413,10 @@ int insert_device(fr_recon *r, const float2 *d_slices, const float *d_t3d, const
   TRY(r->s_counter.ensure(sizeof(int)));
   CU(cudaMemcpyAsync(r->s_jobs.p, &j, sizeof(InsertJob), cudaMemcpyHostToDevice, st));
   if (prof) CU(cudaEventRecord(ev[0], st));
-  if (tile == kColumnTile)
+  if (tile == kColumn3Tile)
+    CU(launch_column3(r->s_jobs.as<InsertJob>(), r->s_work.as<int4>(), nwork, kColumnBlock,
+                      r->s_counter.as<int>(), r->N, st));
+  else if (tile == kColumnTile)
     CU(launch_column(r->s_jobs.as<InsertJob>(), r->s_work.as<int4>(), nwork, kColumnBlock,
                      r->s_counter.as<int>(), r->mode, st));
   else

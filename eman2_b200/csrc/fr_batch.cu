@@ -35,7 +35,7 @@ int tuned_tile(int N, int mode, int nsym) {
 
 int default_tile(int mode, int N, int nsym, int np) {
   (void)nsym; (void)np; (void)N; (void)mode;
-  return kColumnTile;   // the column-owner kernel unless the autotuner measured otherwise
+  return kColumn3Tile;   // the barrier-free column kernel unless the autotuner measured otherwise
 }
 
 }  // namespace fr
@@ -127,12 +127,12 @@ static int batch_insert(std::vector<fr_recon *> &jobs, BatchScratch &bs, int til
   const int chunk = 4096;
   int rounds = 0;
   for (int j = 0; j < nj; j++) rounds = std::max(rounds, (counts[j] + chunk - 1) / chunk);
-  const int tile = tile_pref >= 0 ? tile_pref : kColumnTile;
-  const bool column = tile == kColumnTile;
+  const int tile = tile_pref >= 0 ? tile_pref : default_tile(0, 0, 0, 0);
+  const bool column = tile == kColumnTile || tile == kColumn3Tile;
   for (int rd = 0; rd < rounds; rd++) {
     std::vector<InsertJob> hj;
     std::vector<int> owner;
-    int max_mode = FR_MODE_NEAREST;
+    int max_mode = FR_MODE_NEAREST, maxN = 0;
     for (int j = 0; j < nj; j++) {
       fr_recon *r = jobs[j];
       const int p0 = rd * chunk;
@@ -155,6 +155,7 @@ static int batch_insert(std::vector<fr_recon *> &jobs, BatchScratch &bs, int til
       J.tiles_z = r->tz;
       hj.push_back(J);
       owner.push_back(j);
+      maxN = std::max(maxN, r->N);
       if (r->mode == FR_MODE_GAUSS5) max_mode = FR_MODE_GAUSS5;
       else if (max_mode != FR_MODE_GAUSS5 && r->mode != FR_MODE_NEAREST) max_mode = r->mode;
     }
@@ -195,8 +196,12 @@ static int batch_insert(std::vector<fr_recon *> &jobs, BatchScratch &bs, int til
       TRY(bs.d_work.ensure(sizeof(int4) * work.size()));
       CU(cudaMemcpyAsync(bs.d_work.p, work.data(), sizeof(int4) * work.size(),
                          cudaMemcpyHostToDevice, st));
-      CU(launch_column(bs.d_jobs.as<InsertJob>(), bs.d_work.as<int4>(), (int)work.size(),
-                       kColumnBlock, bs.d_counter.as<int>(), max_mode, st));
+      if (tile == kColumn3Tile)
+        CU(launch_column3(bs.d_jobs.as<InsertJob>(), bs.d_work.as<int4>(), (int)work.size(),
+                          kColumnBlock, bs.d_counter.as<int>(), maxN, st));
+      else
+        CU(launch_column(bs.d_jobs.as<InsertJob>(), bs.d_work.as<int4>(), (int)work.size(),
+                         kColumnBlock, bs.d_counter.as<int>(), max_mode, st));
     } else {
       std::vector<int2> work(items.size());
       for (size_t i = 0; i < items.size(); i++) work[i] = make_int2(items[i].second.x, items[i].second.y);
@@ -259,7 +264,7 @@ int fr_batch_get_accumulators(fr_batch *b, int job, float *data, float *norm) {
 }
 
 int fr_set_tile(int N, int mode, int nsym, int tile) {
-  if (tile != kTunedScatter && (tile < -1 || tile > kColumnTile))
+  if (tile != kTunedScatter && (tile < -1 || tile > kColumn3Tile))
     return fail(FR_EINVAL_PARAM, "tile %d out of range", tile);
   std::lock_guard<std::mutex> lk(g_tune_mu);
   if (tile == -1) g_tuned.erase(std::make_tuple(N, mode, nsym));

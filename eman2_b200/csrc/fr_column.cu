@@ -27,6 +27,8 @@ namespace col {
 constexpr int T = 16;          // tile edge
 constexpr int NT = 256;        // threads: one per column
 constexpr int NV = T * T * T;  // voxels per tile
+constexpr int PIXCAP = 1024;   // staged pixels per patch chunk (rows are chunked to fit)
+constexpr int STEPCAP = 1360;  // step-table entries held in shared memory
 constexpr float kDel = 0.02f;  // slack on the approximate plane geometry
 constexpr float kPlaneTol = 0.05f;
 
@@ -67,13 +69,25 @@ __device__ __forceinline__ void box_dot(const float *m, const float *lo, const f
 
 __device__ __forceinline__ float comp(const float4 &v, int a) { return a == 0 ? v.x : (a == 1 ? v.y : v.z); }
 
+// fast_exp(-r*h) through the exact step table (see ExpSteps): one exact bin
+// (K is a power of two, so r*K is exact), one compare.  Past the table the
+// reference calls exp(f) with f = -r*h in float.
+__device__ __forceinline__ float step_exp(float r, float h, const ExpSteps &st,
+                                          const float4 *__restrict__ bins) {
+  if (r >= st.rout) return expf(__fmul_rn(-r, h));
+  const int b = (int)floorf(__fmul_rn(r, st.K));
+  const float4 e = bins[b];
+  return r >= e.x ? e.z : e.y;
+}
+
 struct Smem {
   float4 *acc;      // [NV] (re, im, w, origin-touched)
-  float4 *pt;       // [side^2] (xx, yy, zz, re)
-  float *pim;       // [side^2] im
+  float4 *steps;    // [STEPCAP] fast_exp step table of the current mode
+  float4 *pt;       // [PIXCAP] (xx, yy, zz, re)
+  float *pim;       // [PIXCAP] im
   int *hits;        // [block]
-  float *exp;       // [1000]
   int *wcount;      // [8]
+  int *steps_mode;  // mode whose table is loaded
 };
 
 // One pass (direct or conjugate targets) of one slice for the thread's column.
@@ -81,7 +95,8 @@ struct Smem {
 template <int MODE, int A>
 __device__ __forceinline__ void column_pass(const Smem &S, const float *m0, const float *m1, int sg,
                                             const int *base, const int *ext, int px0, int py0,
-                                            int PW, int PH, float w, float h) {
+                                            int PW, int PH, float w, float h,
+                                            const ExpSteps &steps) {
   constexpr int B = (A == 0) ? 1 : 0;
   constexpr int C = (A == 2) ? 1 : 2;
   constexpr float RLO = Win<MODE>::lo, RHI = Win<MODE>::hi;
@@ -137,26 +152,66 @@ __device__ __forceinline__ void column_pass(const Smem &S, const float *m0, cons
       const float pa = comp(pt, A), pb = comp(pt, B), pc = comp(pt, C);
       if (!(in_win<MODE>(tb, pb) && in_win<MODE>(tc, pc))) continue;
       const int a0 = win_start<MODE>(pa);
-      const int k0 = max(a0, ta_lo), k1 = min(a0 + K - 1, ta_hi);
-      if (k0 > k1) continue;
+      if (a0 + K - 1 < ta_lo || a0 > ta_hi) continue;
       const float pim = S.pim[rowoff + x];
-      for (int k = k0; k <= k1; k++) {
-        int t[3];
-        t[A] = k; t[B] = tb; t[C] = tc;
+      const float re = pt.w;
+      // fixed parts of the distance, kept in the reference's order
+      // ((dx^2 + dy^2) + dz^2) (libEM/util.h:816-819)
+      float f0 = 0.f, f1 = 0.f;
+      if (MODE == MODE_GAUSS2 || MODE == MODE_GAUSS5) {
+        if (A == 0) {
+          const float dy = __fsub_rn((float)tb, pt.y), dz = __fsub_rn((float)tc, pt.z);
+          f0 = __fmul_rn(dy, dy);
+          f1 = __fmul_rn(dz, dz);
+        } else if (A == 1) {
+          const float dx = __fsub_rn((float)tb, pt.x), dz = __fsub_rn((float)tc, pt.z);
+          f0 = __fmul_rn(dx, dx);
+          f1 = __fmul_rn(dz, dz);
+        } else {
+          const float dx = __fsub_rn((float)tb, pt.x), dy = __fsub_rn((float)tc, pt.y);
+          f0 = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
+        }
+      }
+#pragma unroll
+      for (int kk = 0; kk < K; kk++) {
+        const int k = a0 + kk;
+        if (k < ta_lo || k > ta_hi) continue;
         float vre, vim, vw;
-        tap_value<MODE>(t[0], t[1], t[2], pt.x, pt.y, pt.z, pt.w, pim, w, h, S.exp, vre, vim, vw);
+        if (MODE == MODE_GAUSS2 || MODE == MODE_GAUSS5) {
+          const float d = __fsub_rn((float)k, pa);
+          const float d2 = __fmul_rn(d, d);
+          float r;
+          if (A == 0) r = __fadd_rn(__fadd_rn(d2, f0), f1);
+          else if (A == 1) r = __fadd_rn(__fadd_rn(f0, d2), f1);
+          else r = __fadd_rn(f0, d2);
+          if (MODE == MODE_GAUSS2) {
+            const float gg = __fmul_rn(step_exp(r, h, steps, S.steps), w);
+            vre = __fmul_rn(re, gg);
+            vim = __fmul_rn(pim, gg);
+            vw = gg;
+          } else {
+            const float gg = step_exp(r, h, steps, S.steps);
+            vre = __fmul_rn(__fmul_rn(re, gg), w);
+            vim = __fmul_rn(__fmul_rn(pim, gg), w);
+            vw = __fmul_rn(gg, w);
+          }
+        } else {
+          int t[3];
+          t[A] = k; t[B] = tb; t[C] = tc;
+          tap_value<MODE>(t[0], t[1], t[2], pt.x, pt.y, pt.z, re, pim, w, h, nullptr, vre, vim, vw);
+        }
         const int la = sg * k + la_off;
         float4 *cell = &S.acc[col_addr + la * str[A]];
         float4 v = *cell;
+        const bool origin = (k == 0 && tb == 0 && tc == 0);
         if (sg > 0) {
           // direct add; the origin keeps only its real part and is marked
-          const bool origin = (t[0] == 0 && t[1] == 0 && t[2] == 0);
           v.x += vre;
           if (origin) v.w = 1.0f;
           else v.y += vim;
           v.z += vw;
         } else {
-          if (t[0] == 0 && t[1] == 0 && t[2] == 0) continue;   // the origin adds no conjugate
+          if (origin) continue;   // the origin adds no conjugate
           v.x += vre;
           v.y -= vim;
           const bool xzero = (A == 0) ? (k == 0) : xzero_col;
@@ -170,7 +225,7 @@ __device__ __forceinline__ void column_pass(const Smem &S, const float *m0, cons
 
 template <int MODE>
 __device__ void tile_item(const InsertJob &J, int tile, int s0, int s1, const Smem &S, int side,
-                          float h, int *err) {
+                          float h, const ExpSteps &steps, int *err) {
   constexpr float RLO = Win<MODE>::lo, RHI = Win<MODE>::hi;
   const int N = J.N, n2 = N >> 1, w2 = n2 + 1;
   const float Nf = (float)N;
@@ -208,9 +263,16 @@ __device__ void tile_item(const InsertJob &J, int tile, int s0, int s1, const Sm
     __syncthreads();
   }
   if (nhit == 0) return;
+  // ---- this mode's exp step table into shared memory (if not there yet)
+  if ((MODE == MODE_GAUSS2 || MODE == MODE_GAUSS5) && *S.steps_mode != MODE) {
+    const int nb = min(steps.nbins, STEPCAP);
+    for (int i = threadIdx.x; i < nb; i += NT) S.steps[i] = __ldg(&steps.d_bins[i]);
+    if (threadIdx.x == 0 && steps.nbins > STEPCAP) atomicOr(err, 8);
+  }
   // ---- zero the tile accumulators
   for (int i = threadIdx.x; i < NV; i += NT) S.acc[i] = make_float4(0.f, 0.f, 0.f, 0.f);
   __syncthreads();
+  if (threadIdx.x == 0) *S.steps_mode = MODE;
   for (int hI = 0; hI < nhit; hI++) {
     const int s = S.hits[hI];
     const int p = s / J.nsym;
@@ -237,33 +299,38 @@ __device__ void tile_item(const InsertJob &J, int tile, int s0, int s1, const Sm
       const int px0 = max(0, (int)floorf(xl) - 1), px1 = min(n2, (int)ceilf(xh) + 1);
       const int py0 = max(-n2, (int)floorf(yl) - 1), py1 = min(n2 - 1, (int)ceilf(yh) + 1);
       if (px0 > px1 || py0 > py1) continue;
-      int PW = px1 - px0 + 1, PH = py1 - py0 + 1;
-      if (PW > side || PH > side) {
+      const int PW = px1 - px0 + 1;
+      if (PW > side) {   // cannot happen for an orthonormal block; stay in bounds
         if (threadIdx.x == 0) atomicOr(err, 2);
-        PW = min(PW, side);
-        PH = min(PH, side);
+        continue;
       }
-      __syncthreads();
-      for (int i = threadIdx.x; i < PW * PH; i += NT) {
-        const int x = px0 + i % PW, y = py0 + i / PW;
-        float4 pt;
-        float pim = 0.f;
-        if (x > __ldg(&J.xmax[y + n2])) {
-          pt = make_float4(1e30f, 1e30f, 1e30f, 0.f);
-        } else {
-          pixel_coords(__ldg(&J.rtab[x + n2]), __ldg(&J.rtab[y + n2]), M, Nf, pt.x, pt.y, pt.z);
-          const float2 v = slice_value(sl, N, x, y);
-          pt.w = v.x;
-          pim = v.y;
+      const int rows_per = PIXCAP / PW;
+      // patches larger than the staging buffer go through in row chunks: the
+      // column work of one pixel row does not depend on any other row
+      for (int ry0 = py0; ry0 <= py1; ry0 += rows_per) {
+        const int PH = min(rows_per, py1 - ry0 + 1);
+        __syncthreads();
+        for (int i = threadIdx.x; i < PW * PH; i += NT) {
+          const int x = px0 + i % PW, y = ry0 + i / PW;
+          float4 pt;
+          float pim = 0.f;
+          if (x > __ldg(&J.xmax[y + n2])) {
+            pt = make_float4(1e30f, 1e30f, 1e30f, 0.f);
+          } else {
+            pixel_coords(__ldg(&J.rtab[x + n2]), __ldg(&J.rtab[y + n2]), M, Nf, pt.x, pt.y, pt.z);
+            const float2 v = slice_value_cg(sl, N, x, y);
+            pt.w = v.x;
+            pim = v.y;
+          }
+          S.pt[i] = pt;
+          S.pim[i] = pim;
         }
-        S.pt[i] = pt;
-        S.pim[i] = pim;
-      }
-      __syncthreads();
-      switch (A) {
-        case 0: column_pass<MODE, 0>(S, m0, m1, sg, base, ext, px0, py0, PW, PH, w, h); break;
-        case 1: column_pass<MODE, 1>(S, m0, m1, sg, base, ext, px0, py0, PW, PH, w, h); break;
-        default: column_pass<MODE, 2>(S, m0, m1, sg, base, ext, px0, py0, PW, PH, w, h); break;
+        __syncthreads();
+        switch (A) {
+          case 0: column_pass<MODE, 0>(S, m0, m1, sg, base, ext, px0, ry0, PW, PH, w, h, steps); break;
+          case 1: column_pass<MODE, 1>(S, m0, m1, sg, base, ext, px0, ry0, PW, PH, w, h, steps); break;
+          default: column_pass<MODE, 2>(S, m0, m1, sg, base, ext, px0, ry0, PW, PH, w, h, steps); break;
+        }
       }
     }
   }
@@ -290,23 +357,320 @@ __device__ void tile_item(const InsertJob &J, int tile, int s0, int s1, const Sm
   __syncthreads();
 }
 
+// ------------------------------------------------------------------ v3
+// Barrier-free variant: no patch staging.  Hits are grouped by the column
+// axis A; within a group every thread walks all slices for its own column,
+// computing each candidate pixel's coordinates itself (the same exact
+// operations), so threads never wait for one another until A changes.
+struct Smem3 {
+  float4 *acc;      // [NV]
+  float4 *steps;    // gauss_2 step table
+  float *exp;       // [1000] fast_exp table (gauss_5)
+  float *rtab;      // [N+2]
+  int *xmax;        // [N]
+  int *hits;        // [block] grouped by axis
+  int *tmp;         // [block]
+  int *wcount;      // [3 * NT/32]
+  int *gcount;      // [3]
+  int *state;       // [0] steps mode loaded, [1] job geometry loaded (N)
+};
+constexpr int STEP2CAP = 800;   // gauss_2 step table entries (K = 256 over r <= 3.01: 772)
+
+template <int MODE, int A>
+__device__ __forceinline__ void column_work(const Smem3 &S, const float *M, int sg, const int *base,
+                                            const int *ext, int N, const float2 *__restrict__ sl,
+                                            float w, float h, const ExpSteps &steps) {
+  constexpr int B = (A == 0) ? 1 : 0;
+  constexpr int C = (A == 2) ? 1 : 2;
+  constexpr float RLO = Win<MODE>::lo, RHI = Win<MODE>::hi;
+  constexpr int K = Win<MODE>::K;
+  const int n2 = N >> 1;
+  const float Nf = (float)N;
+  const float *m0 = M, *m1 = M + 3, *nrm = M + 6;
+  const int lb = threadIdx.x & 15, lc = threadIdx.x >> 4;
+  const int vb = base[B] + lb, vc = base[C] + lc;
+  if (vb > ext[B] || vc > ext[C]) return;
+  const int tb = sg * vb, tc = sg * vc;
+  const int ta_lo = sg > 0 ? base[A] : -ext[A];
+  const int ta_hi = sg > 0 ? ext[A] : -base[A];
+  float lo[3], hi[3];
+  lo[A] = ta_lo - RLO - kDel; hi[A] = ta_hi + RHI + kDel;
+  lo[B] = tb - RLO - kDel;    hi[B] = tb + RHI + kDel;
+  lo[C] = tc - RLO - kDel;    hi[C] = tc + RHI + kDel;
+  // quick reject: heights of the plane over the column's (b, c) window
+  {
+    const float ia = 1.0f / nrm[A];
+    float pmin = 1e30f, pmax = -1e30f;
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      const float pb = (i & 1) ? hi[B] : lo[B], pc = (i & 2) ? hi[C] : lo[C];
+      const float pa = -(nrm[B] * pb + nrm[C] * pc) * ia;
+      pmin = fminf(pmin, pa);
+      pmax = fmaxf(pmax, pa);
+    }
+    if (pmax < lo[A] - 0.05f || pmin > hi[A] + 0.05f) return;
+  }
+  const float det = m0[B] * m1[C] - m0[C] * m1[B];
+  const float idet = 1.0f / det;
+  float ymin = 1e30f, ymax = -1e30f;
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    const float pb = (i & 1) ? hi[B] : lo[B], pc = (i & 2) ? hi[C] : lo[C];
+    const float y = (m0[B] * pc - m0[C] * pb) * idet;
+    ymin = fminf(ymin, y);
+    ymax = fmaxf(ymax, y);
+  }
+  const int r0 = max(-n2, (int)ceilf(ymin)), r1 = min(n2 - 1, (int)floorf(ymax));
+  float inv0[3];
+#pragma unroll
+  for (int a = 0; a < 3; a++) inv0[a] = fabsf(m0[a]) > 1e-4f ? 1.0f / m0[a] : 0.0f;
+  const int str[3] = {1, T, T * T};
+  const int col_addr = lb * str[B] + lc * str[C];
+  const bool xzero_col = (A != 0) && (vb == 0);
+  for (int y = r0; y <= r1; y++) {
+    const int xm = S.xmax[y + n2];
+    float xlo = 0.f, xhi = (float)xm;
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      const float c = m1[a] * (float)y;
+      const float L = lo[a] - c, U = hi[a] - c;
+      if (inv0[a] > 0.f) { xlo = fmaxf(xlo, L * inv0[a]); xhi = fminf(xhi, U * inv0[a]); }
+      else if (inv0[a] < 0.f) { xlo = fmaxf(xlo, U * inv0[a]); xhi = fminf(xhi, L * inv0[a]); }
+      else if (L > 0.05f || U < -0.05f) xhi = -1e30f;
+    }
+    const int c0 = max(0, (int)ceilf(xlo)), c1 = min(xm, (int)floorf(xhi));
+    if (c0 > c1) continue;
+    const float ry = S.rtab[y + n2];
+    for (int x = c0; x <= c1; x++) {
+      float xx, yy, zz;
+      pixel_coords(S.rtab[x + n2], ry, M, Nf, xx, yy, zz);
+      const float pa = A == 0 ? xx : (A == 1 ? yy : zz);
+      const float pb = B == 0 ? xx : yy;
+      const float pc = C == 1 ? yy : zz;
+      if (!(in_win<MODE>(tb, pb) && in_win<MODE>(tc, pc))) continue;
+      const int a0 = win_start<MODE>(pa);
+      const int k0 = max(a0, ta_lo), k1 = min(a0 + K - 1, ta_hi);
+      if (k0 > k1) continue;
+      const float2 v = slice_value(sl, N, x, y);
+      float f0 = 0.f, f1 = 0.f;
+      if (MODE == MODE_GAUSS2 || MODE == MODE_GAUSS5) {
+        if (A == 0) {
+          const float dy = __fsub_rn((float)tb, yy), dz = __fsub_rn((float)tc, zz);
+          f0 = __fmul_rn(dy, dy); f1 = __fmul_rn(dz, dz);
+        } else if (A == 1) {
+          const float dx = __fsub_rn((float)tb, xx), dz = __fsub_rn((float)tc, zz);
+          f0 = __fmul_rn(dx, dx); f1 = __fmul_rn(dz, dz);
+        } else {
+          const float dx = __fsub_rn((float)tb, xx), dy = __fsub_rn((float)tc, yy);
+          f0 = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
+        }
+      }
+      for (int k = k0; k <= k1; k++) {
+        float vre, vim, vw;
+        if (MODE == MODE_GAUSS2 || MODE == MODE_GAUSS5) {
+          const float d = __fsub_rn((float)k, pa);
+          const float d2 = __fmul_rn(d, d);
+          float r;
+          if (A == 0) r = __fadd_rn(__fadd_rn(d2, f0), f1);
+          else if (A == 1) r = __fadd_rn(__fadd_rn(f0, d2), f1);
+          else r = __fadd_rn(f0, d2);
+          if (MODE == MODE_GAUSS2) {
+            const float gg = __fmul_rn(step_exp(r, h, steps, S.steps), w);
+            vre = __fmul_rn(v.x, gg);
+            vim = __fmul_rn(v.y, gg);
+            vw = gg;
+          } else {
+            const float gg = fast_exp(__fmul_rn(-r, h), S.exp);
+            vre = __fmul_rn(__fmul_rn(v.x, gg), w);
+            vim = __fmul_rn(__fmul_rn(v.y, gg), w);
+            vw = __fmul_rn(gg, w);
+          }
+        } else {
+          int t[3];
+          t[A] = k; t[B] = tb; t[C] = tc;
+          tap_value<MODE>(t[0], t[1], t[2], xx, yy, zz, v.x, v.y, w, h, nullptr, vre, vim, vw);
+        }
+        const int la = sg * k - base[A];
+        float4 *cell = &S.acc[col_addr + la * str[A]];
+        float4 u = *cell;
+        const bool origin = (k == 0 && tb == 0 && tc == 0);
+        if (sg > 0) {
+          u.x += vre;
+          if (origin) u.w = 1.0f;
+          else u.y += vim;
+          u.z += vw;
+        } else {
+          if (origin) continue;
+          u.x += vre;
+          u.y -= vim;
+          const bool xzero = (A == 0) ? (k == 0) : xzero_col;
+          if (!xzero) u.z += vw;
+        }
+        *cell = u;
+      }
+    }
+  }
+}
+
+template <int MODE, int A>
+__device__ __forceinline__ void group_work(const InsertJob &J, const Smem3 &S, int g0, int g1,
+                                           const int *base, const int *ext, float h,
+                                           const ExpSteps &steps) {
+  const int N = J.N, w2 = (N >> 1) + 1;
+  for (int hI = g0; hI < g1; hI++) {
+    const int s = S.hits[hI];
+    const int p = s / J.nsym;
+    float M[9];
+#pragma unroll
+    for (int i = 0; i < 9; i++) M[i] = __ldg(&J.t3d[9 * s + i]);
+    const float w = __ldg(&J.pw[p]);
+    const float2 *sl = J.slices + (size_t)p * N * w2;
+    column_work<MODE, A>(S, M, 1, base, ext, N, sl, w, h, steps);
+    column_work<MODE, A>(S, M, -1, base, ext, N, sl, w, h, steps);
+  }
+}
+
+template <int MODE>
+__device__ void tile_item3(const InsertJob &J, int tile, int s0, int s1, const Smem3 &S, float h,
+                           const ExpSteps &steps, int *err) {
+  constexpr float RLO = Win<MODE>::lo, RHI = Win<MODE>::hi;
+  const int N = J.N, n2 = N >> 1;
+  const int tix = tile % J.tiles_x, tiy = (tile / J.tiles_x) % J.tiles_y,
+            tiz = tile / (J.tiles_x * J.tiles_y);
+  const int base[3] = {tix * T, -n2 + 1 + tiy * T, -n2 + 1 + tiz * T};
+  const int ext[3] = {min(base[0] + T - 1, n2 - 1), min(base[1] + T - 1, n2 - 1),
+                      min(base[2] + T - 1, n2 - 1)};
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int NW = NT / 32;
+  // ---- cull, and count the hits of each axis group
+  int nhit = 0;
+  for (int r = s0; r < s1; r += NT) {
+    const int s = r + threadIdx.x;
+    int grp = -1;
+    if (s < s1 && __ldg(&J.pw[s / J.nsym]) != 0.0f) {
+      const float n[3] = {__ldg(&J.t3d[9 * s + 6]), __ldg(&J.t3d[9 * s + 7]), __ldg(&J.t3d[9 * s + 8])};
+      const float lo[3] = {base[0] - RLO - kDel, base[1] - RLO - kDel, base[2] - RLO - kDel};
+      const float hi[3] = {ext[0] + RHI + kDel, ext[1] + RHI + kDel, ext[2] + RHI + kDel};
+      float mn, mx;
+      box_dot(n, lo, hi, mn, mx);
+      if (mn <= kPlaneTol && mx >= -kPlaneTol) {
+        const float a0 = fabsf(n[0]), a1 = fabsf(n[1]), a2 = fabsf(n[2]);
+        grp = (a0 >= a1 && a0 >= a2) ? 0 : (a1 >= a2 ? 1 : 2);
+      }
+    }
+    const unsigned b = __ballot_sync(0xffffffffu, grp >= 0);
+    if (lane == 0) S.wcount[warp] = __popc(b);
+    __syncthreads();
+    int off = 0, tot = 0;
+#pragma unroll
+    for (int i = 0; i < NW; i++) {
+      const int c = S.wcount[i];
+      off += (i < warp) ? c : 0;
+      tot += c;
+    }
+    if (grp >= 0) {
+      const int at = nhit + off + __popc(b & ((1u << lane) - 1u));
+      S.tmp[at] = s | (grp << 28);
+    }
+    nhit += tot;
+    __syncthreads();
+  }
+  if (nhit == 0) return;
+  // ---- stable partition of the hits by axis group
+  if (threadIdx.x < 3) S.gcount[threadIdx.x] = 0;
+  __syncthreads();
+  int gstart[4];
+  {
+    int base_g = 0;
+    for (int g = 0; g < 3; g++) {
+      gstart[g] = base_g;
+      for (int r = 0; r < nhit; r += NT) {
+        const int i = r + threadIdx.x;
+        const bool in = i < nhit && (S.tmp[i] >> 28) == g;
+        const unsigned b = __ballot_sync(0xffffffffu, in);
+        if (lane == 0) S.wcount[warp] = __popc(b);
+        __syncthreads();
+        int off = 0, tot = 0;
+#pragma unroll
+        for (int q = 0; q < NW; q++) {
+          const int c = S.wcount[q];
+          off += (q < warp) ? c : 0;
+          tot += c;
+        }
+        if (in) S.hits[base_g + off + __popc(b & ((1u << lane) - 1u))] = S.tmp[i] & 0x0FFFFFFF;
+        base_g += tot;
+        __syncthreads();
+      }
+    }
+    gstart[3] = base_g;
+  }
+  // ---- per-job tables and this mode's exp table
+  if (*(S.state + 1) != J.N) {
+    for (int i = threadIdx.x; i < N + 2; i += NT) S.rtab[i] = __ldg(&J.rtab[i]);
+    for (int i = threadIdx.x; i < N; i += NT) S.xmax[i] = __ldg(&J.xmax[i]);
+  }
+  if (MODE == MODE_GAUSS2 && *S.state != MODE) {
+    const int nb = min(steps.nbins, STEP2CAP);
+    for (int i = threadIdx.x; i < nb; i += NT) S.steps[i] = __ldg(&steps.d_bins[i]);
+    if (threadIdx.x == 0 && steps.nbins > STEP2CAP) atomicOr(err, 8);
+  }
+  for (int i = threadIdx.x; i < NV; i += NT) S.acc[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (MODE == MODE_GAUSS2) *S.state = MODE;
+    *(S.state + 1) = J.N;
+  }
+  // ---- the three axis groups; ownership of a voxel changes only between them
+  if (gstart[1] > gstart[0]) group_work<MODE, 0>(J, S, gstart[0], gstart[1], base, ext, h, steps);
+  __syncthreads();
+  if (gstart[2] > gstart[1]) group_work<MODE, 1>(J, S, gstart[1], gstart[2], base, ext, h, steps);
+  __syncthreads();
+  if (gstart[3] > gstart[2]) group_work<MODE, 2>(J, S, gstart[2], gstart[3], base, ext, h, steps);
+  __syncthreads();
+  // ---- flush
+  const size_t nxf = (size_t)N + 2;
+  const int w2 = n2 + 1;
+  for (int i = threadIdx.x; i < NV; i += NT) {
+    const float4 v = S.acc[i];
+    if (v.x == 0.f && v.y == 0.f && v.z == 0.f && v.w == 0.f) continue;
+    const int vx = base[0] + (i & 15), vy = base[1] + ((i >> 4) & 15), vz = base[2] + (i >> 8);
+    if (vx > ext[0] || vy > ext[1] || vz > ext[2]) continue;
+    const size_t row = (size_t)(vy < 0 ? N + vy : vy);
+    const size_t slab = (size_t)(vz < 0 ? N + vz : vz);
+    const size_t di = (size_t)vx * 2 + row * nxf + slab * nxf * (size_t)N;
+    const size_t ni = (size_t)vx + row * (size_t)w2 + slab * (size_t)w2 * (size_t)N;
+    if (v.w != 0.f) {
+      atomicAdd(&J.data[di], v.x);
+      J.data[di + 1] = 0.0f;
+    } else {
+      atomicAdd(reinterpret_cast<float2 *>(&J.data[di]), make_float2(v.x, v.y));
+    }
+    if (v.z != 0.f) atomicAdd(&J.norm[ni], v.z);
+  }
+  __syncthreads();
+}
+
 }  // namespace col
 
 // work[i] = (job, tile, first slice, end slice); blocks are at most `block`.
 __global__ void __launch_bounds__(col::NT, 2)
     k_column(const InsertJob *__restrict__ jobs, const int4 *__restrict__ work, int nwork, int block,
-             int *counter, const float *__restrict__ exp_g, float h2, float h5, int side, int *err) {
+             int *counter, const float *__restrict__ exp_g, float h2, float h5, ExpSteps st2,
+             ExpSteps st5, int side, int *err) {
   extern __shared__ float4 s_dyn[];
   __shared__ int s_work;
   __shared__ int s_wcount[col::NT / 32];
+  __shared__ int s_steps_mode;
   col::Smem S;
   S.acc = s_dyn;
-  S.pt = s_dyn + col::NV;
-  S.pim = reinterpret_cast<float *>(S.pt + side * side);
-  S.hits = reinterpret_cast<int *>(S.pim + side * side);
-  S.exp = reinterpret_cast<float *>(S.hits + block);
+  S.steps = s_dyn + col::NV;
+  S.pt = S.steps + col::STEPCAP;
+  S.pim = reinterpret_cast<float *>(S.pt + col::PIXCAP);
+  S.hits = reinterpret_cast<int *>(S.pim + col::PIXCAP);
   S.wcount = s_wcount;
-  for (int i = threadIdx.x; i < 1000; i += blockDim.x) S.exp[i] = exp_g[i];
+  S.steps_mode = &s_steps_mode;
+  if (threadIdx.x == 0) s_steps_mode = -1;
+  (void)exp_g;
   while (true) {
     __syncthreads();
     if (threadIdx.x == 0) s_work = atomicAdd(counter, 1);
@@ -317,14 +681,81 @@ __global__ void __launch_bounds__(col::NT, 2)
     const InsertJob J = jobs[wk.x];
     const int s0 = wk.z, s1 = min(min(wk.w, wk.z + block), J.np * J.nsym);
     switch (J.mode) {
-      case MODE_GAUSS2: col::tile_item<MODE_GAUSS2>(J, wk.y, s0, s1, S, side, h2, err); break;
-      case MODE_GAUSS5: col::tile_item<MODE_GAUSS5>(J, wk.y, s0, s1, S, side, h5, err); break;
-      case MODE_NEAREST: col::tile_item<MODE_NEAREST>(J, wk.y, s0, s1, S, side, h2, err); break;
-      case MODE_TRILINEAR: col::tile_item<MODE_TRILINEAR>(J, wk.y, s0, s1, S, side, h2, err); break;
+      case MODE_GAUSS2: col::tile_item<MODE_GAUSS2>(J, wk.y, s0, s1, S, side, h2, st2, err); break;
+      case MODE_GAUSS5: col::tile_item<MODE_GAUSS5>(J, wk.y, s0, s1, S, side, h5, st5, err); break;
+      case MODE_NEAREST: col::tile_item<MODE_NEAREST>(J, wk.y, s0, s1, S, side, h2, st2, err); break;
+      case MODE_TRILINEAR: col::tile_item<MODE_TRILINEAR>(J, wk.y, s0, s1, S, side, h2, st2, err); break;
       default:
         if (threadIdx.x == 0) atomicOr(err, 4);
     }
   }
+}
+
+__global__ void __launch_bounds__(col::NT, 2)
+    k_column3(const InsertJob *__restrict__ jobs, const int4 *__restrict__ work, int nwork,
+              int block, int *counter, const float *__restrict__ exp_g, float h2, float h5,
+              ExpSteps st2, ExpSteps st5, int maxN, int *err) {
+  extern __shared__ float4 s_dyn[];
+  __shared__ int s_work;
+  __shared__ int s_wcount[col::NT / 32];
+  __shared__ int s_gcount[3];
+  __shared__ int s_state[2];
+  col::Smem3 S;
+  S.acc = s_dyn;
+  S.steps = s_dyn + col::NV;
+  S.exp = reinterpret_cast<float *>(S.steps + col::STEP2CAP);
+  S.rtab = S.exp + 1000;
+  S.xmax = reinterpret_cast<int *>(S.rtab + maxN + 2);
+  S.hits = S.xmax + maxN;
+  S.tmp = S.hits + block;
+  S.wcount = s_wcount;
+  S.gcount = s_gcount;
+  S.state = s_state;
+  for (int i = threadIdx.x; i < 1000; i += blockDim.x) S.exp[i] = exp_g[i];
+  if (threadIdx.x == 0) { s_state[0] = -1; s_state[1] = -1; }
+  while (true) {
+    __syncthreads();
+    if (threadIdx.x == 0) s_work = atomicAdd(counter, 1);
+    __syncthreads();
+    const int wi = s_work;
+    if (wi >= nwork) break;
+    const int4 wk = work[wi];
+    const InsertJob J = jobs[wk.x];
+    const int s0 = wk.z, s1 = min(min(wk.w, wk.z + block), J.np * J.nsym);
+    switch (J.mode) {
+      case MODE_GAUSS2: col::tile_item3<MODE_GAUSS2>(J, wk.y, s0, s1, S, h2, st2, err); break;
+      case MODE_GAUSS5: col::tile_item3<MODE_GAUSS5>(J, wk.y, s0, s1, S, h5, st5, err); break;
+      case MODE_NEAREST: col::tile_item3<MODE_NEAREST>(J, wk.y, s0, s1, S, h2, st2, err); break;
+      case MODE_TRILINEAR: col::tile_item3<MODE_TRILINEAR>(J, wk.y, s0, s1, S, h2, st2, err); break;
+      default:
+        if (threadIdx.x == 0) atomicOr(err, 4);
+    }
+  }
+}
+
+cudaError_t launch_column3(const InsertJob *d_jobs, const int4 *d_work, int nwork, int block,
+                           int *d_counter, int maxN, cudaStream_t st) {
+  if (nwork == 0) return cudaSuccess;
+  const Consts &c = consts();
+  const size_t smem = sizeof(float4) * (col::NV + col::STEP2CAP) + sizeof(float) * 1000 +
+                      sizeof(float) * (maxN + 2) + sizeof(int) * maxN + 2 * sizeof(int) * block;
+  static size_t configured = 0;
+  if (configured < smem) {
+    cudaFuncSetAttribute(k_column3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    configured = smem;
+  }
+  cudaError_t e = cudaMemsetAsync(d_counter, 0, sizeof(int), st);
+  if (e != cudaSuccess) return e;
+  int dev = 0, sms = 148, per_sm = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_column3, col::NT, smem);
+  if (per_sm < 1) per_sm = 1;
+  const int grid = std::max(1, std::min(nwork, sms * per_sm));
+  note_launch();
+  k_column3<<<grid, col::NT, smem, st>>>(d_jobs, d_work, nwork, block, d_counter, c.d_exp, c.h2,
+                                         c.h5, c.steps2, c.steps5, maxN, c.d_err);
+  return cudaGetLastError();
 }
 
 int column_side(int max_mode) {
@@ -335,8 +766,9 @@ int column_side(int max_mode) {
 }
 
 size_t column_smem(int side, int block) {
-  return sizeof(float4) * (col::NV + (size_t)side * side) + sizeof(float) * side * side +
-         sizeof(int) * block + sizeof(float) * 1000;
+  (void)side;
+  return sizeof(float4) * (col::NV + col::STEPCAP + col::PIXCAP) + sizeof(float) * col::PIXCAP +
+         sizeof(int) * block;
 }
 
 cudaError_t launch_column(const InsertJob *d_jobs, const int4 *d_work, int nwork, int block,
@@ -360,7 +792,7 @@ cudaError_t launch_column(const InsertJob *d_jobs, const int4 *d_work, int nwork
   const int grid = std::max(1, std::min(nwork, sms * per_sm));
   note_launch();
   k_column<<<grid, col::NT, smem, st>>>(d_jobs, d_work, nwork, block, d_counter, c.d_exp, c.h2, c.h5,
-                                        side, c.d_err);
+                                        c.steps2, c.steps5, side, c.d_err);
   return cudaGetLastError();
 }
 

@@ -146,4 +146,15 @@ __device__ __forceinline__ float2 slice_value(const float2 *__restrict__ s, int 
   return __ldg(&s[(size_t)(y < 0 ? N + y : y) * w + x]);
 }
 
+// The same read with the load cached in L2 only (ld.global.cg): for values
+// staged once into shared memory, so they do not evict L1-resident tables.
+__device__ __forceinline__ float2 slice_value_cg(const float2 *__restrict__ s, int N, int x, int y) {
+  const int w = (N >> 1) + 1;
+  if (x == 0 && y < 0) {
+    const float2 v = __ldcg(&s[(size_t)(-y) * w]);
+    return make_float2(v.x, -v.y);
+  }
+  return __ldcg(&s[(size_t)(y < 0 ? N + y : y) * w + x]);
+}
+
 }  // namespace fr

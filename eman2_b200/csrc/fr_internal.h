@@ -53,10 +53,22 @@ struct InsertJob {
 // Launch accounting (fr_api.cu).
 void note_launch(int n = 1);
 
+// fast_exp(-r*h) as a function of r: the table index is monotone in r, so
+// it is a step function with thresholds R_k.  Bins of width 1/K (K a power
+// of two, so floor(r*K) is exact) hold at most one threshold each; an entry
+// is (threshold, weight below it, weight from it on, unused).  r >= rout
+// leaves the table (the reference's exp() branch).
+struct ExpSteps {
+  float4 *d_bins = nullptr;
+  int nbins = 0;
+  float K = 0, rout = 0;
+};
+
 struct Consts {
   float *d_exp = nullptr;    // Util::fast_exp table [1000]
   float h2 = 0, h5 = 0;      // 1/I2G, 1/I5G as the reference forms them
   int *d_err = nullptr;      // device error word
+  ExpSteps steps2, steps5;   // gauss_2 and gauss_5 step tables
 };
 Consts &consts();            // lazily initialised on the current device
 
@@ -87,6 +99,10 @@ cudaError_t launch_column(const InsertJob *d_jobs, const int4 *d_work, int nwork
                           int *d_counter, int max_mode, cudaStream_t st);
 void column_tiles(int N, int mode, int corners, std::vector<int> &out, int &tx, int &ty, int &tz,
                   std::vector<float> *dist = nullptr);
+// The barrier-free column kernel (no patch staging; hits grouped by axis).
+constexpr int kColumn3Tile = kNumTiles + 1;
+cudaError_t launch_column3(const InsertJob *d_jobs, const int4 *d_work, int nwork, int block,
+                           int *d_counter, int maxN, cudaStream_t st);
 // Ordered work list (tile ids of a job that can receive interior taps).
 void gather_tiles(int N, int mode, int tile, int corners, std::vector<int> &out, int &tx, int &ty,
                   int &tz);
