@@ -35,6 +35,9 @@ WORKLOADS = {
     "c4": dict(box=256, N=384, mode="gauss_5", sym="d7", ctf=True, snr=0.02, shift=4.0,
                weights=(0.5, 1.0), job=200_000,
                desc="box 256 pad 384, gauss_5, d7, CTF, SNR 0.02 (200k-particle job)"),
+    "c4g2": dict(box=256, N=384, mode="gauss_2", sym="d7", ctf=True, snr=0.02, shift=4.0,
+                 weights=(0.5, 1.0), job=200_000,
+                 desc="box 256 pad 384, gauss_2, d7, CTF, SNR 0.02 (the targets' configuration)"),
     "c2": dict(box=128, N=192, mode="gauss_2", sym="c1", ctf=True, snr=0.05, shift=4.0,
                weights=(0.5, 1.0), job=20_000,
                desc="box 128 pad 192, gauss_2, c1, CTF, SNR 0.05 (20k-particle job)"),

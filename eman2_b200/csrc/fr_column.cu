@@ -465,7 +465,10 @@ __device__ __forceinline__ void column_work(const Smem3 &S, const float *M, int 
           f0 = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
         }
       }
-      for (int k = k0; k <= k1; k++) {
+      // the window's taps along A inside the tile (the rest belong to the
+      // neighbouring tile's work item): a predicated straight line for the
+      // 2-tap windows, a loop for gauss_5's 6 (its unrolled form is slower)
+      auto tap = [&](int k) {
         float vre, vim, vw;
         if (MODE == MODE_GAUSS2 || MODE == MODE_GAUSS5) {
           const float d = __fsub_rn((float)k, pa);
@@ -500,13 +503,22 @@ __device__ __forceinline__ void column_work(const Smem3 &S, const float *M, int 
           else u.y += vim;
           u.z += vw;
         } else {
-          if (origin) continue;
+          if (origin) return;
           u.x += vre;
           u.y -= vim;
           const bool xzero = (A == 0) ? (k == 0) : xzero_col;
           if (!xzero) u.z += vw;
         }
         *cell = u;
+      };
+      if (K <= 2) {
+#pragma unroll
+        for (int j = 0; j < K; j++) {
+          const int k = a0 + j;
+          if (k >= k0 && k <= k1) tap(k);
+        }
+      } else {
+        for (int k = k0; k <= k1; k++) tap(k);
       }
     }
   }
