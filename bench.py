@@ -147,6 +147,17 @@ def load_traffic(workload: str, batch: int):
         return None
 
 
+def update_peaks():
+    """Measured scattered-update roofs on this device (taps/s): shared-memory
+    float4 read-modify-write, shared-memory atomics, L2 reductions."""
+    from eman2_b200 import _lib
+    lib = _lib.load()
+    a, b, c = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+    if lib.fr_update_peaks(ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)) != 0:
+        return None
+    return {"smem_rmw": a.value, "smem_atom": b.value, "l2_red": c.value}
+
+
 # ------------------------------------------------------------------ CPU baseline
 def cpu_sample(wl: dict, seed: int, budget_s: float = 15.0, max_n: int = 64, threads: int = 0):
     """The oracle's FP32 restatement (-O3 -ffast-math, OpenMP with private
@@ -177,59 +188,126 @@ def cpu_sample(wl: dict, seed: int, budget_s: float = 15.0, max_n: int = 64, thr
 
 
 # ------------------------------------------------------------------ serving
-def run_serving(dev, seed: int = 4242, nreq: int = 12, rate: float = 4.0, max_particles: int = 4000):
-    """A short Poisson stream of reconstruction requests (the served form):
-    boxes {64, 128, 192} padded x1.5, particle counts log-uniform over
-    [500, max_particles], sym c1/c4/d7, chunks of 512, arrivals at `rate`/s.
-    Returns p50/p99 latency and particle-slices/s, and the same requests run
-    one after another through the plain per-job path for comparison."""
-    import torch
-
-    from eman2_b200 import FourierReconstructor
+def serving_requests(dev, seed: int, nreq: int, rate: float, max_particles: int, chunk: int):
+    """A seeded stream of reconstruction requests: boxes {64, 128, 192, 256}
+    padded x1.5, particle counts log-uniform over [1000, max_particles], sym
+    c1/c4/d7, gauss_2, CTF, chunks of `chunk`; Poisson arrivals at `rate`/s."""
     from eman2_b200.particles import particle_meta
-    from eman2_b200.server import GpuExecutor, Request, Scheduler, Server
+    from eman2_b200.server import Request
     from eman2_b200.synth import make_particles
     rng = np.random.default_rng(seed)
-    pools = {}
-    for box in (64, 128, 192):
-        ps = make_particles(box, 1024, seed=seed + box, snr=0.05, shift=4.0, weights=(0.5, 1.0),
-                            ctf=True, device=dev)
-        pools[box] = ps
+    boxes = (64, 128, 192, 256)
+    pools = {box: make_particles(box, 1024, seed=seed + box, snr=0.05, shift=4.0,
+                                 weights=(0.5, 1.0), ctf=True, device=dev) for box in boxes}
     reqs, t = [], 0.0
     for k in range(nreq):
-        box = int(rng.choice([64, 128, 192]))
-        N = box * 3 // 2
-        n = int(np.exp(rng.uniform(np.log(500), np.log(max_particles))))
+        box = int(rng.choice(boxes))
+        n = int(np.exp(rng.uniform(np.log(1000), np.log(max_particles))))
         sym = str(rng.choice(["c1", "c4", "d7"]))
         ps = pools[box]
         chunks = []
-        for a in range(0, n, 512):
-            b = min(n, a + 512)
-            idx = np.arange(a, b) % 1024
+        for a in range(0, n, chunk):
+            idx = np.arange(a, min(n, a + chunk)) % 1024
             chunks.append((ps.images[idx], particle_meta(ps.rots[idx], ps.shifts[idx],
                                                          ps.weights[idx], defocus=ps.defocus[idx])))
         t += float(rng.exponential(1.0 / rate))
-        reqs.append(Request(k, {"size": [N] * 3, "sym": sym, "mode": "gauss_2"}, chunks, arrival=t))
+        reqs.append(Request(k, {"size": [box * 3 // 2] * 3, "sym": sym, "mode": "gauss_2"},
+                            chunks, arrival=t))
+    return reqs
+
+
+def fifo_latency(arrivals, service):
+    """Latencies of a single server taking requests one at a time in arrival order."""
+    free, lat = 0.0, []
+    for a, s in sorted(zip(arrivals, service)):
+        done = max(free, a) + s
+        lat.append(done - a)
+        free = done
+    return lat
+
+
+def run_serving(dev, seed: int = 4242, nreq: int = 12, rate: float = 4.0,
+                max_particles: int = 8000, chunk: int = 2048, plain_sample: int = 24):
+    """The served form against the plain per-job GPU path on one request stream.
+    Served: continuous batching (fr_insert_particles_multi per tick over every
+    active job), measured saturated (all requests at t=0: throughput) and
+    under Poisson arrivals (p50/p99 latency).  Plain: each request through its
+    own FourierReconstructor with one insert call per particle (the drop-in
+    insert_slice form), timed on `plain_sample` particles per request and
+    scaled to its count; its latency is that of a single FIFO server given
+    those service times and the same arrivals."""
+    import dataclasses
+
+    import torch
+
+    from eman2_b200 import FourierReconstructor, _lib
+    from eman2_b200.server import GpuExecutor, Scheduler, Server
+    reqs = serving_requests(dev, seed, nreq, rate, max_particles, chunk)
+    at0 = [dataclasses.replace(r, arrival=0.0) for r in reqs]
+    parts = sum(r.particles for r in reqs)
+    budget = int(torch.cuda.mem_get_info()[0] * 0.5)
+    exe = GpuExecutor(doift=False)
+    Server(Scheduler(budget, max_active=16), exe).run(at0)            # warm-up (untimed)
     torch.cuda.synchronize()
-    sched = Scheduler(hbm_budget=int(torch.cuda.mem_get_info()[0] * 0.6), max_active=16)
-    res = Server(sched, GpuExecutor(doift=False)).run(reqs)
-    slices = sum(r.particles for r in reqs)
-    # plain per-job path: each request alone, one insert call per chunk
-    t0 = time.perf_counter()
-    for r in reqs:
+    sat = Server(Scheduler(budget, max_active=16), exe).run(at0)
+    torch.cuda.synchronize()
+    poi = Server(Scheduler(budget, max_active=16), exe).run(reqs)
+    torch.cuda.synchronize()
+    exe.close()
+
+    def per_job(r, k=None, schedule="scatter"):
+        """Seconds for request r alone: setup, insert (k particles one per
+        call, or every chunk whole when k is None), finish."""
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
         rec = FourierReconstructor(r.params)
         rec.setup()
-        for img, meta in r.chunks:
-            rec.insert_particles(img, meta, schedule="scatter")
+        t1 = time.perf_counter()
+        if k is None:
+            for img, meta in r.chunks:
+                rec.insert_particles(img, meta, schedule=schedule)
+        else:
+            img, meta = r.chunks[0]
+            sz = ctypes.sizeof(_lib.fr_particle)
+            for i in range(min(k, len(meta))):
+                one = (_lib.fr_particle * 1).from_address(ctypes.addressof(meta) + i * sz)
+                rec.insert_particles(img[i:i + 1], one, schedule=schedule)
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
         rec.finish(False)
+        t3 = time.perf_counter()
         rec.close()
-    torch.cuda.synchronize()
-    plain_s = time.perf_counter() - t0
-    return {"requests": res["requests"], "p50_s": res["p50_s"], "p99_s": res["p99_s"],
-            "particle_slices_per_s": slices / res["wall_s"], "wall_s": res["wall_s"],
-            "plain_per_job_particle_slices_per_s": slices / plain_s,
-            "stream": f"{nreq} requests, Poisson {rate}/s, boxes 64/128/192 x1.5, "
-                      f"500-{max_particles} particles, c1/c4/d7, gauss_2, chunks of 512"}
+        return (t1 - t0) + (t3 - t2), t2 - t1
+
+    for r in reqs[:4]:
+        per_job(r, 4)                                                  # warm-up
+    service = []
+    for r in reqs:
+        fixed, ins = per_job(r, plain_sample)
+        service.append(fixed + ins * r.particles / min(plain_sample, r.particles))
+    chunked = sum(sum(per_job(r, None, "auto")) for r in reqs)
+    plain_lat = fifo_latency([r.arrival for r in reqs], service)
+    served_sat = parts / sat["wall_s"]
+    plain_rate = parts / sum(service)
+    return {
+        "served": {"p50_s": poi["p50_s"], "p99_s": poi["p99_s"],
+                   "particle_slices_per_s_saturated": served_sat,
+                   "particle_slices_per_s_poisson": parts / poi["wall_s"],
+                   "ticks_saturated": sat["ticks"], "requests": poi["requests"]},
+        "plain_per_particle": {"particle_slices_per_s": plain_rate,
+                               "p50_s": percentile(plain_lat, 50), "p99_s": percentile(plain_lat, 99),
+                               "sample": f"{plain_sample} particles per request, scaled to its count; "
+                                         "latency from a FIFO single server under the same arrivals"},
+        "per_job_chunked": {"particle_slices_per_s": parts / chunked,
+                            "note": f"each request alone, one insert call per chunk of {chunk}"},
+        "speedup_served_vs_plain": served_sat / plain_rate,
+        "stream": f"{nreq} requests, Poisson {rate}/s, boxes 64/128/192/256 x1.5, "
+                  f"1000-{max_particles} particles, c1/c4/d7, gauss_2, CTF, chunks of {chunk}",
+    }
+
+
+def percentile(v, q):
+    return float(np.percentile(np.asarray(v, np.float64), q)) if len(v) else None
 
 
 # ------------------------------------------------------------------ GPU run
@@ -376,6 +454,8 @@ def main():
     traffic = load_traffic(args.workload, args.batch)
     p = pixels_per_slice(N)
     taps_per = S * p * (216 if wl["mode"] == "gauss_5" else 8 if wl["mode"] == "gauss_2" else 1)
+    taps_s = taps_per * args.batch / (gms / 1e3)
+    upd = update_peaks()
     line = {
         "metric": metric, "value": value, "unit": "particle-slices/s", "n_gpus": ws,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
@@ -390,16 +470,23 @@ def main():
                      "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
                      "kernel": kname,
                      "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": gms},
-        "taps": {"per_particle_upper": taps_per,
-                 "per_s_upper": taps_per * args.batch / (gms / 1e3)},
+        "taps": {"per_particle_upper": taps_per, "per_s_upper": taps_s},
         "clocks": clk,
     }
+    if upd is not None:
+        # the binding roof: the rate of the accumulator update the kernel uses
+        key = "smem_rmw" if st["gather_launches"] > 0 else "l2_red"
+        line["update_roofline"] = {
+            "bound": {"smem_rmw": "shared-memory float4 read-modify-write",
+                      "l2_red": "L2 red.global.add.f32 (3 per tap)"}[key],
+            "achieved": taps_s, "peak": upd[key], "unit": "taps/s", "frac": taps_s / upd[key],
+            "peaks_measured": upd, "taps": "upper bound S*p(N)*window"}
     if plain is not None:
         line["plain_gpu"] = {"value": plain, "unit": "particle-slices/s", "sample": args.plain,
                              "speedup_batched_vs_plain": value / plain}
     if not args.no_serve and ws == 1:
         import torch
-        line["latency"] = run_serving(torch.device("cuda", local))
+        line["serving"] = run_serving(torch.device("cuda", local))
     if not args.no_cpu and ws == 1:
         v, n, thr, secs = cpu_sample(wl, seed=7000)
         line["cpu_baseline"] = {"value": v, "unit": "particle-slices/s", "cores": thr,

@@ -48,6 +48,7 @@ SIGNATURES = {
     "fr_create": ([ctypes.POINTER(fr_params), ctypes.POINTER(_P)], ctypes.c_int),
     "fr_destroy": ([_P], ctypes.c_int),
     "fr_set_stream": ([_P, _P], ctypes.c_int),
+    "fr_get_stream": ([_P, _P], ctypes.c_int),
     "fr_setup": ([_P], ctypes.c_int),
     "fr_setup_seed": ([_P, _P, ctypes.c_float], ctypes.c_int),
     "fr_setup_seedandweights": ([_P, _P, _P], ctypes.c_int),
@@ -82,6 +83,7 @@ SIGNATURES = {
     "fr_autotune": ([ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _I, _F],
                     ctypes.c_int),
     "fr_set_tile": ([ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+    "fr_update_peaks": ([_P, _P, _P], ctypes.c_int),
     "fr_insert_slices_noalloc": ([_P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_char_p,
                                   _P, _P, _P, _P, _P], ctypes.c_int),
 }

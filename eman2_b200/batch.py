@@ -15,7 +15,7 @@ import numpy as np
 
 from . import _lib
 from .emdata import EMData
-from .reconstructor import FourierReconstructor, _host_or_device
+from .reconstructor import FourierReconstructor, _host_or_device, join_streams, library_stream
 
 
 def insert_particles_multi(recons, images, metas, stream=None):
@@ -31,7 +31,8 @@ def insert_particles_multi(recons, images, metas, stream=None):
     counts = (ctypes.c_int * nj)(*[int(a.shape[0]) for a in keep])
     metas_p = (ctypes.c_void_p * nj)(*[ctypes.cast(m, ctypes.c_void_p).value for m in metas])
     st = ctypes.c_void_p(stream.cuda_stream) if stream is not None else None
-    _lib.check(lib.fr_insert_particles_multi(handles, nj, imgs, boxes, counts, metas_p, st))
+    with join_streams(st.value if st is not None else library_stream(recons[0].handle), *keep):
+        _lib.check(lib.fr_insert_particles_multi(handles, nj, imgs, boxes, counts, metas_p, st))
 
 
 class BatchReconstructor:

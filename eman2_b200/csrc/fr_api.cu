@@ -288,6 +288,17 @@ int check_state(fr_recon *r) {
   return FR_OK;
 }
 
+int stream_enter(fr_recon *r, cudaStream_t st) {
+  if (r->last && r->last != st) CU(cudaStreamWaitEvent(st, r->done, 0));
+  return FR_OK;
+}
+
+int stream_leave(fr_recon *r, cudaStream_t st) {
+  CU(cudaEventRecord(r->done, st));
+  r->last = st;
+  return FR_OK;
+}
+
 // Builds the job view for the insertion kernels.
 InsertJob make_job(fr_recon *r, const float2 *slices, const float *t3d, const float *pw,
                           int np) {
@@ -395,7 +406,6 @@ int insert_device(fr_recon *r, const float2 *d_slices, const float *d_t3d, const
       TRY(r->s_work.ensure(sizeof(int4) * std::max<size_t>(1, work.size())));
       CU(cudaMemcpyAsync(r->s_work.p, work.data(), sizeof(int4) * work.size(),
                          cudaMemcpyHostToDevice, st));
-      CU(cudaStreamSynchronize(st));
       r->work_np = nsl;
       r->nwork = (int)work.size();
     }
@@ -406,7 +416,6 @@ int insert_device(fr_recon *r, const float2 *d_slices, const float *d_t3d, const
     TRY(r->s_work.ensure(sizeof(int2) * std::max<size_t>(1, work.size())));
     CU(cudaMemcpyAsync(r->s_work.p, work.data(), sizeof(int2) * work.size(),
                        cudaMemcpyHostToDevice, st));
-    CU(cudaStreamSynchronize(st));
     r->work_np = -2;
   }
   TRY(r->s_jobs.ensure(sizeof(InsertJob)));
@@ -436,9 +445,9 @@ int insert_device(fr_recon *r, const float2 *d_slices, const float *d_t3d, const
     g_insert_ms += b;
     for (auto &e : ev) cudaEventDestroy(e);
   }
-  // The job struct staged above must outlive the launch: keep the copy in
-  // pinned-order by synchronising before the next reuse of s_jobs.
-  CU(cudaStreamSynchronize(st));
+  // Host-side sources above (work list, job struct) are pageable: the copies
+  // have taken them by the time cudaMemcpyAsync returns.  Later calls reuse
+  // the scratch in stream order (stream_enter for another stream).
   return FR_OK;
 }
 
@@ -501,12 +510,9 @@ int prologue_chunk(fr_recon *r, const float *d_raw, int n, int box, const fr_par
   if (any_ctf) {
     TRY(r->s_spec.ensure(sizeof(cufftComplex) * spec * n));
     TRY(r->s_img2.ensure(sizeof(float) * img * n));
-    cufftHandle f, b;
-    TRY(r->plans.get2d(true, N, n, st, &f));
-    TRY(r->plans.get2d(false, N, n, st, &b));
-    CUFFT(cufftExecR2C(f, r->s_img.as<cufftReal>(), r->s_spec.as<cufftComplex>()));
+    TRY(r->plans.exec2d(true, N, n, r->s_img.p, r->s_spec.p, st));
     CU(launch_ctf_flip_dev(r->s_spec.as<cufftComplex>(), r->s_ctf.p, n, N, st));
-    CUFFT(cufftExecC2R(b, r->s_spec.as<cufftComplex>(), r->s_img2.as<cufftReal>()));
+    TRY(r->plans.exec2d(false, N, n, r->s_spec.p, r->s_img2.p, st));
     img_on = r->s_img2.as<float>();
   }
   CU(launch_edge_mean(r->s_img.as<float>(), img_on, any_ctf ? r->s_ctf.p : nullptr, n, N,
@@ -518,9 +524,7 @@ int prologue_chunk(fr_recon *r, const float *d_raw, int n, int box, const fr_par
   CU(launch_shift_corner(r->s_img.as<float>(), img_on, any_ctf ? r->s_ctf.p : nullptr,
                          r->s_mean.as<float>(), r->s_txy.as<float>(), 2, n, N, scale,
                          r->s_spec.as<float>(), st));
-  cufftHandle f;
-  TRY(r->plans.get2d(true, N, n, st, &f));
-  CUFFT(cufftExecR2C(f, r->s_spec.as<cufftReal>(), r->s_slices.as<cufftComplex>()));
+  TRY(r->plans.exec2d(true, N, n, r->s_spec.p, r->s_slices.p, st));
   TRY(r->s_t3d.ensure(sizeof(float) * 9 * (size_t)n * r->nsym));
   CU(launch_compose(r->s_rot.as<float>(), r->d_sym.as<float>(), n, r->nsym, r->s_t3d.as<float>(),
                     st));
@@ -613,6 +617,11 @@ int fr_create(const fr_params *p, fr_recon **out) {
     return fail(FR_ECUDA, "cudaStreamCreate failed: %s", cudaGetErrorString(cudaGetLastError()));
   }
   r->stream = r->own;
+  if (cudaEventCreateWithFlags(&r->done, cudaEventDisableTiming) != cudaSuccess) {
+    cudaStreamDestroy(r->own);
+    delete r;
+    return fail(FR_ECUDA, "cudaEventCreate failed: %s", cudaGetErrorString(cudaGetLastError()));
+  }
   consts();
   r->geom = get_geom(r->N, p->corners);
   *out = r;
@@ -623,12 +632,14 @@ int fr_destroy(fr_recon *r) {
   if (!r) return FR_OK;
   {
     std::lock_guard<std::mutex> lk(r->mu);
+    if (r->last) cudaEventSynchronize(r->done);
     if (r->stream) cudaStreamSynchronize(r->stream);
     DevBuf *bufs[] = {&r->vol_data, &r->vol_norm, &r->d_sym, &r->s_in, &r->s_slices, &r->s_rot,
                       &r->s_w, &r->s_t3d, &r->s_img, &r->s_img2, &r->s_spec, &r->s_ctf,
                       &r->s_mean, &r->s_txy, &r->s_out, &r->s_ssnr, &r->s_jobs, &r->s_work,
                       &r->s_counter};
     for (DevBuf *b : bufs) b->release();
+    if (r->done) cudaEventDestroy(r->done);
     if (r->own) cudaStreamDestroy(r->own);
   }
   delete r;
@@ -642,6 +653,12 @@ int fr_set_stream(fr_recon *r, void *stream) {
   return FR_OK;
 }
 
+int fr_get_stream(const fr_recon *r, void **stream) {
+  if (!r || !stream) return fail(FR_ENULL, "null argument");
+  *stream = (void *)r->stream;
+  return FR_OK;
+}
+
 int fr_get_size(const fr_recon *r, int *N) {
   if (!r || !N) return fail(FR_ENULL, "null argument");
   *N = r->N;
@@ -651,6 +668,7 @@ int fr_get_size(const fr_recon *r, int *N) {
 int fr_setup(fr_recon *r) {
   if (!r) return fail(FR_ENULL, "null handle");
   std::lock_guard<std::mutex> lk(r->mu);
+  TRY(stream_enter(r, r->stream));
   TRY(alloc_volume(r));
   CU(cudaMemsetAsync(r->vol_data.p, 0, vol_floats(r->N) * sizeof(float), r->stream));
   CU(cudaMemsetAsync(r->vol_norm.p, 0, norm_floats(r->N) * sizeof(float), r->stream));
@@ -668,6 +686,7 @@ int fr_setup_seed(fr_recon *r, const float *seed, float seed_weight) {
   if (!r) return fail(FR_ENULL, "null handle");
   if (!seed) return fail(FR_ENULL, "null seed volume");
   std::lock_guard<std::mutex> lk(r->mu);
+  TRY(stream_enter(r, r->stream));
   TRY(alloc_volume(r));
   const void *d = nullptr;
   TRY(to_device(seed, vol_floats(r->N) * sizeof(float), r->s_in, r->stream, &d));
@@ -682,6 +701,7 @@ int fr_setup_seedandweights(fr_recon *r, const float *seed, const float *weights
   if (!r) return fail(FR_ENULL, "null handle");
   if (!seed || !weights) return fail(FR_ENULL, "null seed or weight volume");
   std::lock_guard<std::mutex> lk(r->mu);
+  TRY(stream_enter(r, r->stream));
   TRY(alloc_volume(r));
   const cudaMemcpyKind k1 = is_device_ptr(seed) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
   const cudaMemcpyKind k2 = is_device_ptr(weights) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
@@ -695,6 +715,7 @@ int fr_setup_seedandweights(fr_recon *r, const float *seed, const float *weights
 int fr_clear(fr_recon *r) {
   TRY(check_state(r));
   std::lock_guard<std::mutex> lk(r->mu);
+  TRY(stream_enter(r, r->stream));
   CU(cudaMemsetAsync(r->vol_data.p, 0, vol_floats(r->N) * sizeof(float), r->stream));
   CU(cudaMemsetAsync(r->vol_norm.p, 0, norm_floats(r->N) * sizeof(float), r->stream));
   CU(cudaStreamSynchronize(r->stream));
@@ -712,9 +733,7 @@ static int preprocess_device(fr_recon *r, const float *d_imgs, int n, const floa
   const float scale = sqrtf(inv * (float)(N + 2));
   CU(launch_shift_corner(d_imgs, nullptr, nullptr, nullptr, d_txy, txy_stride, n, N, scale,
                          r->s_img2.as<float>(), st));
-  cufftHandle plan;
-  TRY(r->plans.get2d(true, N, n, st, &plan));
-  CUFFT(cufftExecR2C(plan, r->s_img2.as<cufftReal>(), reinterpret_cast<cufftComplex *>(d_out_slices)));
+  TRY(r->plans.exec2d(true, N, n, r->s_img2.p, d_out_slices, st));
   return FR_OK;
 }
 
@@ -725,6 +744,7 @@ int fr_preprocess_slices(fr_recon *r, const float *imgs, int n, const float *inv
   if (n == 0) return FR_OK;
   if (!imgs || !out_slices) return fail(FR_ENULL, "null image or output");
   std::lock_guard<std::mutex> lk(r->mu);
+  TRY(stream_enter(r, r->stream));
   const int N = r->N;
   const void *d_in = nullptr, *d_t = nullptr;
   TRY(to_device(imgs, sizeof(float) * (size_t)n * N * N, r->s_in, r->stream, &d_in));
@@ -748,6 +768,7 @@ int fr_insert_slices(fr_recon *r, const float *slices, int n, const float *rot, 
   if (n == 0) return FR_OK;
   if (!slices || !rot || !weights) return fail(FR_ENULL, "EMData pointer (input image) is NULL");
   std::lock_guard<std::mutex> lk(r->mu);
+  TRY(stream_enter(r, r->stream));
   const int N = r->N;
   cudaStream_t st = r->stream;
   // insert_slice (libEM/reconstructor.cpp:1080-1090): usessnr turns the weight
@@ -784,7 +805,10 @@ int fr_insert_slices(fr_recon *r, const float *slices, int n, const float *rot, 
                     st));
   TRY(insert_device(r, (const float2 *)d_sl, r->s_t3d.as<float>(), r->s_w.as<float>(), n, schedule,
                     (const float *)d_ss, nssnr));
-  CU(cudaStreamSynchronize(st));
+  TRY(stream_leave(r, st));
+  // Host sources may be pinned, read by DMA after the call returns: finish
+  // those reads before handing the buffers back to the caller.
+  if (d_sl != slices || d_rot != rot || (use_ssnr && d_ss != ssnr)) CU(cudaStreamSynchronize(st));
   return FR_OK;
 }
 
@@ -795,6 +819,7 @@ int fr_insert_particles(fr_recon *r, const float *imgs, int n, int box, const fr
   if (n == 0) return FR_OK;
   if (!imgs || !meta) return fail(FR_ENULL, "EMData pointer (input image) is NULL");
   std::lock_guard<std::mutex> lk(r->mu);
+  TRY(stream_enter(r, r->stream));
   const int N = r->N;
   // Chunk so the per-chunk scratch (about 5 N^2 floats per particle) stays near 8 GiB.
   const size_t per = (size_t)N * N * 4 * 5 + (size_t)box * box * 4;
@@ -812,7 +837,8 @@ int fr_insert_particles(fr_recon *r, const float *imgs, int n, int box, const fr
     }
     TRY(particles_chunk(r, d_raw, c, box, meta + p0, schedule));
   }
-  CU(cudaStreamSynchronize(r->stream));
+  TRY(stream_leave(r, r->stream));
+  if (!dev) CU(cudaStreamSynchronize(r->stream));   // host images: see fr_insert_slices
   return FR_OK;
 }
 
@@ -827,6 +853,7 @@ int fr_determine_slice_agreement(fr_recon *r, const float *slices, int n, const 
                 "class_ssnr: sub=True inserts the slice through the SSNR path, which needs the "
                 "class_ssnr attribute (NotExistingObjectException in the reference)");
   std::lock_guard<std::mutex> lk(r->mu);
+  TRY(stream_enter(r, r->stream));
   const int N = r->N;
   cudaStream_t st = r->stream;
   const void *d_sl = nullptr, *d_rot = nullptr, *d_w = nullptr;
@@ -853,6 +880,7 @@ int fr_projection(fr_recon *r, const float *rot, float *out_slice) {
   TRY(check_state(r));
   if (!rot || !out_slice) return fail(FR_ENULL, "null argument");
   std::lock_guard<std::mutex> lk(r->mu);
+  TRY(stream_enter(r, r->stream));
   const int N = r->N;
   cudaStream_t st = r->stream;
   TRY(r->s_rot.ensure(sizeof(float) * 9));
@@ -869,6 +897,7 @@ int fr_projection(fr_recon *r, const float *rot, float *out_slice) {
 int fr_get_accumulators(fr_recon *r, float *data, float *norm) {
   TRY(check_state(r));
   std::lock_guard<std::mutex> lk(r->mu);
+  TRY(stream_enter(r, r->stream));
   TRY(check_device_error(r));
   if (data) TRY(from_device(data, r->vol_data.p, vol_floats(r->N) * sizeof(float), r->stream));
   if (norm) TRY(from_device(norm, r->vol_norm.p, norm_floats(r->N) * sizeof(float), r->stream));
@@ -878,6 +907,7 @@ int fr_get_accumulators(fr_recon *r, float *data, float *norm) {
 int fr_finish(fr_recon *r, int doift, float *out, float *normout) {
   TRY(check_state(r));
   std::lock_guard<std::mutex> lk(r->mu);
+  TRY(stream_enter(r, r->stream));
   const int N = r->N;
   cudaStream_t st = r->stream;
   TRY(check_device_error(r));

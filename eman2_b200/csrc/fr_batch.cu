@@ -41,10 +41,23 @@ int default_tile(int mode, int N, int nsym, int np) {
 }  // namespace fr
 
 // ------------------------------------------------------------------ batch
+namespace fr {
+// Device copies of a batched launch's job table and work list.
+struct BatchScratch {
+  DevBuf d_jobs, d_work, d_counter;
+  cudaEvent_t done = nullptr;     // after the last launch that read this scratch
+  cudaStream_t last = nullptr;
+  ~BatchScratch() {
+    if (done) { cudaEventSynchronize(done); cudaEventDestroy(done); }
+  }
+};
+}  // namespace fr
+
 struct fr_batch {
   std::vector<fr_recon *> jobs;
   cudaStream_t own = nullptr, stream = nullptr;
   int tile = -1;
+  fr::BatchScratch *bs = nullptr;
   std::mutex mu;
 };
 
@@ -81,6 +94,7 @@ int fr_batch_create(const fr_params *jobs, int njobs, fr_batch **out) {
 int fr_batch_destroy(fr_batch *b) {
   if (!b) return FR_OK;
   cudaStreamSynchronize(b->stream);
+  delete b->bs;
   for (fr_recon *r : b->jobs) fr_destroy(r);
   if (b->own) cudaStreamDestroy(b->own);
   delete b;
@@ -99,10 +113,6 @@ int fr_batch_set_stream(fr_batch *b, void *stream) {
 
 namespace fr {
 
-struct BatchScratch {
-  DevBuf d_jobs, d_work, d_counter;
-};
-
 // Inserts, for every job, counts[j] particles through the caller pipeline;
 // all jobs' insertion work goes through one persistent launch per round.
 // Every job runs on `st` for the duration of the call.
@@ -118,11 +128,18 @@ static int batch_insert(std::vector<fr_recon *> &jobs, BatchScratch &bs, int til
     }
     ~StreamSwap() { for (size_t i = 0; i < j.size(); i++) j[i]->stream = saved[i]; }
   } swap(jobs, st);
+  bool host_src = false;
   for (int j = 0; j < nj; j++) {
     TRY(check_state(jobs[j]));
     if (counts[j] < 0 || (counts[j] > 0 && (boxes[j] <= 0 || !imgs[j] || !meta[j])))
       return fail(FR_EINVAL_PARAM, "job %d: bad particle count, box or buffers", j);
+    if (counts[j] > 0 && !is_device_ptr(imgs[j])) host_src = true;
   }
+  // Work goes to `st` after each handle's and the scratch's earlier work on
+  // other streams; the call returns once everything is enqueued.
+  if (!bs.done) CU(cudaEventCreateWithFlags(&bs.done, cudaEventDisableTiming));
+  if (bs.last && bs.last != st) CU(cudaStreamWaitEvent(st, bs.done, 0));
+  for (int j = 0; j < nj; j++) TRY(stream_enter(jobs[j], st));
   // Rounds of at most `chunk` particles per job, so scratch stays bounded.
   const int chunk = 4096;
   int rounds = 0;
@@ -212,8 +229,11 @@ static int batch_insert(std::vector<fr_recon *> &jobs, BatchScratch &bs, int til
                        (int)work.size(), tile, bs.d_counter.as<int>(), max_mode, st));
     }
     for (const InsertJob &J : hj) TRY(run_scatter(J, true, st));
-    CU(cudaStreamSynchronize(st));
   }
+  CU(cudaEventRecord(bs.done, st));
+  bs.last = st;
+  for (int j = 0; j < nj; j++) TRY(stream_leave(jobs[j], st));
+  if (host_src) CU(cudaStreamSynchronize(st));   // host images may be pinned: read them before returning
   return FR_OK;
 }
 
@@ -225,10 +245,8 @@ int fr_batch_insert_particles(fr_batch *b, const float *const *imgs, const int *
                               const int *counts, const fr_particle *const *meta) {
   if (!b || !imgs || !boxes || !counts || !meta) return fail(FR_ENULL, "null argument");
   std::lock_guard<std::mutex> lk(b->mu);
-  BatchScratch bs;
-  int rc = batch_insert(b->jobs, bs, b->tile, b->stream, imgs, boxes, counts, meta);
-  bs.d_jobs.release(); bs.d_work.release(); bs.d_counter.release();
-  return rc;
+  if (!b->bs) b->bs = new BatchScratch();
+  return batch_insert(b->jobs, *b->bs, b->tile, b->stream, imgs, boxes, counts, meta);
 }
 
 int fr_insert_particles_multi(fr_recon *const *handles, int nh, const float *const *imgs,

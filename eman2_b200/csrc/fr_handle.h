@@ -93,6 +93,26 @@ struct PlanCache {
     *out = it->second;
     return FR_OK;
   }
+  // n batched 2-D transforms of size N (contiguous, unpadded) run as a
+  // binary decomposition into power-of-two batches (at most 1024), so the
+  // plans are shared by every chunk length instead of one plan per length.
+  int exec2d(bool forward, int N, int n, const void *in, void *out, cudaStream_t st) {
+    const size_t img = (size_t)N * N, spec = (size_t)N * (N / 2 + 1);
+    int done = 0;
+    while (done < n) {
+      int b = 1;
+      while (2 * b <= n - done && 2 * b <= 1024) b *= 2;
+      cufftHandle h;
+      int rc = get2d(forward, N, b, st, &h);
+      if (rc != FR_OK) return rc;
+      if (forward)
+        CUFFT(cufftExecR2C(h, (cufftReal *)in + done * img, (cufftComplex *)out + done * spec));
+      else
+        CUFFT(cufftExecC2R(h, (cufftComplex *)in + done * spec, (cufftReal *)out + done * img));
+      done += b;
+    }
+    return FR_OK;
+  }
   int get3d(int N, cudaStream_t st, cufftHandle *out) {
     if (!c2r3 || c2r3_N != N) {
       if (c2r3) cufftDestroy(c2r3);
@@ -138,12 +158,21 @@ struct fr_recon {
   std::vector<float> tile_dist;   // nearest-cell distance of each tile (column kernel)
   int tiles_tile = -1, tx = 0, ty = 0, tz = 0;
   int work_np = -1, nwork = 0;   // cached work list signature (slices) and size
+  // Insertion calls return once their work is enqueued.  `done` is recorded
+  // after the handle's last enqueued work on stream `last`; a call on another
+  // stream first makes that stream wait for it.
+  cudaEvent_t done = nullptr;
+  cudaStream_t last = nullptr;
   std::mutex mu;
 };
 
 
 namespace fr {
 int check_state(fr_recon *r);
+// Orders work enqueued on st after the handle's earlier work on other streams.
+int stream_enter(fr_recon *r, cudaStream_t st);
+// Marks the end of the handle's work enqueued so far on st.
+int stream_leave(fr_recon *r, cudaStream_t st);
 InsertJob make_job(fr_recon *r, const float2 *slices, const float *t3d, const float *pw, int np);
 int run_scatter(const InsertJob &j0, bool edge_only, cudaStream_t st);
 int insert_device(fr_recon *r, const float2 *d_slices, const float *d_t3d, const float *d_pw, int np,

@@ -63,6 +63,39 @@ def _host_or_device(a):
     return np.ascontiguousarray(a, np.float32)
 
 
+def library_stream(handle) -> int:
+    """cudaStream_t the handle's work goes to."""
+    out = ctypes.c_void_p()
+    _lib.check(_lib.load().fr_get_stream(handle, ctypes.byref(out)))
+    return out.value or 0
+
+
+class join_streams:
+    """Around an insertion call given CUDA tensors (the call returns before
+    its kernels finish): the library stream first waits for torch's current
+    stream, where the tensors were produced, and torch's current stream then
+    waits for the library's work, so memory torch frees and hands out again
+    is not rewritten before the kernels have read it."""
+
+    def __init__(self, stream_ptr: int, *arrays):
+        self.ts = [a for a in arrays if getattr(a, "is_cuda", False)]
+        self.ptr = stream_ptr
+
+    def __enter__(self):
+        if self.ts:
+            import torch
+            dev = self.ts[0].device
+            self.cur = torch.cuda.current_stream(dev)
+            self.ext = torch.cuda.ExternalStream(self.ptr, device=dev)
+            self.ext.wait_stream(self.cur)
+        return self
+
+    def __exit__(self, *exc):
+        if self.ts:
+            self.cur.wait_stream(self.ext)
+        return False
+
+
 def _rot_of(xf) -> np.ndarray:
     if isinstance(xf, Transform):
         return xf.rotation_block().astype(np.float32)
@@ -304,8 +337,9 @@ class FourierReconstructor:
         r = _host_or_device(rots)
         w = _host_or_device(weights)
         status = (ctypes.c_int * n)()
-        _lib.check(_lib.load().fr_insert_slices(self._h, _lib.ptr(s), n, _lib.ptr(r), _lib.ptr(w),
-                                                None, 0, status, _lib.SCHED[schedule]))
+        with join_streams(library_stream(self._h), s, r, w):
+            _lib.check(_lib.load().fr_insert_slices(self._h, _lib.ptr(s), n, _lib.ptr(r), _lib.ptr(w),
+                                                    None, 0, status, _lib.SCHED[schedule]))
         return list(status)
 
     def insert_particles(self, images, meta, schedule: str = "auto"):
@@ -317,9 +351,10 @@ class FourierReconstructor:
             self._require_setup()
         a = _host_or_device(images)
         n, box = int(a.shape[0]), int(a.shape[-1])
-        _lib.check(_lib.load().fr_insert_particles(self._h, _lib.ptr(a), n, box,
-                                                   ctypes.cast(meta, ctypes.c_void_p),
-                                                   _lib.SCHED[schedule]))
+        with join_streams(library_stream(self._h), a):
+            _lib.check(_lib.load().fr_insert_particles(self._h, _lib.ptr(a), n, box,
+                                                       ctypes.cast(meta, ctypes.c_void_p),
+                                                       _lib.SCHED[schedule]))
 
     def determine_slice_agreement(self, img, xform, weight: float = 1.0, sub: bool = True) -> int:
         """FourierReconstructor::determine_slice_agreement

@@ -169,20 +169,46 @@ class Server:
 
 class GpuExecutor:
     """Device execution for the scheduler: a resident FourierReconstructor per
-    job; each tick's chunks go through one fr_insert_particles_multi call."""
+    job; each tick's chunks go through one fr_insert_particles_multi call.
 
-    def __init__(self, doift: bool = False, stream=None):
+    Finished jobs' reconstructors return to a pool keyed by their parameters;
+    a later job with the same parameters takes one (setup() zeroes its
+    accumulators) and so reuses its volumes, FFT plans and scratch instead of
+    allocating them.  At most ``pool_bytes`` of idle volumes are kept."""
+
+    def __init__(self, doift: bool = False, stream=None, pool_bytes: int = 8 << 30):
         self.doift = doift
         self.stream = stream
+        self.pool_bytes = int(pool_bytes)
+        self.pool: dict = {}            # key -> [FourierReconstructor]
+        self.pooled = 0
+        self.reused = 0
+
+    @staticmethod
+    def _key(params: dict):
+        return tuple(sorted((k, tuple(v) if isinstance(v, (list, tuple)) else v)
+                            for k, v in params.items()))
 
     def create(self, params: dict):
         from .reconstructor import FourierReconstructor
-        r = FourierReconstructor(params)
+        key = self._key(params)
+        free = self.pool.get(key)
+        if free:
+            r = free.pop()
+            self.pooled -= r._pool_bytes
+            self.reused += 1
+        else:
+            r = FourierReconstructor(params)
+            r._pool_key, r._pool_bytes = key, footprint_bytes(params, 0, 0)
         r.setup()
         return r
 
     def insert(self, items):
         from .batch import insert_particles_multi
+        if self.stream is None:
+            # one stream for every tick: the ticks' launches queue back to back
+            import torch
+            self.stream = torch.cuda.Stream()
         recons = [h for h, _ in items]
         # a handle may appear once per call: group repeated jobs into rounds
         while items:
@@ -197,5 +223,17 @@ class GpuExecutor:
 
     def finish(self, handle):
         out = handle.finish(self.doift)
-        handle.close()
+        vol = handle._pool_bytes
+        if self.pooled + vol <= self.pool_bytes:
+            self.pool.setdefault(handle._pool_key, []).append(handle)
+            self.pooled += vol
+        else:
+            handle.close()
         return out
+
+    def close(self):
+        for free in self.pool.values():
+            for r in free:
+                r.close()
+        self.pool.clear()
+        self.pooled = 0

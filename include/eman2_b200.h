@@ -93,8 +93,17 @@ FR_API int fr_create(const fr_params *p, fr_recon **out);
 FR_API int fr_destroy(fr_recon *r);
 
 /* Binds the handle to an existing CUDA stream (cudaStream_t); 0 restores the
- * handle's own stream. */
+ * handle's own stream.  Insertion calls (fr_insert_slices,
+ * fr_insert_particles and the batched forms) return once their work is
+ * enqueued on that stream, after copying any host inputs; device inputs must
+ * stay valid until the stream reaches that point.  A call on another stream
+ * first waits for the handle's earlier work.  Calls that return results
+ * (agreement, accumulators, finish) synchronise. */
 FR_API int fr_set_stream(fr_recon *r, void *stream);
+
+/* The stream the handle's work goes to (cudaStream_t), for callers that
+ * order their own work against it.  No counterpart in the reference. */
+FR_API int fr_get_stream(const fr_recon *r, void **stream);
 
 /* FourierReconstructor::setup (libEM/reconstructor.cpp:730-818). */
 FR_API int fr_setup(fr_recon *r);
@@ -244,6 +253,14 @@ FR_API int fr_batch_get_accumulators(fr_batch *b, int job, float *data, float *n
 FR_API int fr_autotune(int N, int mode, int nsym, int nparticles, int *tile_out,
                        float *ms_out);
 FR_API int fr_set_tile(int N, int mode, int nsym, int tile);
+
+/* Measured roofs of the scattered accumulation, in taps/s (a tap adds a
+ * complex value and a weight to one voxel): conflict-free float4
+ * read-modify-write in shared memory (the column kernel's update), FP32
+ * atomicAdd to random shared-memory words, and FP32 red.global.add to an
+ * L2-resident buffer (the scatter schedule's update).  Runs three short
+ * microbenchmarks on the current device.  No counterpart in the reference. */
+FR_API int fr_update_peaks(double *smem_rmw_taps, double *smem_atom_taps, double *l2_red_taps);
 
 #ifdef __cplusplus
 }
