@@ -134,15 +134,16 @@ def load_peaks():
 
 
 def load_traffic(workload: str, batch: int):
-    """DRAM traffic of one gather launch from the committed ncu summary,
-    scaled to `batch` particles (traffic grows with the particles staged and
-    is flat in the volume term): None when no capture exists."""
-    path = os.path.join(ROOT, "profiles", "gather_traffic.json")
+    """DRAM bytes (read + write) of one insertion launch of this workload and
+    batch, from the committed ncu capture of the same bench command; None
+    when no capture of that size exists."""
+    path = os.path.join(ROOT, "profiles", "k_column3_dram.json")
     try:
         with open(path) as f:
-            d = json.load(f)
-        e = d[workload]
-        return float(e["fixed_bytes"]) + float(e["bytes_per_particle"]) * batch
+            e = json.load(f)[workload]
+        if int(e["particles_per_launch"]) != batch:
+            return None
+        return float(e["dram_bytes_read"]) + float(e["dram_bytes_write"])
     except Exception:
         return None
 
@@ -345,11 +346,13 @@ def run_gpu(args, wl, ws, rank, local):
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
+        torch.cuda.nvtx.range_push("timed")      # ncu --nvtx --nvtx-include timed/
         e0.record(stream)
         for _ in range(args.steps):
             step(d_imgs)
         e1.record(stream)
         e1.synchronize()
+        torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize()
     barrier(ws)
     ms = e0.elapsed_time(e1)
@@ -446,7 +449,9 @@ def main():
     V = (N // 2 + 1) * N * N
     alg_bytes = args.batch * (8 * (N // 2 + 1) * N + 64) + 24 * V
     if st["gather_launches"] > 0:
-        kname, gms = "k_column (gather schedule)", st["gather_ms"] / st["gather_launches"]
+        tile = args.tile if args.tile != -1 else 5          # the library's default: k_column3
+        kname = {5: "k_column3", 4: "k_column"}.get(tile, "k_gather") + " (gather schedule)"
+        gms = st["gather_ms"] / st["gather_launches"]
     else:
         kname, gms = "k_scatter", st["insert_ms"] / max(1, st["insert_launches"])
     achieved = alg_bytes / (gms / 1e3) / 1e9

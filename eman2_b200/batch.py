@@ -35,6 +35,28 @@ def insert_particles_multi(recons, images, metas, stream=None):
         _lib.check(lib.fr_insert_particles_multi(handles, nj, imgs, boxes, counts, metas_p, st))
 
 
+TILE_NAMES = {0: "gather 8x8x8", 1: "gather 16x8x8", 2: "gather 8x8x4", 3: "gather 16x16x4",
+              4: "column (staged)", 5: "column (barrier-free)", -2: "scatter"}
+
+
+def autotune(N: int, mode: str, nsym: int, nparticles: int = 256):
+    """Times every insertion schedule for (N, mode, nsym) on random slices and
+    records the fastest; batched and plain insertions of that shape use it
+    from then on.  Returns (tile id, {schedule name: ms})."""
+    lib = _lib.load()
+    tile = ctypes.c_int()
+    ms = (ctypes.c_float * 7)()
+    _lib.check(lib.fr_autotune(int(N), _lib.MODE_IDS[mode], int(nsym), int(nparticles),
+                               ctypes.byref(tile), ms))
+    names = [TILE_NAMES[i] for i in range(6)] + [TILE_NAMES[-2]]
+    return tile.value, dict(zip(names, list(ms)))
+
+
+def set_tile(N: int, mode: str, nsym: int, tile: int):
+    """Pins the schedule for (N, mode, nsym) (tile ids as TILE_NAMES; -1 clears)."""
+    _lib.check(_lib.load().fr_set_tile(int(N), _lib.MODE_IDS[mode], int(nsym), int(tile)))
+
+
 class BatchReconstructor:
     """A fixed set of reconstructions inserted together (fr_batch_*)."""
 

@@ -397,12 +397,20 @@ int insert_device(fr_recon *r, const float2 *d_slices, const float *d_t3d, const
   if (column) {
     // work items (job 0, tile, first slice of the block)
     if (r->work_np != nsl) {
+      // Slice-bucket-major order: every item of a bucket (slice_bucket;
+      // all block sizes divide it) before the next bucket, tiles nearest the
+      // origin (heaviest) first within a bucket.  The CTAs in flight then
+      // read one bucket's slices, mostly from L2, instead of each tile
+      // streaming every slice from HBM.
+      const int bucket = slice_bucket(r->N, r->nsym);
       std::vector<int4> work;
-      for (size_t ti = 0; ti < r->tiles.size(); ti++) {
-        const int blk = column_block(r->tile_dist[ti]);
-        for (int s0 = 0; s0 < nsl; s0 += blk)
-          work.push_back(make_int4(0, r->tiles[ti], s0, std::min(nsl, s0 + blk)));
-      }
+      for (int b0 = 0; b0 < nsl; b0 += bucket)
+        for (size_t ti = 0; ti < r->tiles.size(); ti++) {
+          const int blk = column_block(r->tile_dist[ti]);
+          const int b1 = std::min(nsl, b0 + bucket);
+          for (int s0 = b0; s0 < b1; s0 += blk)
+            work.push_back(make_int4(0, r->tiles[ti], s0, std::min(b1, s0 + blk)));
+        }
       TRY(r->s_work.ensure(sizeof(int4) * std::max<size_t>(1, work.size())));
       CU(cudaMemcpyAsync(r->s_work.p, work.data(), sizeof(int4) * work.size(),
                          cudaMemcpyHostToDevice, st));

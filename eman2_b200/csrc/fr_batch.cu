@@ -144,12 +144,17 @@ static int batch_insert(std::vector<fr_recon *> &jobs, BatchScratch &bs, int til
   const int chunk = 4096;
   int rounds = 0;
   for (int j = 0; j < nj; j++) rounds = std::max(rounds, (counts[j] + chunk - 1) / chunk);
-  const int tile = tile_pref >= 0 ? tile_pref : default_tile(0, 0, 0, 0);
-  const bool column = tile == kColumnTile || tile == kColumn3Tile;
+  // Each job's schedule: the caller's pin, else the autotuner's measurement
+  // for its (N, mode, nsym), else the barrier-free column kernel.  Jobs that
+  // share a schedule share one persistent launch per round.
+  auto job_tile = [&](const fr_recon *r) {
+    if (tile_pref != -1) return tile_pref;
+    const int t = tuned_tile(r->N, r->mode, r->nsym);
+    return t != -1 ? t : default_tile(r->mode, r->N, r->nsym, 0);
+  };
   for (int rd = 0; rd < rounds; rd++) {
     std::vector<InsertJob> hj;
-    std::vector<int> owner;
-    int max_mode = FR_MODE_NEAREST, maxN = 0;
+    std::vector<int> owner, jt;
     for (int j = 0; j < nj; j++) {
       fr_recon *r = jobs[j];
       const int p0 = rd * chunk;
@@ -161,74 +166,98 @@ static int batch_insert(std::vector<fr_recon *> &jobs, BatchScratch &bs, int til
       TRY(to_device(src, sizeof(float) * (size_t)c * box * box, r->s_in, st, &d_raw));
       TRY(prologue_chunk(r, (const float *)d_raw, c, box, meta[j] + p0));
       InsertJob J = make_job(r, r->s_slices.as<float2>(), r->s_t3d.as<float>(), r->s_w.as<float>(), c);
-      if (r->tiles_tile != tile) {
-        if (column)
+      const int tile = job_tile(r);
+      if (tile != kTunedScatter && r->tiles_tile != tile) {
+        if (tile == kColumnTile || tile == kColumn3Tile)
           column_tiles(r->N, r->mode, r->p.corners, r->tiles, r->tx, r->ty, r->tz, &r->tile_dist);
         else gather_tiles(r->N, r->mode, tile, r->p.corners, r->tiles, r->tx, r->ty, r->tz);
         r->tiles_tile = tile;
+        r->work_np = -1;
       }
       J.tiles_x = r->tx;
       J.tiles_y = r->ty;
       J.tiles_z = r->tz;
       hj.push_back(J);
       owner.push_back(j);
-      maxN = std::max(maxN, r->N);
-      if (r->mode == FR_MODE_GAUSS5) max_mode = FR_MODE_GAUSS5;
-      else if (max_mode != FR_MODE_GAUSS5 && r->mode != FR_MODE_NEAREST) max_mode = r->mode;
+      jt.push_back(tile);
     }
     if (hj.empty()) continue;
-    // Interleave every job's work items by estimated cost, heaviest first: the
-    // slices meeting a tile fall off with its distance from the origin (tiles
-    // are sorted by distance), times the slices in the item's block.
-    std::vector<std::pair<double, int4>> items;
-    for (size_t k = 0; k < hj.size(); k++) {
-      fr_recon *r = jobs[owner[k]];
-      const int nsl = hj[k].np * hj[k].nsym;
-      const double nt = (double)r->tiles.size();
-      for (size_t t = 0; t < r->tiles.size(); t++) {
-        const double frac = (double)t / std::max(1.0, nt);
-        const double fall = 1.0 / (1.0 + 8.0 * std::cbrt(frac) * r->N / 16.0);
-        if (column) {
-          const int blk = column_block(r->tile_dist[t]);
-          for (int s0 = 0; s0 < nsl; s0 += blk) {
-            const int len = std::min(blk, nsl - s0);
-            items.push_back({-len * fall, make_int4((int)k, r->tiles[t], s0, s0 + len)});
-          }
-        } else {
-          items.push_back({-nsl * fall, make_int4((int)k, r->tiles[t], 0, 0)});
-        }
-      }
-    }
-    std::stable_sort(items.begin(), items.end(),
-                     [](const std::pair<double, int4> &a, const std::pair<double, int4> &c) {
-                       return a.first < c.first;
-                     });
     TRY(bs.d_jobs.ensure(sizeof(InsertJob) * hj.size()));
     TRY(bs.d_counter.ensure(sizeof(int)));
     CU(cudaMemcpyAsync(bs.d_jobs.p, hj.data(), sizeof(InsertJob) * hj.size(),
                        cudaMemcpyHostToDevice, st));
-    if (column) {
-      std::vector<int4> work(items.size());
-      for (size_t i = 0; i < items.size(); i++) work[i] = items[i].second;
-      TRY(bs.d_work.ensure(sizeof(int4) * work.size()));
-      CU(cudaMemcpyAsync(bs.d_work.p, work.data(), sizeof(int4) * work.size(),
-                         cudaMemcpyHostToDevice, st));
-      if (tile == kColumn3Tile)
-        CU(launch_column3(bs.d_jobs.as<InsertJob>(), bs.d_work.as<int4>(), (int)work.size(),
-                          kColumnBlock, bs.d_counter.as<int>(), maxN, st));
-      else
-        CU(launch_column(bs.d_jobs.as<InsertJob>(), bs.d_work.as<int4>(), (int)work.size(),
-                         kColumnBlock, bs.d_counter.as<int>(), max_mode, st));
-    } else {
-      std::vector<int2> work(items.size());
-      for (size_t i = 0; i < items.size(); i++) work[i] = make_int2(items[i].second.x, items[i].second.y);
-      TRY(bs.d_work.ensure(sizeof(int2) * work.size()));
-      CU(cudaMemcpyAsync(bs.d_work.p, work.data(), sizeof(int2) * work.size(),
-                         cudaMemcpyHostToDevice, st));
-      CU(launch_gather(bs.d_jobs.as<InsertJob>(), hj.data(), (int)hj.size(), bs.d_work.as<int2>(),
-                       (int)work.size(), tile, bs.d_counter.as<int>(), max_mode, st));
+    std::vector<int> tiles_used(jt);
+    std::sort(tiles_used.begin(), tiles_used.end());
+    tiles_used.erase(std::unique(tiles_used.begin(), tiles_used.end()), tiles_used.end());
+    for (const int tile : tiles_used) {
+      if (tile == kTunedScatter) {
+        for (size_t k = 0; k < hj.size(); k++)
+          if (jt[k] == tile) TRY(run_scatter(hj[k], false, st));
+        continue;
+      }
+      const bool column = tile == kColumnTile || tile == kColumn3Tile;
+      int max_mode = FR_MODE_NEAREST, maxN = 0;
+      // Order the group's work items slice-bucket-major (slice_bucket per
+      // job, so the CTAs in flight share a bucket's slices in
+      // L2), and within a bucket by estimated cost, heaviest first: the slices
+      // meeting a tile fall off with its distance from the origin (tiles are
+      // sorted by distance), times the slices in the item's block.
+      std::vector<std::pair<double, int4>> items;
+      std::vector<int> bucket_of;
+      for (size_t k = 0; k < hj.size(); k++) {
+        if (jt[k] != tile) continue;
+        fr_recon *r = jobs[owner[k]];
+        maxN = std::max(maxN, r->N);
+        if (r->mode == FR_MODE_GAUSS5) max_mode = FR_MODE_GAUSS5;
+        else if (max_mode != FR_MODE_GAUSS5 && r->mode != FR_MODE_NEAREST) max_mode = r->mode;
+        const int nsl = hj[k].np * hj[k].nsym;
+        const double nt = (double)r->tiles.size();
+        for (size_t t = 0; t < r->tiles.size(); t++) {
+          const double frac = (double)t / std::max(1.0, nt);
+          const double fall = 1.0 / (1.0 + 8.0 * std::cbrt(frac) * r->N / 16.0);
+          if (column) {
+            const int blk = column_block(r->tile_dist[t]);
+            for (int s0 = 0; s0 < nsl; s0 += blk) {
+              const int len = std::min(blk, nsl - s0);
+              items.push_back({-len * fall, make_int4((int)k, r->tiles[t], s0, s0 + len)});
+            bucket_of.push_back(s0 / slice_bucket(r->N, r->nsym));
+            }
+          } else {
+            items.push_back({-nsl * fall, make_int4((int)k, r->tiles[t], 0, 0)});
+            bucket_of.push_back(0);
+          }
+        }
+      }
+      // bucket first (costs are below 1e4), then heaviest first
+      for (size_t i = 0; i < items.size(); i++) items[i].first += 1e12 * bucket_of[i];
+      std::stable_sort(items.begin(), items.end(),
+                       [](const std::pair<double, int4> &a, const std::pair<double, int4> &c) {
+                         return a.first < c.first;
+                       });
+      if (column) {
+        std::vector<int4> work(items.size());
+        for (size_t i = 0; i < items.size(); i++) work[i] = items[i].second;
+        TRY(bs.d_work.ensure(sizeof(int4) * std::max<size_t>(1, work.size())));
+        CU(cudaMemcpyAsync(bs.d_work.p, work.data(), sizeof(int4) * work.size(),
+                           cudaMemcpyHostToDevice, st));
+        if (tile == kColumn3Tile)
+          CU(launch_column3(bs.d_jobs.as<InsertJob>(), bs.d_work.as<int4>(), (int)work.size(),
+                            kColumnBlock, bs.d_counter.as<int>(), maxN, st));
+        else
+          CU(launch_column(bs.d_jobs.as<InsertJob>(), bs.d_work.as<int4>(), (int)work.size(),
+                           kColumnBlock, bs.d_counter.as<int>(), max_mode, st));
+      } else {
+        std::vector<int2> work(items.size());
+        for (size_t i = 0; i < items.size(); i++) work[i] = make_int2(items[i].second.x, items[i].second.y);
+        TRY(bs.d_work.ensure(sizeof(int2) * std::max<size_t>(1, work.size())));
+        CU(cudaMemcpyAsync(bs.d_work.p, work.data(), sizeof(int2) * work.size(),
+                           cudaMemcpyHostToDevice, st));
+        CU(launch_gather(bs.d_jobs.as<InsertJob>(), hj.data(), (int)hj.size(), bs.d_work.as<int2>(),
+                         (int)work.size(), tile, bs.d_counter.as<int>(), max_mode, st));
+      }
+      for (size_t k = 0; k < hj.size(); k++)
+        if (jt[k] == tile) TRY(run_scatter(hj[k], true, st));
     }
-    for (const InsertJob &J : hj) TRY(run_scatter(J, true, st));
   }
   CU(cudaEventRecord(bs.done, st));
   bs.last = st;
@@ -293,7 +322,8 @@ int fr_set_tile(int N, int mode, int nsym, int tile) {
 // Measures the gather schedule with every tile shape, and the scatter
 // schedule, on random slices of size N through random orientations; records
 // the fastest for (N, mode, nsym).  tile_out: chosen tile (-2 = scatter);
-// ms_out[kNumTiles+1]: per-candidate milliseconds (tiles, then scatter).
+// ms_out[kColumn3Tile+2]: per-candidate milliseconds (register tiles 0-3,
+// staged column 4, barrier-free column 5, then scatter).
 int fr_autotune(int N, int mode, int nsym, int nparticles, int *tile_out, float *ms_out) {
   if (nparticles <= 0) return fail(FR_EINVAL_PARAM, "nparticles must be positive");
   fr_params p;
@@ -331,8 +361,8 @@ int fr_autotune(int N, int mode, int nsym, int nparticles, int *tile_out, float 
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
-  for (int cand = 0; cand <= kNumTiles && rc == FR_OK; cand++) {
-    const bool scatter = cand == kNumTiles;
+  for (int cand = 0; cand <= kColumn3Tile + 1 && rc == FR_OK; cand++) {
+    const bool scatter = cand == kColumn3Tile + 1;
     r->tile = scatter ? -1 : cand;
     const int sched = scatter ? FR_SCHED_SCATTER : FR_SCHED_GATHER;
     // one warm-up call, then one timed call

@@ -248,8 +248,12 @@ FR_API int fr_insert_particles_multi(fr_recon *const *handles, int nh, const flo
 FR_API int fr_batch_finish(fr_batch *b, int job, int doift, float *out, float *normout);
 FR_API int fr_batch_get_accumulators(fr_batch *b, int job, float *data, float *norm);
 
-/* Tile shape / schedule selection for the gather insertion, measured on the
- * device and cached per (N, mode, nsym).  Returns the chosen tile index. */
+/* Schedule selection for the insertion, measured on the device with
+ * nparticles random slices and cached per (N, mode, nsym): candidates are the
+ * register-tile gather shapes 0-3, the staged column kernel (4), the
+ * barrier-free column kernel (5) and the atomic scatter (tile_out = -2).
+ * ms_out, if not NULL, receives 7 timings in that order.  fr_set_tile pins a
+ * choice (-1 clears it).  No counterpart in the reference. */
 FR_API int fr_autotune(int N, int mode, int nsym, int nparticles, int *tile_out,
                        float *ms_out);
 FR_API int fr_set_tile(int N, int mode, int nsym, int tile);

@@ -56,6 +56,30 @@ def test_batch_equals_each_job_alone(gpu):
     assert oracle.rel_l2(n, o.norm) < RTOL and oracle.rel_l2(d, o.data) < 2e-5
 
 
+def test_autotune_and_mixed_schedules_in_one_batch(gpu):
+    """The autotuner times all seven schedules; with each job pinned to a
+    different one, the batch still gives every job its alone result."""
+    from eman2_b200.batch import BatchReconstructor, autotune, set_tile
+    tile, ms = autotune(48, "gauss_2", 1, nparticles=64)
+    assert tile in (0, 1, 2, 3, 4, 5, -2) and len(ms) == 7 and all(v > 0 for v in ms.values())
+    set_tile(48, "gauss_2", 1, -1)
+    jobs = _jobs()
+    nsym = {"c1": 1, "d2": 4, "c3": 3}
+    pins = [-2, 1, 5, 4]
+    try:
+        for (params, _, _), t in zip(jobs, pins):
+            set_tile(params["size"][0], params["mode"], nsym[params["sym"]], t)
+        b = BatchReconstructor([p for p, _, _ in jobs])
+        b.insert_particles([ps.images for _, ps, _ in jobs], [m for _, _, m in jobs])
+        got = [b.get_accumulators(j) for j in range(len(jobs))]
+    finally:
+        for (params, _, _) in jobs:
+            set_tile(params["size"][0], params["mode"], nsym[params["sym"]], -1)
+    for j, (params, ps, meta) in enumerate(jobs):
+        d0, n0 = _alone(params, ps.images, meta)
+        assert oracle.rel_l2(got[j][0], d0) < RTOL and oracle.rel_l2(got[j][1], n0) < RTOL
+
+
 def test_served_result_equals_alone(gpu):
     """Requests arriving at different times, split into chunks, admitted by
     footprint and batched together: each result equals the job run alone."""
@@ -70,11 +94,16 @@ def test_served_result_equals_alone(gpu):
                                                   defocus=ps.defocus[a:b]))
                   for a, b in zip(cut[:-1], cut[1:])]
         reqs.append(Request(k, params, chunks, arrival=0.02 * k))
+    # a late request with job 0's parameters takes job 0's pooled reconstructor
+    reqs.append(Request(4, jobs[0][0], reqs[0].chunks, arrival=1.0))
     sched = Scheduler(hbm_budget=8 << 30, max_active=3)
-    res = Server(sched, GpuExecutor(doift=False)).run(reqs)
-    assert res["requests"] == 4 and res["p99_s"] >= res["p50_s"] > 0
+    exe = GpuExecutor(doift=False)
+    res = Server(sched, exe).run(reqs)
+    assert res["requests"] == 5 and res["p99_s"] >= res["p50_s"] > 0
+    assert exe.reused >= 1
+    exe.close()
     by_id = {j.req.rid: j for j in sched.done}
-    for k, (params, ps, meta) in enumerate(jobs):
+    for k, (params, ps, meta) in enumerate(jobs + [jobs[0]]):
         want = _alone(params, ps.images, meta)
         from eman2_b200 import FourierReconstructor
         r = FourierReconstructor(params)
