@@ -1,4 +1,4 @@
-"""Known-answer tests of the CPU oracle (SURVEY.md §8c list): exact taps of a
+"""Known-answer tests of the CPU oracle: exact taps of a
 single pixel, Hermitian duplicates on the x=0 plane, insert-then-remove,
 dihedral operators, reconstruction conventions (a blob lands where it was
 projected; noiseless projections reproduce the phantom), agreement of a
