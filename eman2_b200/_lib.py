@@ -84,6 +84,11 @@ SIGNATURES = {
                     ctypes.c_int),
     "fr_set_tile": ([ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int),
     "fr_update_peaks": ([_P, _P, _P], ctypes.c_int),
+    "fr_batch_graph_create": ([_P, _P, _P, _P, _P], ctypes.c_int),
+    "fr_graph_create": ([_P, ctypes.c_int, _P, _P, _P, _P, _P], ctypes.c_int),
+    "fr_graph_slot": ([_P, ctypes.c_int, _P], ctypes.c_int),
+    "fr_graph_launch": ([_P, _P, _P], ctypes.c_int),
+    "fr_graph_destroy": ([_P], ctypes.c_int),
     "fr_insert_slices_noalloc": ([_P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_char_p,
                                   _P, _P, _P, _P, _P], ctypes.c_int),
 }

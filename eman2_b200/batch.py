@@ -57,6 +57,63 @@ def set_tile(N: int, mode: str, nsym: int, tile: int):
     _lib.check(_lib.load().fr_set_tile(int(N), _lib.MODE_IDS[mode], int(nsym), int(tile)))
 
 
+class InsertGraph:
+    """A batched insertion round of fixed shapes captured once as a CUDA graph
+    (fr_graph_create): every replay inserts counts[j] particles of box
+    boxes[j] into recons[j] through the same prologue and persistent launches
+    as insert_particles_multi, without per-round host work beyond staging
+    the particles' metadata.  ctf[j]: whether job j's particles carry a CTF
+    (its replays must agree)."""
+
+    def __init__(self, recons, boxes, counts, ctf, stream=None):
+        lib = _lib.load()
+        self.recons = list(recons)
+        nj = len(self.recons)
+        self.boxes, self.counts = [int(b) for b in boxes], [int(c) for c in counts]
+        handles = (ctypes.c_void_p * nj)(*[r.handle.value for r in self.recons])
+        cb = (ctypes.c_int * nj)(*self.boxes)
+        cc = (ctypes.c_int * nj)(*self.counts)
+        cf = (ctypes.c_int * nj)(*[1 if c else 0 for c in ctf])
+        self.stream_ptr = stream.cuda_stream if stream is not None else \
+            library_stream(self.recons[0].handle)
+        out = ctypes.c_void_p()
+        _lib.check(lib.fr_graph_create(handles, nj, cb, cc, cf, ctypes.c_void_p(self.stream_ptr),
+                                       ctypes.byref(out)))
+        self._g = out
+
+    def slot(self, j: int) -> int:
+        """Device address of job j's image slot, float[counts[j]][box][box]."""
+        p = ctypes.c_void_p()
+        _lib.check(_lib.load().fr_graph_slot(self._g, int(j), ctypes.byref(p)))
+        return p.value
+
+    def launch(self, images, metas):
+        """One replay.  images[j]: (counts[j], box, box) host or device
+        particles, or None to insert what the slots hold; metas[j]: fr_particle
+        arrays of counts[j] entries."""
+        nj = len(self.recons)
+        metas_p = (ctypes.c_void_p * nj)(*[ctypes.cast(m, ctypes.c_void_p).value if m is not None
+                                          else None for m in metas])
+        if images is None:
+            _lib.check(_lib.load().fr_graph_launch(self._g, None, metas_p))
+            return
+        keep = [_host_or_device(im) if im is not None else None for im in images]
+        imgs = (ctypes.c_void_p * nj)(*[_lib.ptr(a) if a is not None else None for a in keep])
+        with join_streams(self.stream_ptr, *[a for a in keep if a is not None]):
+            _lib.check(_lib.load().fr_graph_launch(self._g, imgs, metas_p))
+
+    def close(self):
+        if getattr(self, "_g", None):
+            _lib.check(_lib.load().fr_graph_destroy(self._g))
+            self._g = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class BatchReconstructor:
     """A fixed set of reconstructions inserted together (fr_batch_*)."""
 
@@ -78,6 +135,10 @@ class BatchReconstructor:
             return
         insert_particles_multi([self.recons[j] for j in active], [images[j] for j in active],
                                [metas[j] for j in active], stream)
+
+    def capture(self, boxes, counts, ctf, stream=None) -> InsertGraph:
+        """A CUDA graph of one insertion round of these shapes (InsertGraph)."""
+        return InsertGraph(self.recons, boxes, counts, ctf, stream)
 
     def get_accumulators(self, j: int):
         return self.recons[j].get_accumulators()

@@ -38,6 +38,7 @@ static std::mutex g_stat_mu;
 static double g_insert_ms = 0.0, g_gather_ms = 0.0;
 
 void note_launch(int n) { g_launches += n; }
+long long launches_noted() { return g_launches.load(); }
 
 // ----------------------------------------------------------- device consts
 static std::mutex g_mu;
@@ -480,44 +481,67 @@ int alloc_volume(fr_recon *r) {
 }
 
 // The caller pipeline of programs/e2spa_make3d.py:300-345 for one chunk of
-// particles already on the device.
-int prologue_chunk(fr_recon *r, const float *d_raw, int n, int box, const fr_particle *meta) {
-  const int N = r->N;
-  cudaStream_t st = r->stream;
-  const size_t img = (size_t)N * N, spec = (size_t)N * (N / 2 + 1);
-  TRY(r->s_img.ensure(sizeof(float) * img * n));
-  TRY(r->s_slices.ensure(sizeof(float) * slice_floats(N) * n));
-  CU(launch_pad(d_raw, n, box, N, r->s_img.as<float>(), st));
-  // CTF constants and per-particle vectors on the host.
+// particles already on the device, in two halves: the host half turns the
+// particles' metadata into one block of device-ready arrays, the device half
+// is kernels and FFTs only (so it can be captured in a CUDA graph).
+
+size_t prologue_meta_bytes(int n) {
+  return ctf_dev_size() * (size_t)n + sizeof(float) * 12 * (size_t)n;
+}
+
+// Writes [CTF constants: ctf_dev_size()*n][txy: 2n][w: n][rot: 9n] into blk;
+// returns whether any particle carries a CTF.
+bool prologue_meta(int N, int n, const fr_particle *meta, unsigned char *blk) {
   const size_t cs = ctf_dev_size();
-  std::vector<unsigned char> ctf(cs * n);
-  std::vector<float> txy(2 * n), w(n), rot(9 * n);
+  float *txy = reinterpret_cast<float *>(blk + cs * n);
+  float *w = txy + 2 * (size_t)n;
+  float *rot = w + n;
   bool any_ctf = false;
   for (int i = 0; i < n; i++) {
     const fr_particle &m = meta[i];
     ctf_constants(m.defocus, m.dfdiff, m.dfang, m.voltage, m.cs, m.apix, m.ampcont, N,
-                  ctf.data() + cs * i);
+                  blk + cs * i);
     if (std::fabs(m.defocus) > 1e-4f) any_ctf = true;
     // ts = inverse of the translation-only part of xform.projection; the
     // bilinear xform then applies ts^-1, i.e. +(tx, ty) (programs/e2spa_make3d.py:339-342).
     txy[2 * i] = m.tx;
     txy[2 * i + 1] = m.ty;
     w[i] = m.weight > 0 ? m.weight : 0.0f;   // wt <= 0: skipped (programs/e2spa_make3d.py:304)
-    memcpy(&rot[9 * i], m.rot, sizeof(float) * 9);
+    memcpy(&rot[9 * (size_t)i], m.rot, sizeof(float) * 9);
   }
+  return any_ctf;
+}
+
+// Copies a metadata block into the handle's per-particle device arrays.
+int prologue_upload(fr_recon *r, int n, const unsigned char *blk, cudaStream_t st) {
+  const size_t cs = ctf_dev_size();
   TRY(r->s_ctf.ensure(cs * n));
   TRY(r->s_txy.ensure(sizeof(float) * 2 * n));
   TRY(r->s_w.ensure(sizeof(float) * n));
   TRY(r->s_rot.ensure(sizeof(float) * 9 * n));
+  const unsigned char *txy = blk + cs * n;
+  const unsigned char *w = txy + sizeof(float) * 2 * n;
+  const unsigned char *rot = w + sizeof(float) * n;
+  CU(cudaMemcpyAsync(r->s_ctf.p, blk, cs * n, cudaMemcpyHostToDevice, st));
+  CU(cudaMemcpyAsync(r->s_txy.p, txy, sizeof(float) * 2 * n, cudaMemcpyHostToDevice, st));
+  CU(cudaMemcpyAsync(r->s_w.p, w, sizeof(float) * n, cudaMemcpyHostToDevice, st));
+  CU(cudaMemcpyAsync(r->s_rot.p, rot, sizeof(float) * 9 * n, cudaMemcpyHostToDevice, st));
+  return FR_OK;
+}
+
+int prologue_device(fr_recon *r, const float *d_raw, int n, int box, bool any_ctf) {
+  const int N = r->N;
+  cudaStream_t st = r->stream;
+  const size_t img = (size_t)N * N, spec = (size_t)N * (N / 2 + 1);
+  TRY(r->s_img.ensure(sizeof(float) * img * n));
+  TRY(r->s_slices.ensure(sizeof(float) * slice_floats(N) * n));
   TRY(r->s_mean.ensure(sizeof(float) * n));
-  CU(cudaMemcpyAsync(r->s_ctf.p, ctf.data(), cs * n, cudaMemcpyHostToDevice, st));
-  CU(cudaMemcpyAsync(r->s_txy.p, txy.data(), sizeof(float) * 2 * n, cudaMemcpyHostToDevice, st));
-  CU(cudaMemcpyAsync(r->s_w.p, w.data(), sizeof(float) * n, cudaMemcpyHostToDevice, st));
-  CU(cudaMemcpyAsync(r->s_rot.p, rot.data(), sizeof(float) * 9 * n, cudaMemcpyHostToDevice, st));
+  TRY(r->s_spec.ensure(std::max(sizeof(cufftComplex) * spec, sizeof(float) * img) * n));
+  TRY(r->s_t3d.ensure(sizeof(float) * 9 * (size_t)n * r->nsym));
+  if (any_ctf) TRY(r->s_img2.ensure(sizeof(float) * img * n));
+  CU(launch_pad(d_raw, n, box, N, r->s_img.as<float>(), st));
   const float *img_on = nullptr;
   if (any_ctf) {
-    TRY(r->s_spec.ensure(sizeof(cufftComplex) * spec * n));
-    TRY(r->s_img2.ensure(sizeof(float) * img * n));
     TRY(r->plans.exec2d(true, N, n, r->s_img.p, r->s_spec.p, st));
     CU(launch_ctf_flip_dev(r->s_spec.as<cufftComplex>(), r->s_ctf.p, n, N, st));
     TRY(r->plans.exec2d(false, N, n, r->s_spec.p, r->s_img2.p, st));
@@ -526,17 +550,23 @@ int prologue_chunk(fr_recon *r, const float *d_raw, int n, int box, const fr_par
   CU(launch_edge_mean(r->s_img.as<float>(), img_on, any_ctf ? r->s_ctf.p : nullptr, n, N,
                       r->s_mean.as<float>(), st));
   // preprocess_slice: shift, phase origin to corner, x sqrt((N+2)/N), r2c.
-  TRY(r->s_spec.ensure(sizeof(float) * img * n));  // real staging for the r2c input
+  // s_spec is the real staging for the r2c input.
   volatile float inv = 1.0f / (float)N;
   const float scale = sqrtf(inv * (float)(N + 2));
   CU(launch_shift_corner(r->s_img.as<float>(), img_on, any_ctf ? r->s_ctf.p : nullptr,
                          r->s_mean.as<float>(), r->s_txy.as<float>(), 2, n, N, scale,
                          r->s_spec.as<float>(), st));
   TRY(r->plans.exec2d(true, N, n, r->s_spec.p, r->s_slices.p, st));
-  TRY(r->s_t3d.ensure(sizeof(float) * 9 * (size_t)n * r->nsym));
   CU(launch_compose(r->s_rot.as<float>(), r->d_sym.as<float>(), n, r->nsym, r->s_t3d.as<float>(),
                     st));
   return FR_OK;
+}
+
+int prologue_chunk(fr_recon *r, const float *d_raw, int n, int box, const fr_particle *meta) {
+  std::vector<unsigned char> blk(prologue_meta_bytes(n));
+  const bool any_ctf = prologue_meta(r->N, n, meta, blk.data());
+  TRY(prologue_upload(r, n, blk.data(), r->stream));
+  return prologue_device(r, d_raw, n, box, any_ctf);
 }
 
 int particles_chunk(fr_recon *r, const float *d_raw, int n, int box, const fr_particle *meta,

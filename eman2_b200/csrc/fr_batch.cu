@@ -26,6 +26,8 @@ namespace fr {
 static std::mutex g_tune_mu;
 static std::map<std::tuple<int, int, int>, int> g_tuned;
 constexpr int kTunedScatter = -2;
+// Particles per job per round of a batched insertion (bounds the scratch).
+constexpr int kBatchChunk = 4096;
 
 int tuned_tile(int N, int mode, int nsym) {
   std::lock_guard<std::mutex> lk(g_tune_mu);
@@ -113,9 +115,162 @@ int fr_batch_set_stream(fr_batch *b, void *stream) {
 
 namespace fr {
 
+// One caller at a time per handle: lock them in address order.
+static int lock_handles(const std::vector<fr_recon *> &jobs,
+                        std::vector<std::unique_lock<std::mutex>> &locks) {
+  std::vector<fr_recon *> order(jobs);
+  std::sort(order.begin(), order.end());
+  if (std::adjacent_find(order.begin(), order.end()) != order.end())
+    return fail(FR_EINVAL_PARAM, "a handle appears twice");
+  for (fr_recon *r : order) locks.emplace_back(r->mu);
+  return FR_OK;
+}
+
+// One round of a batched insertion: every participating job's InsertJob,
+// its schedule, and per schedule the ordered work list of one launch.
+struct RoundGroup {
+  int tile = 0, max_mode = FR_MODE_NEAREST, maxN = 0;
+  size_t off = 0, nwork = 0;   // byte offset and item count in the work buffer
+};
+struct RoundPlan {
+  std::vector<InsertJob> hj;
+  std::vector<int> owner, jt;
+  std::vector<RoundGroup> groups;
+  std::vector<unsigned char> work;   // every group's items, 16-byte aligned
+};
+
+static bool is_column(int tile) { return tile == kColumnTile || tile == kColumn3Tile; }
+
+// Each job's schedule: the caller's pin, else the autotuner's measurement for
+// its (N, mode, nsym), else the barrier-free column kernel.  Jobs that share
+// a schedule share one persistent launch per round.
+static int job_tile(const fr_recon *r, int tile_pref) {
+  if (tile_pref != -1) return tile_pref;
+  const int t = tuned_tile(r->N, r->mode, r->nsym);
+  return t != -1 ? t : default_tile(r->mode, r->N, r->nsym, 0);
+}
+
+// Adds job r's InsertJob (its chunk's slices, rotations and weights in its
+// scratch) to the plan, with the tile list of its schedule.
+static void plan_add(RoundPlan &P, fr_recon *r, int owner, int np, int tile_pref) {
+  InsertJob J = make_job(r, r->s_slices.as<float2>(), r->s_t3d.as<float>(), r->s_w.as<float>(), np);
+  const int tile = job_tile(r, tile_pref);
+  if (tile != kTunedScatter && r->tiles_tile != tile) {
+    if (is_column(tile))
+      column_tiles(r->N, r->mode, r->p.corners, r->tiles, r->tx, r->ty, r->tz, &r->tile_dist);
+    else gather_tiles(r->N, r->mode, tile, r->p.corners, r->tiles, r->tx, r->ty, r->tz);
+    r->tiles_tile = tile;
+    r->work_np = -1;
+  }
+  J.tiles_x = r->tx;
+  J.tiles_y = r->ty;
+  J.tiles_z = r->tz;
+  P.hj.push_back(J);
+  P.owner.push_back(owner);
+  P.jt.push_back(tile);
+}
+
+// Builds each schedule group's work list.  Column items run slice-bucket-major
+// (slice_bucket per job, so the CTAs in flight share a bucket's slices in L2)
+// and within a bucket by estimated cost, heaviest first: the slices meeting a
+// tile fall off with its distance from the origin (tiles are sorted by
+// distance), times the slices in the item's block.
+static void plan_groups(const std::vector<fr_recon *> &jobs, RoundPlan &P) {
+  std::vector<int> tiles_used(P.jt);
+  std::sort(tiles_used.begin(), tiles_used.end());
+  tiles_used.erase(std::unique(tiles_used.begin(), tiles_used.end()), tiles_used.end());
+  for (const int tile : tiles_used) {
+    RoundGroup g;
+    g.tile = tile;
+    if (tile == kTunedScatter) { P.groups.push_back(g); continue; }
+    const bool column = is_column(tile);
+    std::vector<std::pair<double, int4>> items;
+    for (size_t k = 0; k < P.hj.size(); k++) {
+      if (P.jt[k] != tile) continue;
+      const fr_recon *r = jobs[P.owner[k]];
+      g.maxN = std::max(g.maxN, r->N);
+      if (r->mode == FR_MODE_GAUSS5) g.max_mode = FR_MODE_GAUSS5;
+      else if (g.max_mode != FR_MODE_GAUSS5 && r->mode != FR_MODE_NEAREST) g.max_mode = r->mode;
+      const int nsl = P.hj[k].np * P.hj[k].nsym;
+      const double nt = (double)r->tiles.size();
+      const int bucket = slice_bucket(r->N, r->nsym);
+      for (size_t t = 0; t < r->tiles.size(); t++) {
+        const double frac = (double)t / std::max(1.0, nt);
+        const double fall = 1.0 / (1.0 + 8.0 * std::cbrt(frac) * r->N / 16.0);
+        if (column) {
+          const int blk = column_block(r->tile_dist[t]);
+          for (int s0 = 0; s0 < nsl; s0 += blk) {
+            const int len = std::min(blk, nsl - s0);
+            // bucket first (costs are below 1e4), then heaviest first
+            items.push_back({1e12 * (s0 / bucket) - len * fall,
+                             make_int4((int)k, r->tiles[t], s0, s0 + len)});
+          }
+        } else {
+          items.push_back({-nsl * fall, make_int4((int)k, r->tiles[t], 0, 0)});
+        }
+      }
+    }
+    std::stable_sort(items.begin(), items.end(),
+                     [](const std::pair<double, int4> &a, const std::pair<double, int4> &c) {
+                       return a.first < c.first;
+                     });
+    g.off = (P.work.size() + 15) & ~(size_t)15;
+    g.nwork = items.size();
+    const size_t isz = column ? sizeof(int4) : sizeof(int2);
+    P.work.resize(g.off + isz * items.size());
+    for (size_t i = 0; i < items.size(); i++) {
+      if (column) memcpy(&P.work[g.off + i * isz], &items[i].second, isz);
+      else {
+        const int2 w2 = make_int2(items[i].second.x, items[i].second.y);
+        memcpy(&P.work[g.off + i * isz], &w2, isz);
+      }
+    }
+    P.groups.push_back(g);
+  }
+}
+
+// Job table and work lists to the device (host sources are pageable
+// vectors: the copies have taken them when cudaMemcpyAsync returns).
+static int plan_upload(const RoundPlan &P, BatchScratch &bs, cudaStream_t st) {
+  TRY(bs.d_jobs.ensure(sizeof(InsertJob) * std::max<size_t>(1, P.hj.size())));
+  TRY(bs.d_counter.ensure(sizeof(int)));
+  TRY(bs.d_work.ensure(std::max<size_t>(16, P.work.size())));
+  CU(cudaMemcpyAsync(bs.d_jobs.p, P.hj.data(), sizeof(InsertJob) * P.hj.size(),
+                     cudaMemcpyHostToDevice, st));
+  if (!P.work.empty())
+    CU(cudaMemcpyAsync(bs.d_work.p, P.work.data(), P.work.size(), cudaMemcpyHostToDevice, st));
+  return FR_OK;
+}
+
+// Device work of the round: per schedule group one persistent launch (or the
+// scatter), then the face taps.  Kernels and memsets only.
+static int plan_launch(const RoundPlan &P, BatchScratch &bs, cudaStream_t st) {
+  const InsertJob *d_jobs = bs.d_jobs.as<InsertJob>();
+  for (const RoundGroup &g : P.groups) {
+    if (g.tile == kTunedScatter) {
+      for (size_t k = 0; k < P.hj.size(); k++)
+        if (P.jt[k] == g.tile) TRY(run_scatter(P.hj[k], false, st));
+      continue;
+    }
+    const void *w = (const unsigned char *)bs.d_work.p + g.off;
+    if (g.tile == kColumn3Tile)
+      CU(launch_column3(d_jobs, (const int4 *)w, (int)g.nwork, kColumnBlock, bs.d_counter.as<int>(),
+                        g.maxN, st));
+    else if (g.tile == kColumnTile)
+      CU(launch_column(d_jobs, (const int4 *)w, (int)g.nwork, kColumnBlock, bs.d_counter.as<int>(),
+                       g.max_mode, st));
+    else
+      CU(launch_gather(d_jobs, P.hj.data(), (int)P.hj.size(), (const int2 *)w, (int)g.nwork,
+                       g.tile, bs.d_counter.as<int>(), g.max_mode, st));
+    for (size_t k = 0; k < P.hj.size(); k++)
+      if (P.jt[k] == g.tile) TRY(run_scatter(P.hj[k], true, st));
+  }
+  return FR_OK;
+}
+
 // Inserts, for every job, counts[j] particles through the caller pipeline;
-// all jobs' insertion work goes through one persistent launch per round.
-// Every job runs on `st` for the duration of the call.
+// all jobs' insertion work goes through one persistent launch per schedule
+// per round.  Every job runs on `st` for the duration of the call.
 static int batch_insert(std::vector<fr_recon *> &jobs, BatchScratch &bs, int tile_pref,
                         cudaStream_t st, const float *const *imgs, const int *boxes,
                         const int *counts, const fr_particle *const *meta) {
@@ -141,123 +296,27 @@ static int batch_insert(std::vector<fr_recon *> &jobs, BatchScratch &bs, int til
   if (bs.last && bs.last != st) CU(cudaStreamWaitEvent(st, bs.done, 0));
   for (int j = 0; j < nj; j++) TRY(stream_enter(jobs[j], st));
   // Rounds of at most `chunk` particles per job, so scratch stays bounded.
-  const int chunk = 4096;
+  const int chunk = kBatchChunk;
   int rounds = 0;
   for (int j = 0; j < nj; j++) rounds = std::max(rounds, (counts[j] + chunk - 1) / chunk);
-  // Each job's schedule: the caller's pin, else the autotuner's measurement
-  // for its (N, mode, nsym), else the barrier-free column kernel.  Jobs that
-  // share a schedule share one persistent launch per round.
-  auto job_tile = [&](const fr_recon *r) {
-    if (tile_pref != -1) return tile_pref;
-    const int t = tuned_tile(r->N, r->mode, r->nsym);
-    return t != -1 ? t : default_tile(r->mode, r->N, r->nsym, 0);
-  };
   for (int rd = 0; rd < rounds; rd++) {
-    std::vector<InsertJob> hj;
-    std::vector<int> owner, jt;
+    RoundPlan P;
     for (int j = 0; j < nj; j++) {
       fr_recon *r = jobs[j];
       const int p0 = rd * chunk;
       const int c = std::max(0, std::min(chunk, counts[j] - p0));
       if (c == 0) continue;
       const int box = boxes[j];
-      const float *src = imgs[j] + (size_t)p0 * box * box;
       const void *d_raw = nullptr;
-      TRY(to_device(src, sizeof(float) * (size_t)c * box * box, r->s_in, st, &d_raw));
+      TRY(to_device(imgs[j] + (size_t)p0 * box * box, sizeof(float) * (size_t)c * box * box,
+                    r->s_in, st, &d_raw));
       TRY(prologue_chunk(r, (const float *)d_raw, c, box, meta[j] + p0));
-      InsertJob J = make_job(r, r->s_slices.as<float2>(), r->s_t3d.as<float>(), r->s_w.as<float>(), c);
-      const int tile = job_tile(r);
-      if (tile != kTunedScatter && r->tiles_tile != tile) {
-        if (tile == kColumnTile || tile == kColumn3Tile)
-          column_tiles(r->N, r->mode, r->p.corners, r->tiles, r->tx, r->ty, r->tz, &r->tile_dist);
-        else gather_tiles(r->N, r->mode, tile, r->p.corners, r->tiles, r->tx, r->ty, r->tz);
-        r->tiles_tile = tile;
-        r->work_np = -1;
-      }
-      J.tiles_x = r->tx;
-      J.tiles_y = r->ty;
-      J.tiles_z = r->tz;
-      hj.push_back(J);
-      owner.push_back(j);
-      jt.push_back(tile);
+      plan_add(P, r, j, c, tile_pref);
     }
-    if (hj.empty()) continue;
-    TRY(bs.d_jobs.ensure(sizeof(InsertJob) * hj.size()));
-    TRY(bs.d_counter.ensure(sizeof(int)));
-    CU(cudaMemcpyAsync(bs.d_jobs.p, hj.data(), sizeof(InsertJob) * hj.size(),
-                       cudaMemcpyHostToDevice, st));
-    std::vector<int> tiles_used(jt);
-    std::sort(tiles_used.begin(), tiles_used.end());
-    tiles_used.erase(std::unique(tiles_used.begin(), tiles_used.end()), tiles_used.end());
-    for (const int tile : tiles_used) {
-      if (tile == kTunedScatter) {
-        for (size_t k = 0; k < hj.size(); k++)
-          if (jt[k] == tile) TRY(run_scatter(hj[k], false, st));
-        continue;
-      }
-      const bool column = tile == kColumnTile || tile == kColumn3Tile;
-      int max_mode = FR_MODE_NEAREST, maxN = 0;
-      // Order the group's work items slice-bucket-major (slice_bucket per
-      // job, so the CTAs in flight share a bucket's slices in
-      // L2), and within a bucket by estimated cost, heaviest first: the slices
-      // meeting a tile fall off with its distance from the origin (tiles are
-      // sorted by distance), times the slices in the item's block.
-      std::vector<std::pair<double, int4>> items;
-      std::vector<int> bucket_of;
-      for (size_t k = 0; k < hj.size(); k++) {
-        if (jt[k] != tile) continue;
-        fr_recon *r = jobs[owner[k]];
-        maxN = std::max(maxN, r->N);
-        if (r->mode == FR_MODE_GAUSS5) max_mode = FR_MODE_GAUSS5;
-        else if (max_mode != FR_MODE_GAUSS5 && r->mode != FR_MODE_NEAREST) max_mode = r->mode;
-        const int nsl = hj[k].np * hj[k].nsym;
-        const double nt = (double)r->tiles.size();
-        for (size_t t = 0; t < r->tiles.size(); t++) {
-          const double frac = (double)t / std::max(1.0, nt);
-          const double fall = 1.0 / (1.0 + 8.0 * std::cbrt(frac) * r->N / 16.0);
-          if (column) {
-            const int blk = column_block(r->tile_dist[t]);
-            for (int s0 = 0; s0 < nsl; s0 += blk) {
-              const int len = std::min(blk, nsl - s0);
-              items.push_back({-len * fall, make_int4((int)k, r->tiles[t], s0, s0 + len)});
-            bucket_of.push_back(s0 / slice_bucket(r->N, r->nsym));
-            }
-          } else {
-            items.push_back({-nsl * fall, make_int4((int)k, r->tiles[t], 0, 0)});
-            bucket_of.push_back(0);
-          }
-        }
-      }
-      // bucket first (costs are below 1e4), then heaviest first
-      for (size_t i = 0; i < items.size(); i++) items[i].first += 1e12 * bucket_of[i];
-      std::stable_sort(items.begin(), items.end(),
-                       [](const std::pair<double, int4> &a, const std::pair<double, int4> &c) {
-                         return a.first < c.first;
-                       });
-      if (column) {
-        std::vector<int4> work(items.size());
-        for (size_t i = 0; i < items.size(); i++) work[i] = items[i].second;
-        TRY(bs.d_work.ensure(sizeof(int4) * std::max<size_t>(1, work.size())));
-        CU(cudaMemcpyAsync(bs.d_work.p, work.data(), sizeof(int4) * work.size(),
-                           cudaMemcpyHostToDevice, st));
-        if (tile == kColumn3Tile)
-          CU(launch_column3(bs.d_jobs.as<InsertJob>(), bs.d_work.as<int4>(), (int)work.size(),
-                            kColumnBlock, bs.d_counter.as<int>(), maxN, st));
-        else
-          CU(launch_column(bs.d_jobs.as<InsertJob>(), bs.d_work.as<int4>(), (int)work.size(),
-                           kColumnBlock, bs.d_counter.as<int>(), max_mode, st));
-      } else {
-        std::vector<int2> work(items.size());
-        for (size_t i = 0; i < items.size(); i++) work[i] = make_int2(items[i].second.x, items[i].second.y);
-        TRY(bs.d_work.ensure(sizeof(int2) * std::max<size_t>(1, work.size())));
-        CU(cudaMemcpyAsync(bs.d_work.p, work.data(), sizeof(int2) * work.size(),
-                           cudaMemcpyHostToDevice, st));
-        CU(launch_gather(bs.d_jobs.as<InsertJob>(), hj.data(), (int)hj.size(), bs.d_work.as<int2>(),
-                         (int)work.size(), tile, bs.d_counter.as<int>(), max_mode, st));
-      }
-      for (size_t k = 0; k < hj.size(); k++)
-        if (jt[k] == tile) TRY(run_scatter(hj[k], true, st));
-    }
+    if (P.hj.empty()) continue;
+    plan_groups(jobs, P);
+    TRY(plan_upload(P, bs, st));
+    TRY(plan_launch(P, bs, st));
   }
   CU(cudaEventRecord(bs.done, st));
   bs.last = st;
@@ -286,16 +345,280 @@ int fr_insert_particles_multi(fr_recon *const *handles, int nh, const float *con
   std::vector<fr_recon *> jobs(handles, handles + nh);
   for (fr_recon *r : jobs)
     if (!r) return fail(FR_ENULL, "null reconstructor handle");
-  // One caller at a time per handle: lock them in address order.
-  std::vector<fr_recon *> order(jobs);
-  std::sort(order.begin(), order.end());
-  order.erase(std::unique(order.begin(), order.end()), order.end());
-  if (order.size() != jobs.size()) return fail(FR_EINVAL_PARAM, "a handle appears twice");
   std::vector<std::unique_lock<std::mutex>> locks;
-  for (fr_recon *r : order) locks.emplace_back(r->mu);
+  TRY(lock_handles(jobs, locks));
   static thread_local BatchScratch bs;
   cudaStream_t st = stream ? (cudaStream_t)stream : jobs[0]->stream;
   return batch_insert(jobs, bs, -1, st, imgs, boxes, counts, meta);
+}
+
+// ------------------------------------------------------------------ graphs
+// A batched insertion round of fixed shapes captured once as a CUDA graph.
+// The graph owns the images' device slots and every job's chunk scratch (so
+// later calls on the same handles cannot move them); a replay writes the
+// particles' metadata into pinned staging, copies it and the images in, and
+// launches the graph.
+}  // extern "C"
+
+namespace fr {
+struct JobBufs {
+  DevBuf img, slices, mean, spec, t3d, img2, ctf, txy, w, rot;
+  void swap_with(fr_recon *r) {
+    std::swap(img, r->s_img);
+    std::swap(slices, r->s_slices);
+    std::swap(mean, r->s_mean);
+    std::swap(spec, r->s_spec);
+    std::swap(t3d, r->s_t3d);
+    std::swap(img2, r->s_img2);
+    std::swap(ctf, r->s_ctf);
+    std::swap(txy, r->s_txy);
+    std::swap(w, r->s_w);
+    std::swap(rot, r->s_rot);
+  }
+  void release() {
+    for (DevBuf *b : {&img, &slices, &mean, &spec, &t3d, &img2, &ctf, &txy, &w, &rot}) b->release();
+  }
+};
+}  // namespace fr
+
+struct fr_graph {
+  std::vector<fr_recon *> jobs;
+  cudaStream_t st = nullptr;
+  std::vector<int> boxes, counts, ctf;
+  std::vector<fr::DevBuf> slots;
+  std::vector<fr::JobBufs> bufs;
+  std::vector<size_t> meta_off;
+  size_t meta_bytes = 0;
+  unsigned char *pinned[2] = {nullptr, nullptr};
+  cudaEvent_t staged[2] = {nullptr, nullptr};
+  bool staged_used[2] = {false, false};
+  int next = 0;
+  long long kernels = 0;          // this library's kernels per replay
+  fr::BatchScratch bs;
+  fr::RoundPlan plan;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  std::mutex mu;
+};
+
+namespace fr {
+
+static void graph_free(fr_graph *g) {
+  if (!g) return;
+  if (g->exec) cudaGraphExecDestroy(g->exec);
+  if (g->graph) cudaGraphDestroy(g->graph);
+  for (auto &s : g->slots) s.release();
+  for (auto &jb : g->bufs) jb.release();
+  g->bs.d_jobs.release();
+  g->bs.d_work.release();
+  g->bs.d_counter.release();
+  for (int k = 0; k < 2; k++) {
+    if (g->pinned[k]) cudaFreeHost(g->pinned[k]);
+    if (g->staged[k]) cudaEventDestroy(g->staged[k]);
+  }
+  delete g;
+}
+
+static int graph_create(const std::vector<fr_recon *> &jobs, cudaStream_t st, int tile_pref,
+                        const int *boxes, const int *counts, const int *ctf, fr_graph **out) {
+  const int nj = (int)jobs.size();
+  int total = 0;
+  for (int j = 0; j < nj; j++) {
+    TRY(check_state(jobs[j]));
+    if (counts[j] < 0 || counts[j] > kBatchChunk || (counts[j] > 0 && boxes[j] <= 0))
+      return fail(FR_EINVAL_PARAM, "job %d: count must be in [0, %d] with a positive box", j,
+                  kBatchChunk);
+    total += counts[j];
+  }
+  if (total == 0) return fail(FR_EINVAL_PARAM, "a graph needs at least one particle");
+  fr_graph *g = new fr_graph();
+  g->jobs = jobs;
+  g->st = st;
+  g->boxes.assign(boxes, boxes + nj);
+  g->counts.assign(counts, counts + nj);
+  g->ctf.assign(nj, 0);
+  for (int j = 0; ctf && j < nj; j++) g->ctf[j] = ctf[j] ? 1 : 0;
+  g->slots.resize(nj);
+  g->bufs.resize(nj);
+  g->meta_off.assign(nj, 0);
+  for (int j = 0; j < nj; j++) {
+    g->meta_off[j] = g->meta_bytes;
+    g->meta_bytes += (prologue_meta_bytes(counts[j]) + 15) & ~(size_t)15;
+  }
+  std::vector<cudaStream_t> saved;
+  for (fr_recon *r : jobs) { saved.push_back(r->stream); r->stream = st; }
+  // Sizing pass on the graph-owned scratch (swapped into the handles): a
+  // prologue of weight-0 particles allocates every buffer and FFT plan the
+  // capture uses, so the captured work allocates nothing.
+  for (int j = 0; j < nj; j++) g->bufs[j].swap_with(jobs[j]);
+  int rc = FR_OK;
+  for (int j = 0; j < nj && rc == FR_OK; j++) rc = stream_enter(jobs[j], st);
+  std::vector<unsigned char> blk(std::max<size_t>(16, g->meta_bytes));
+  for (int j = 0; j < nj && rc == FR_OK; j++) {
+    fr_recon *r = jobs[j];
+    const int n = counts[j];
+    if (n == 0) continue;
+    const size_t bytes = sizeof(float) * (size_t)n * boxes[j] * boxes[j];
+    if ((rc = g->slots[j].ensure(bytes)) != FR_OK) break;
+    if (cudaMemsetAsync(g->slots[j].p, 0, bytes, st) != cudaSuccess) {
+      rc = fail(FR_ECUDA, "memset failed");
+      break;
+    }
+    std::vector<fr_particle> parts(n);
+    for (fr_particle &m : parts) {
+      memset(&m, 0, sizeof m);
+      m.rot[0] = m.rot[4] = m.rot[8] = 1.0f;
+      m.defocus = g->ctf[j] ? 1.5f : 0.0f;
+      m.voltage = 300.0f;
+      m.cs = 2.7f;
+      m.apix = 1.0f;
+      m.ampcont = 10.0f;
+    }
+    prologue_meta(r->N, n, parts.data(), blk.data() + g->meta_off[j]);
+    if ((rc = prologue_upload(r, n, blk.data() + g->meta_off[j], st)) != FR_OK) break;
+    if ((rc = prologue_device(r, g->slots[j].as<float>(), n, boxes[j], g->ctf[j])) != FR_OK) break;
+    plan_add(g->plan, r, j, n, tile_pref);
+  }
+  if (rc == FR_OK) {
+    plan_groups(jobs, g->plan);
+    rc = plan_upload(g->plan, g->bs, st);
+  }
+  if (rc == FR_OK && cudaStreamSynchronize(st) != cudaSuccess)
+    rc = fail(FR_ECUDA, "sizing pass failed: %s", cudaGetErrorString(cudaGetLastError()));
+  // Capture: the device halves of the prologues and the round's launches.
+  if (rc == FR_OK) {
+    if (cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed) != cudaSuccess) {
+      rc = fail(FR_ECUDA, "cudaStreamBeginCapture failed");
+    } else {
+      const long long noted = launches_noted();
+      for (int j = 0; j < nj && rc == FR_OK; j++)
+        if (counts[j] > 0)
+          rc = prologue_device(jobs[j], g->slots[j].as<float>(), counts[j], boxes[j], g->ctf[j]);
+      if (rc == FR_OK) rc = plan_launch(g->plan, g->bs, st);
+      const cudaError_t e = cudaStreamEndCapture(st, &g->graph);
+      if (rc == FR_OK && e != cudaSuccess)
+        rc = fail(FR_ECUDA, "stream capture failed: %s", cudaGetErrorString(e));
+      g->kernels = launches_noted() - noted;
+    }
+  }
+  if (rc == FR_OK && cudaGraphInstantiate(&g->exec, g->graph, 0) != cudaSuccess)
+    rc = fail(FR_ECUDA, "cudaGraphInstantiate failed: %s", cudaGetErrorString(cudaGetLastError()));
+  for (int j = 0; j < nj; j++) g->bufs[j].swap_with(jobs[j]);
+  for (int k = 0; k < 2 && rc == FR_OK; k++) {
+    if (cudaHostAlloc((void **)&g->pinned[k], std::max<size_t>(16, g->meta_bytes),
+                      cudaHostAllocDefault) != cudaSuccess ||
+        cudaEventCreateWithFlags(&g->staged[k], cudaEventDisableTiming) != cudaSuccess)
+      rc = fail(FR_ENOMEM, "pinned staging allocation failed");
+  }
+  for (int j = 0; j < nj; j++) {
+    stream_leave(jobs[j], st);
+    jobs[j]->stream = saved[j];
+  }
+  if (rc != FR_OK) {
+    cudaGetLastError();
+    graph_free(g);
+    return rc;
+  }
+  *out = g;
+  return FR_OK;
+}
+
+}  // namespace fr
+
+extern "C" {
+
+int fr_graph_create(fr_recon *const *handles, int nh, const int *boxes, const int *counts,
+                    const int *ctf, void *stream, fr_graph **out) {
+  if (!handles || nh <= 0 || !boxes || !counts || !out) return fail(FR_ENULL, "null argument");
+  *out = nullptr;
+  std::vector<fr_recon *> jobs(handles, handles + nh);
+  for (fr_recon *r : jobs)
+    if (!r) return fail(FR_ENULL, "null reconstructor handle");
+  std::vector<std::unique_lock<std::mutex>> locks;
+  TRY(lock_handles(jobs, locks));
+  cudaStream_t st = stream ? (cudaStream_t)stream : jobs[0]->stream;
+  return graph_create(jobs, st, -1, boxes, counts, ctf, out);
+}
+
+int fr_batch_graph_create(fr_batch *b, const int *boxes, const int *counts, const int *ctf,
+                          fr_graph **out) {
+  if (!b || !boxes || !counts || !out) return fail(FR_ENULL, "null argument");
+  *out = nullptr;
+  std::lock_guard<std::mutex> lk(b->mu);
+  std::vector<std::unique_lock<std::mutex>> locks;
+  TRY(lock_handles(b->jobs, locks));
+  return graph_create(b->jobs, b->stream, b->tile, boxes, counts, ctf, out);
+}
+
+int fr_graph_slot(fr_graph *g, int job, float **d_images) {
+  if (!g || !d_images) return fail(FR_ENULL, "null argument");
+  if (job < 0 || job >= (int)g->slots.size()) return fail(FR_EINVAL_PARAM, "job %d out of range", job);
+  *d_images = g->slots[job].as<float>();
+  return FR_OK;
+}
+
+int fr_graph_launch(fr_graph *g, const float *const *imgs, const fr_particle *const *meta) {
+  if (!g || !meta) return fail(FR_ENULL, "null argument");
+  std::lock_guard<std::mutex> glk(g->mu);
+  std::vector<std::unique_lock<std::mutex>> locks;
+  TRY(lock_handles(g->jobs, locks));
+  for (fr_recon *r : g->jobs) TRY(check_state(r));
+  cudaStream_t st = g->st;
+  const int nj = (int)g->counts.size();
+  const int k = g->next;
+  // this staging block was last read by the copies two replays ago
+  if (g->staged_used[k]) CU(cudaEventSynchronize(g->staged[k]));
+  const size_t cs = ctf_dev_size();
+  for (int j = 0; j < nj; j++) {
+    const int n = g->counts[j];
+    if (n == 0) continue;
+    if (!meta[j]) return fail(FR_ENULL, "job %d: null metadata", j);
+    if (imgs && !imgs[j]) return fail(FR_ENULL, "job %d: null images", j);
+    const bool any = prologue_meta(g->jobs[j]->N, n, meta[j], g->pinned[k] + g->meta_off[j]);
+    if ((int)any != g->ctf[j])
+      return fail(FR_EINVAL_PARAM, "job %d: the graph was captured %s a CTF phase flip", j,
+                  g->ctf[j] ? "with" : "without");
+  }
+  g->next ^= 1;
+  for (fr_recon *r : g->jobs) TRY(stream_enter(r, st));
+  bool host_src = false;
+  for (int j = 0; j < nj; j++) {
+    const int n = g->counts[j];
+    if (n == 0) continue;
+    const unsigned char *blk = g->pinned[k] + g->meta_off[j];
+    const unsigned char *txy = blk + cs * n;
+    const unsigned char *w = txy + sizeof(float) * 2 * n;
+    const unsigned char *rot = w + sizeof(float) * n;
+    fr::JobBufs &jb = g->bufs[j];
+    CU(cudaMemcpyAsync(jb.ctf.p, blk, cs * n, cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(jb.txy.p, txy, sizeof(float) * 2 * n, cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(jb.w.p, w, sizeof(float) * n, cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(jb.rot.p, rot, sizeof(float) * 9 * n, cudaMemcpyHostToDevice, st));
+  }
+  CU(cudaEventRecord(g->staged[k], st));
+  g->staged_used[k] = true;
+  for (int j = 0; imgs && j < nj; j++) {
+    const int n = g->counts[j];
+    if (n == 0 || imgs[j] == g->slots[j].as<float>()) continue;
+    const size_t bytes = sizeof(float) * (size_t)n * g->boxes[j] * g->boxes[j];
+    host_src |= !is_device_ptr(imgs[j]);
+    CU(cudaMemcpyAsync(g->slots[j].p, imgs[j], bytes, cudaMemcpyDefault, st));
+  }
+  CU(cudaGraphLaunch(g->exec, st));
+  note_launch((int)g->kernels);
+  for (fr_recon *r : g->jobs) TRY(stream_leave(r, st));
+  if (host_src) CU(cudaStreamSynchronize(st));   // host images may be pinned: read them first
+  return FR_OK;
+}
+
+int fr_graph_destroy(fr_graph *g) {
+  if (!g) return FR_OK;
+  {
+    std::lock_guard<std::mutex> lk(g->mu);
+    cudaStreamSynchronize(g->st);
+  }
+  graph_free(g);
+  return FR_OK;
 }
 
 int fr_batch_finish(fr_batch *b, int job, int doift, float *out, float *normout) {

@@ -182,6 +182,11 @@ int alloc_volume(fr_recon *r);
 // Prologue of one chunk of device particles into r's scratch: s_slices,
 // s_t3d and s_w hold the chunk's slices, composed rotations and weights.
 int prologue_chunk(fr_recon *r, const float *d_raw, int n, int box, const fr_particle *meta);
+// Its halves: metadata block on the host, upload, device work only.
+size_t prologue_meta_bytes(int n);
+bool prologue_meta(int N, int n, const fr_particle *meta, unsigned char *blk);
+int prologue_upload(fr_recon *r, int n, const unsigned char *blk, cudaStream_t st);
+int prologue_device(fr_recon *r, const float *d_raw, int n, int box, bool any_ctf);
 int particles_chunk(fr_recon *r, const float *d_raw, int n, int box, const fr_particle *meta,
                     int schedule);
 }  // namespace fr

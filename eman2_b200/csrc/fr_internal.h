@@ -52,6 +52,7 @@ struct InsertJob {
 
 // Launch accounting (fr_api.cu).
 void note_launch(int n = 1);
+long long launches_noted();
 
 // fast_exp(-r*h) as a function of r: the table index is monotone in r, so
 // it is a step function with thresholds R_k.  Bins of width 1/K (K a power

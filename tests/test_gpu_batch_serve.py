@@ -80,6 +80,53 @@ def test_autotune_and_mixed_schedules_in_one_batch(gpu):
         assert oracle.rel_l2(got[j][0], d0) < RTOL and oracle.rel_l2(got[j][1], n0) < RTOL
 
 
+def _split(ps, meta_fn, a, b):
+    return ps.images[a:b], meta_fn(ps.rots[a:b], ps.shifts[a:b], ps.weights[a:b],
+                                   defocus=ps.defocus[a:b])
+
+
+def test_graph_replays_equal_batched_rounds(gpu):
+    """Two replays of a captured round (new particles each time, then the
+    slots as filled) give each job what two batched calls give it."""
+    import torch
+
+    from eman2_b200.batch import BatchReconstructor
+    from eman2_b200.particles import particle_meta
+    jobs = _jobs()
+    half = [len(ps.images) // 2 for _, ps, _ in jobs]
+    first = [_split(ps, particle_meta, 0, h) for (_, ps, _), h in zip(jobs, half)]
+    second = [_split(ps, particle_meta, h, 2 * h) for (_, ps, _), h in zip(jobs, half)]
+    ctf = [bool(np.any(np.abs(ps.defocus) > 1e-4)) for _, ps, _ in jobs]
+    boxes = [ps.images.shape[-1] for _, ps, _ in jobs]
+    b1 = BatchReconstructor([p for p, _, _ in jobs])
+    for part in (first, second, second):
+        b1.insert_particles([im for im, _ in part], [m for _, m in part])
+    b2 = BatchReconstructor([p for p, _, _ in jobs])
+    g = b2.capture(boxes, half, ctf)
+    g.launch([torch.as_tensor(im, device="cuda") for im, _ in first], [m for _, m in first])
+    g.launch([im for im, _ in second], [m for _, m in second])      # host images
+    g.launch(None, [m for _, m in second])                           # the slots as filled
+    torch.cuda.synchronize()
+    for j in range(len(jobs)):
+        d1, n1 = b1.get_accumulators(j)
+        d2, n2 = b2.get_accumulators(j)
+        assert oracle.rel_l2(d2, d1) < RTOL and oracle.rel_l2(n2, n1) < RTOL
+    g.close()
+
+
+def test_graph_rejects_ctf_mismatch(gpu):
+    from eman2_b200.batch import BatchReconstructor
+    from eman2_b200.exceptions import InvalidParameterException
+    from eman2_b200.particles import particle_meta
+    params, ps, meta = _jobs()[0]                 # particles with a CTF
+    b = BatchReconstructor([params])
+    g = b.capture([ps.images.shape[-1]], [8], [False])
+    im, m = _split(ps, particle_meta, 0, 8)
+    with pytest.raises(InvalidParameterException):
+        g.launch([im], [m])
+    g.close()
+
+
 def test_served_result_equals_alone(gpu):
     """Requests arriving at different times, split into chunks, admitted by
     footprint and batched together: each result equals the job run alone."""
