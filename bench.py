@@ -311,6 +311,100 @@ def percentile(v, q):
     return float(np.percentile(np.asarray(v, np.float64), q)) if len(v) else None
 
 
+# ------------------------------------------------------------------ batched
+def run_batched(dev, seed: int = 33, pairs: int = 32, reps: int = 5, plain_sample: int = 16):
+    """The batched form on a round of SURVEY config 3's shape: 32 even/odd
+    half-map pairs (64 reconstructions), boxes {64, 96, 128, 160} padded x1.5,
+    sym c1/d7, gauss_2/gauss_5 (each 50/50), CTF; per round every job inserts
+    a chunk of log-uniform [64, 512] particles.  Schedules come from the
+    autotuner; the round is captured once as a CUDA graph and replayed.
+    Reported beside the same rounds without the graph and the plain
+    per-particle path (sampled)."""
+    import torch
+
+    from eman2_b200 import FourierReconstructor, _lib
+    from eman2_b200.batch import BatchReconstructor, autotune, insert_particles_multi, set_tile
+    from eman2_b200.particles import particle_meta
+    from eman2_b200.synth import make_particles
+    rng = np.random.default_rng(seed)
+    sizes = (64, 96, 128, 160)
+    pools = {b: make_particles(b, 1024, seed=seed + b, snr=0.05, shift=4.0, weights=(0.5, 1.0),
+                               ctf=True, device=dev) for b in sizes}
+    params, boxes, counts, imgs, metas = [], [], [], [], []
+    for _ in range(pairs):
+        b = int(rng.choice(sizes))
+        sym, mode = str(rng.choice(["c1", "d7"])), str(rng.choice(["gauss_2", "gauss_5"]))
+        n = int(np.exp(rng.uniform(np.log(64), np.log(512))))
+        for half in range(2):                       # even / odd particles of one phantom
+            idx = np.arange(half, 2 * n, 2) % 1024
+            ps = pools[b]
+            params.append({"size": [b * 3 // 2] * 3, "sym": sym, "mode": mode})
+            boxes.append(b)
+            counts.append(n)
+            imgs.append(ps.images[idx])
+            metas.append(particle_meta(ps.rots[idx], ps.shifts[idx], ps.weights[idx],
+                                       defocus=ps.defocus[idx]))
+    total = sum(counts)
+    combos = {}
+    for p, n in zip(params, counts):
+        key = (p["size"][0], p["mode"], nsym_of(p["sym"]))
+        combos[key] = max(combos.get(key, 0), n)
+    tuned = {f"N{k[0]} {k[1]} nsym{k[2]}": autotune(k[0], k[1], k[2], nparticles=n)[0]
+             for k, n in combos.items()}
+    stream = torch.cuda.Stream(device=dev)
+
+    def timed(fn):
+        for _ in range(2):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    try:
+        b1 = BatchReconstructor(params)
+        ms_multi = timed(lambda: insert_particles_multi(b1.recons, imgs, metas, stream))
+        b1.close()
+        b2 = BatchReconstructor(params)
+        t0 = time.perf_counter()
+        g = b2.capture(boxes, counts, [True] * len(params), stream=stream)
+        capture_s = time.perf_counter() - t0
+        ms_graph = timed(lambda: g.launch(imgs, metas))
+        g.close()
+        b2.close()
+    finally:
+        for k in combos:
+            set_tile(k[0], k[1], k[2], -1)
+    sz = ctypes.sizeof(_lib.fr_particle)
+    spent, done = 0.0, 0
+    for j in range(0, len(params), 4):
+        rec = FourierReconstructor(params[j])
+        rec.setup()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for i in range(min(plain_sample, counts[j])):
+            one = (_lib.fr_particle * 1).from_address(ctypes.addressof(metas[j]) + i * sz)
+            rec.insert_particles(imgs[j][i:i + 1], one, schedule="scatter")
+        torch.cuda.synchronize()
+        spent += time.perf_counter() - t0
+        done += min(plain_sample, counts[j])
+        rec.close()
+    plain = done / spent
+    graph_rate = total / (ms_graph / 1e3)
+    return {"jobs": len(params), "particles_per_round": total,
+            "graph": {"ms_per_round": ms_graph, "particle_slices_per_s": graph_rate,
+                      "capture_s": capture_s},
+            "no_graph": {"ms_per_round": ms_multi, "particle_slices_per_s": total / (ms_multi / 1e3)},
+            "plain_per_particle": {"particle_slices_per_s": plain,
+                                   "sample": f"{plain_sample} particles of every 4th job"},
+            "speedup_batched_vs_plain": graph_rate / plain,
+            "autotuned": tuned}
+
+
 # ------------------------------------------------------------------ GPU run
 def run_gpu(args, wl, ws, rank, local):
     import torch
@@ -403,7 +497,7 @@ def main():
     ap.add_argument("--batch", type=int, default=2048, help="particles per step")
     ap.add_argument("--plain", type=int, default=64, help="particles timed on the plain path")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--no-serve", action="store_true", help="skip the serving latency leg")
+    ap.add_argument("--no-serve", action="store_true", help="skip the batched and serving legs")
     ap.add_argument("--tile", type=int, default=-1,
                     help="pin the insertion kernel (0-3 register tiles, 4 staged column, "
                          "5 barrier-free column, -2 scatter); default: library choice")
@@ -491,6 +585,7 @@ def main():
                              "speedup_batched_vs_plain": value / plain}
     if not args.no_serve and ws == 1:
         import torch
+        line["batched"] = run_batched(torch.device("cuda", local))
         line["serving"] = run_serving(torch.device("cuda", local))
     if not args.no_cpu and ws == 1:
         v, n, thr, secs = cpu_sample(wl, seed=7000)

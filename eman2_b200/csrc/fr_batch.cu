@@ -684,36 +684,47 @@ int fr_autotune(int N, int mode, int nsym, int nparticles, int *tile_out, float 
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
+  // inputs staged on the device so the timing covers the insertion only
+  DevBuf ds, dr, dw;
+  if (rc == FR_OK) rc = ds.ensure(sizeof(float) * sl.size());
+  if (rc == FR_OK) rc = dr.ensure(sizeof(float) * rot.size());
+  if (rc == FR_OK) rc = dw.ensure(sizeof(float) * w.size());
+  if (rc == FR_OK &&
+      (cudaMemcpy(ds.p, sl.data(), sizeof(float) * sl.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+       cudaMemcpy(dr.p, rot.data(), sizeof(float) * rot.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+       cudaMemcpy(dw.p, w.data(), sizeof(float) * w.size(), cudaMemcpyHostToDevice) != cudaSuccess))
+    rc = fail(FR_ECUDA, "autotune: staging failed");
+  int measured = 0;
   for (int cand = 0; cand <= kColumn3Tile + 1 && rc == FR_OK; cand++) {
     const bool scatter = cand == kColumn3Tile + 1;
     r->tile = scatter ? -1 : cand;
     const int sched = scatter ? FR_SCHED_SCATTER : FR_SCHED_GATHER;
-    // one warm-up call, then one timed call
-    rc = fr_insert_slices(r, sl.data(), nparticles, rot.data(), w.data(), nullptr, 0, nullptr, sched);
-    if (rc != FR_OK) break;
-    // stage inputs on the device so the timing covers the insertion only
-    float ms = 0;
-    {
-      DevBuf ds, dr, dw;
-      if ((rc = ds.ensure(sizeof(float) * sl.size())) != FR_OK) break;
-      if ((rc = dr.ensure(sizeof(float) * rot.size())) != FR_OK) break;
-      if ((rc = dw.ensure(sizeof(float) * w.size())) != FR_OK) break;
-      cudaMemcpy(ds.p, sl.data(), sizeof(float) * sl.size(), cudaMemcpyHostToDevice);
-      cudaMemcpy(dr.p, rot.data(), sizeof(float) * rot.size(), cudaMemcpyHostToDevice);
-      cudaMemcpy(dw.p, w.data(), sizeof(float) * w.size(), cudaMemcpyHostToDevice);
+    // one warm-up call, then one timed call; a schedule that cannot run this
+    // shape (a launch error) is skipped with ms = -1
+    float ms = -1.0f;
+    int crc = fr_insert_slices(r, ds.as<float>(), nparticles, dr.as<float>(), dw.as<float>(),
+                               nullptr, 0, nullptr, sched);
+    if (crc == FR_OK) {
       cudaEventRecord(e0, r->stream);
-      rc = fr_insert_slices(r, ds.as<float>(), nparticles, dr.as<float>(), dw.as<float>(), nullptr,
-                            0, nullptr, sched);
+      crc = fr_insert_slices(r, ds.as<float>(), nparticles, dr.as<float>(), dw.as<float>(),
+                             nullptr, 0, nullptr, sched);
       cudaEventRecord(e1, r->stream);
-      cudaEventSynchronize(e1);
-      cudaEventElapsedTime(&ms, e0, e1);
-      ds.release();
-      dr.release();
-      dw.release();
+      if (cudaEventSynchronize(e1) != cudaSuccess) crc = FR_ECUDA;
+      if (crc == FR_OK) cudaEventElapsedTime(&ms, e0, e1);
+    }
+    if (crc != FR_OK) {
+      cudaGetLastError();
+      ms = -1.0f;
+    } else {
+      measured++;
     }
     if (ms_out) ms_out[cand] = ms;
-    if (ms < best) { best = ms; best_tile = scatter ? kTunedScatter : cand; }
+    if (ms >= 0 && ms < best) { best = ms; best_tile = scatter ? kTunedScatter : cand; }
   }
+  if (rc == FR_OK && measured == 0) rc = fail(FR_ECUDA, "autotune: no schedule ran");
+  ds.release();
+  dr.release();
+  dw.release();
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   fr_destroy(r);
