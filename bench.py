@@ -311,6 +311,61 @@ def percentile(v, q):
     return float(np.percentile(np.asarray(v, np.float64), q)) if len(v) else None
 
 
+# ------------------------------------------------------------------ finish
+def run_finish(dev, wl: dict, reps: int = 3):
+    """finish(True) + math.gausskernelfix + centred clip to the box (what
+    e2make3dpar does after the last insert) on a seeded N^3 volume: the fused
+    fr_finish_corrected against finish, the processor and the clip as three
+    device passes.  Device-timed with CUDA events, outputs in HBM."""
+    import torch
+
+    from eman2_b200 import FourierReconstructor, _lib
+    lib = _lib.load()
+    N, box = wl["N"], wl["box"]
+    width = FourierReconstructor.KERNEL_FIX_WIDTH.get(wl["mode"], 0.0)
+    g = torch.Generator(device=dev).manual_seed(5)
+    seed = torch.randn((N, N, N + 2), device=dev, generator=g)
+    wts = torch.rand((N, N, N // 2 + 1), device=dev, generator=g) + 0.5
+    stream = torch.cuda.Stream(device=dev)
+    full = torch.empty((N, N, N), device=dev)
+    out = torch.empty((box, box, box), device=dev)
+    torch.cuda.synchronize()
+    r = FourierReconstructor({"size": [N] * 3, "sym": wl["sym"], "mode": wl["mode"]})
+    r.setup()
+    _lib.check(lib.fr_set_stream(r.handle, ctypes.c_void_p(stream.cuda_stream)))
+    x0 = (N - box) // 2
+
+    def fused():
+        r.setup_seedandweights(seed, wts)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        _lib.check(lib.fr_finish_corrected(r.handle, width, box, box, box, out.data_ptr(), None))
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+
+    def separate():
+        r.setup_seedandweights(seed, wts)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        _lib.check(lib.fr_finish(r.handle, 1, full.data_ptr(), None))
+        _lib.check(lib.fr_kernel_fix(full.data_ptr(), N, N, N, width,
+                                     ctypes.c_void_p(stream.cuda_stream)))
+        with torch.cuda.stream(stream):
+            out.copy_(full[x0:x0 + box, x0:x0 + box, x0:x0 + box])
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+
+    for f in (fused, separate):
+        f()
+    t_fused = min(fused() for _ in range(reps))
+    t_sep = min(separate() for _ in range(reps))
+    r.close()
+    return {"N": N, "out": box, "gauss_width": width, "fused_ms": t_fused, "separate_ms": t_sep,
+            "note": "normalize + c2r 3-D + depad/centre/scale + kernel fix + clip"}
+
+
 # ------------------------------------------------------------------ batched
 def run_batched(dev, seed: int = 33, pairs: int = 32, reps: int = 5, plain_sample: int = 16):
     """The batched form on a round of SURVEY config 3's shape: 32 even/odd
@@ -585,6 +640,7 @@ def main():
                              "speedup_batched_vs_plain": value / plain}
     if not args.no_serve and ws == 1:
         import torch
+        line["finish"] = run_finish(torch.device("cuda", local), wl)
         line["batched"] = run_batched(torch.device("cuda", local))
         line["serving"] = run_serving(torch.device("cuda", local))
     if not args.no_cpu and ws == 1:

@@ -15,7 +15,7 @@ reconstructions per launch (``eman2_b200.batch``) and a serving loop
 (``eman2_b200.server``).  The compute runs in libeman2_b200.so (CUDA for
 sm_100a) through a C ABI (include/eman2_b200.h).
 """
-from .emdata import EMData
+from .emdata import EMData, Region
 from .exceptions import (DeviceException, ImageDimensionException, InvalidParameterException,
                          NotExistingObjectException, NullPointerException, StateException,
                          UnsupportedParameterException)
@@ -23,7 +23,7 @@ from .reconstructor import FourierReconstructor, Reconstructors
 from .transform import Transform
 
 __all__ = [
-    "EMData", "Transform", "Reconstructors", "FourierReconstructor",
+    "EMData", "Region", "Transform", "Reconstructors", "FourierReconstructor",
     "InvalidParameterException", "ImageDimensionException", "NullPointerException",
     "NotExistingObjectException", "StateException", "DeviceException",
     "UnsupportedParameterException",

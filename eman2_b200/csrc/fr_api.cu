@@ -975,4 +975,57 @@ int fr_finish(fr_recon *r, int doift, float *out, float *normout) {
   return FR_OK;
 }
 
+int fr_finish_corrected(fr_recon *r, float gauss_width, int outx, int outy, int outz, float *out,
+                        float *normout) {
+  TRY(check_state(r));
+  if (!out) return fail(FR_ENULL, "null output");
+  const int N = r->N;
+  if (outx <= 0 || outy <= 0 || outz <= 0 || outx > N || outy > N || outz > N)
+    return fail(FR_EINVAL_PARAM, "clip size %d %d %d outside (0, %d]", outx, outy, outz, N);
+  std::lock_guard<std::mutex> lk(r->mu);
+  TRY(stream_enter(r, r->stream));
+  cudaStream_t st = r->stream;
+  TRY(check_device_error(r));
+  CU(launch_normalize(r->vol_data.as<float>(), r->vol_norm.as<float>(), N, r->p.sqrtnorm, st));
+  if (normout) TRY(from_device(normout, r->vol_norm.p, norm_floats(N) * sizeof(float), st));
+  cufftHandle plan;
+  TRY(r->plans.get3d(N, st, &plan));
+  CUFFT(cufftExecC2R(plan, r->vol_data.as<cufftComplex>(), r->vol_data.as<cufftReal>()));
+  const float scale = 1.0f / (float)((size_t)N * N * N);
+  const size_t bytes = sizeof(float) * (size_t)outx * outy * outz;
+  if (is_device_ptr(out)) {
+    CU(launch_finish_out(r->vol_data.as<float>(), N, scale, gauss_width, outx, outy, outz, out, st));
+  } else {
+    TRY(r->s_out.ensure(bytes));
+    CU(launch_finish_out(r->vol_data.as<float>(), N, scale, gauss_width, outx, outy, outz,
+                         r->s_out.as<float>(), st));
+    TRY(from_device(out, r->s_out.p, bytes, st));
+  }
+  CU(cudaStreamSynchronize(st));
+  r->state = 2;
+  return FR_OK;
+}
+
+int fr_kernel_fix(float *vol, int nx, int ny, int nz, float gauss_width, void *stream) {
+  if (!vol) return fail(FR_ENULL, "null volume");
+  if (nx <= 0 || ny <= 0 || nz <= 0) return fail(FR_EDIM, "bad volume size %d %d %d", nx, ny, nz);
+  cudaStream_t st = (cudaStream_t)stream;
+  const size_t bytes = sizeof(float) * (size_t)nx * ny * nz;
+  if (is_device_ptr(vol)) {
+    CU(launch_kernel_fix(vol, nx, ny, nz, gauss_width, st));
+    CU(cudaStreamSynchronize(st));
+    return FR_OK;
+  }
+  DevBuf d;
+  TRY(d.ensure(bytes));
+  int rc = FR_OK;
+  if (cudaMemcpyAsync(d.p, vol, bytes, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+      launch_kernel_fix(d.as<float>(), nx, ny, nz, gauss_width, st) != cudaSuccess ||
+      cudaMemcpyAsync(vol, d.p, bytes, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    rc = fail(FR_ECUDA, "kernel fix failed: %s", cudaGetErrorString(cudaGetLastError()));
+  d.release();
+  return rc;
+}
+
 }  // extern "C"

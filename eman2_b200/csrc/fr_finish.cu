@@ -91,6 +91,71 @@ cudaError_t launch_depad_center(const float *d_real_padded, int N, float scale, 
   return cudaGetLastError();
 }
 
+// math.gausskernelfix: MaskGaussInvProcessor (libEM/processor.h:4131-4176)
+// run by CoordinateProcessor::process_inplace (libEM/processor.cpp:2439-2473)
+// divides each voxel by exp(-dist * gauss_width / (ny*ny)), dist the squared
+// distance (float, as CircularMaskProcessor::process_pixel forms it,
+// libEM/processor.h:3785-3789) to (floor(nx/2), floor(ny/2), floor(nz/2)).
+// The quotient is taken in double and rounded once.
+__device__ __forceinline__ float kernel_fix(float v, int x, int y, int z, float xc, float yc,
+                                            float zc, float sv) {
+  const float dx = __fsub_rn((float)x, xc), dy = __fsub_rn((float)y, yc),
+              dz = __fsub_rn((float)z, zc);
+  const float dist = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+  const float f = __fmul_rn(-dist, sv);
+  return (float)((double)v / exp((double)f));
+}
+
+__global__ void k_kernel_fix(float *__restrict__ vol, int nx, int ny, int nz, float sv) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (long)nx * ny * nz) return;
+  const int x = (int)(i % nx), y = (int)((i / nx) % ny), z = (int)(i / ((long)nx * ny));
+  vol[i] = kernel_fix(vol[i], x, y, z, floorf(nx / 2.0f), floorf(ny / 2.0f), floorf(nz / 2.0f), sv);
+}
+
+cudaError_t launch_kernel_fix(float *d_vol, int nx, int ny, int nz, float gauss_width,
+                              cudaStream_t st) {
+  const long n = (long)nx * ny * nz;
+  if (n == 0) return cudaSuccess;
+  const float sv = gauss_width / (float)(ny * ny);   // gauss_width / (ny * ny), float
+  note_launch();
+  k_kernel_fix<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(d_vol, nx, ny, nz, sv);
+  return cudaGetLastError();
+}
+
+// The end of e2make3dpar's reconstruction (programs/e2make3dpar.py:421-431)
+// fused into finish's last pass: depad + phase origin to centre + 1/N^3
+// (as k_depad_center), the radial kernel correction when sv > 0, and the
+// clip to the centred (onx, ony, onz) region starting at (x0, y0, z0).
+__global__ void k_finish_out(const float *__restrict__ in, int N, float scale, float sv, int x0,
+                             int y0, int z0, int onx, int ony, int onz, float *__restrict__ out) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (long)onx * ony * onz) return;
+  const int x = x0 + (int)(i % onx), y = y0 + (int)((i / onx) % ony),
+            z = z0 + (int)(i / ((long)onx * ony));
+  const int h = N / 2;
+  const int sx = (x + h) % N, sy = (y + h) % N, sz = (z + h) % N;
+  float v = __fmul_rn(in[((long)sz * N + sy) * (N + 2) + sx], scale);
+  if (sv > 0.0f) {
+    const float c = floorf(N / 2.0f);
+    v = kernel_fix(v, x, y, z, c, c, c, sv);
+  }
+  out[i] = v;
+}
+
+cudaError_t launch_finish_out(const float *d_real_padded, int N, float scale, float gauss_width,
+                              int onx, int ony, int onz, float *d_out, cudaStream_t st) {
+  const long n = (long)onx * ony * onz;
+  if (n == 0) return cudaSuccess;
+  const float sv = gauss_width > 0.0f ? gauss_width / (float)(N * N) : 0.0f;
+  // Region((nx-outx)/2, ...) with Python floor division
+  const int x0 = (N - onx) / 2, y0 = (N - ony) / 2, z0 = (N - onz) / 2;
+  note_launch();
+  k_finish_out<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(d_real_padded, N, scale, sv, x0, y0,
+                                                           z0, onx, ony, onz, d_out);
+  return cudaGetLastError();
+}
+
 // FourierReconstructor::setup_seed (libEM/reconstructor.cpp:865-895):
 // data = seed * w (mult skips f == 1), norm = w, with the x=0 and x=N/2
 // planes at w/2 and four cells restored to w.

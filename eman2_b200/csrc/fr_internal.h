@@ -138,6 +138,10 @@ cudaError_t launch_shift_corner(const float *d_img_off, const float *d_img_on, c
 cudaError_t launch_normalize(float *d_data, float *d_norm, int N, int sqrtnorm, cudaStream_t st);
 cudaError_t launch_depad_center(const float *d_real_padded, int N, float scale, float *d_out,
                                 cudaStream_t st);
+cudaError_t launch_kernel_fix(float *d_vol, int nx, int ny, int nz, float gauss_width,
+                              cudaStream_t st);
+cudaError_t launch_finish_out(const float *d_real_padded, int N, float scale, float gauss_width,
+                              int onx, int ony, int onz, float *d_out, cudaStream_t st);
 cudaError_t launch_seed(const float *d_seed, float w, int N, float *d_data, float *d_norm,
                         cudaStream_t st);
 cudaError_t launch_agree_rt(const float *d_data, const float *d_norm, int N, const float *d_slices,

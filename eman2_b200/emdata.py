@@ -13,6 +13,14 @@ import numpy as np
 from .exceptions import NotExistingObjectException
 
 
+class Region:
+    """Region(x0, y0, z0, nx, ny, nz) (libEM/geometry.h)."""
+
+    def __init__(self, x0, y0, z0=0, nx=1, ny=1, nz=1):
+        self.origin = (int(x0), int(y0), int(z0))
+        self.size = (int(nx), int(ny), int(nz))
+
+
 class EMData:
     def __init__(self, data=None, nx=None, ny=None, nz=1, is_complex=False, attrs=None):
         if data is None:
@@ -50,6 +58,34 @@ class EMData:
 
     def copy(self) -> "EMData":
         return EMData(self._data.copy(), is_complex=self._complex, attrs=dict(self.attrs))
+
+    # ------------------------------------------------------------- processing
+    def process_inplace(self, name: str, params: dict | None = None):
+        """EMData::process_inplace for the processors this path uses:
+        math.gausskernelfix (MaskGaussInvProcessor, libEM/processor.h:4131-4176),
+        run on the GPU."""
+        params = params or {}
+        if name == "math.gausskernelfix":
+            if self._complex:
+                return        # CoordinateProcessor::is_valid: real images only
+            from . import _lib
+            _lib.check(_lib.load().fr_kernel_fix(
+                _lib.ptr(self._data), self.get_xsize(), self.get_ysize(), self.get_zsize(),
+                float(params.get("gauss_width", 0.0)), None))
+            return
+        raise NotExistingObjectException(f"No such an instance existing: {name}")
+
+    def clip_inplace(self, region: "Region"):
+        """EMData::clip_inplace to a region inside the image (zero fill outside)."""
+        x0, y0, z0, nx, ny, nz = region.origin + region.size
+        src = self._data if self._data.ndim == 3 else self._data[None]
+        out = np.zeros((nz, ny, nx), np.float32)
+        zs, ys, xs = src.shape
+        sz = slice(max(0, z0), min(zs, z0 + nz)); sy = slice(max(0, y0), min(ys, y0 + ny))
+        sx = slice(max(0, x0), min(xs, x0 + nx))
+        out[sz.start - z0:sz.stop - z0, sy.start - y0:sy.stop - y0, sx.start - x0:sx.stop - x0] = \
+            src[sz, sy, sx]
+        self._data = out if self._data.ndim == 3 else out[0]
 
     def complex_view(self) -> np.ndarray:
         """The complex64 view of a complex image (..., nx/2)."""

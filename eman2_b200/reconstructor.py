@@ -430,6 +430,37 @@ class FourierReconstructor:
             np.save(str(self.params["savenorm"]), norm)
         return EMData(out, is_complex=not doift)
 
+    # e2make3dpar's Gaussian widths per mode (programs/e2make3dpar.py:422)
+    KERNEL_FIX_WIDTH = {"gauss_2": 4.0, "gauss_3": 6.4, "gauss_4": 8.8, "gauss_5": 10.4,
+                        "gauss_5_slow": 10.4}
+
+    def finish_corrected(self, gauss_width: float | None = None, outsize=None) -> EMData:
+        """finish(True) plus what e2make3dpar does next (programs/e2make3dpar.py:421-431):
+        math.gausskernelfix with the mode's Gaussian width (or ``gauss_width``;
+        0 or a mode without one: no correction) and the clip to ``outsize``
+        (an int or (x, y, z); default N), fused into the pass that writes the
+        real map."""
+        if self._state != 1:
+            self._require_setup()
+        N = self.N
+        if gauss_width is None:
+            gauss_width = self.KERNEL_FIX_WIDTH.get(self.params.get("mode", "gauss_2"), 0.0)
+        if outsize is None:
+            outsize = (N, N, N)
+        elif np.isscalar(outsize):
+            outsize = (int(outsize),) * 3
+        ox, oy, oz = (int(v) for v in outsize)
+        out = np.empty((oz, oy, ox), np.float32)
+        norm = np.empty((N, N, N // 2 + 1), np.float32)
+        _lib.check(_lib.load().fr_finish_corrected(self._h, float(gauss_width), ox, oy, oz,
+                                                   _lib.ptr(out), _lib.ptr(norm)))
+        self._state = 2
+        if "normout" in self.params and isinstance(self.params["normout"], EMData):
+            self.params["normout"].set_data(norm)
+        if self.params.get("savenorm"):
+            np.save(str(self.params["savenorm"]), norm)
+        return EMData(out)
+
     def _require_setup(self):
         raise StateException("setup() has not been called" if self._state == 0 else
                              "finish() was called; call setup() again")

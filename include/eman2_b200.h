@@ -162,6 +162,21 @@ FR_API int fr_projection(fr_recon *r, const float *rot, float *out_slice);
  * The handle needs fr_setup() again afterwards (ownership passes out). */
 FR_API int fr_finish(fr_recon *r, int doift, float *out, float *normout);
 
+/* finish(True) followed by what e2make3dpar does with the map
+ * (programs/e2make3dpar.py:421-431): the radial kernel correction
+ * math.gausskernelfix with gauss_width (MaskGaussInvProcessor,
+ * libEM/processor.h:4131-4176; <= 0 skips it) and the clip to the centred
+ * outx x outy x outz region (clip_inplace(Region((N-outx)/2, ...))), fused
+ * into the pass that writes the real map.  out: float[outz][outy][outx]. */
+FR_API int fr_finish_corrected(fr_recon *r, float gauss_width, int outx, int outy, int outz,
+                               float *out, float *normout);
+
+/* The processor math.gausskernelfix on a real volume float[nz][ny][nx], host
+ * or device, in place (EMData::process_inplace("math.gausskernelfix",
+ * {"gauss_width": w}), libEM/processor.h:4131-4176,
+ * libEM/processor.cpp:2439-2473).  stream: NULL for the default stream. */
+FR_API int fr_kernel_fix(float *vol, int nx, int ny, int nz, float gauss_width, void *stream);
+
 /* Un-normalised accumulators (finish(False) + normout before normalisation);
  * the form the reference's parallel make3d merges (programs/e2spa_make3d.py:175-188).
  * Either pointer may be NULL. */

@@ -556,6 +556,27 @@ OR_EXPORT void or_translate_bilinear(const float *src, float *dst, int nx, int n
   }
 }
 
+/* math.gausskernelfix (MaskGaussInvProcessor, libEM/processor.h:4131-4176,
+ * through CoordinateProcessor::process_inplace, libEM/processor.cpp:2439-2473):
+ * centre (floor(nx/2), floor(ny/2), floor(nz/2)), slice_value =
+ * gauss_width / (ny*ny) in float, dist the float squared distance formed as
+ * CircularMaskProcessor::process_pixel does (libEM/processor.h:3785-3789),
+ * and the voxel divided by exp(-dist*slice_value) in double. */
+OR_EXPORT void or_kernel_fix(float *vol, int nx, int ny, int nz, float gauss_width) {
+  const float xc = floorf(nx / 2.0f), yc = floorf(ny / 2.0f), zc = floorf(nz / 2.0f);
+  const float sv = gauss_width / (float)(ny * ny);
+  size_t i = 0;
+  for (int z = 0; z < nz; z++)
+    for (int y = 0; y < ny; y++)
+      for (int x = 0; x < nx; x++, i++) {
+        const float dx = (float)x - xc, dy = (float)y - yc, dz = (float)z - zc;
+        const float dxx = dx * dx, dyy = dy * dy, dzz = dz * dz;
+        const float dist = (dxx + dyy) + dzz;
+        const float f = -dist * sv;
+        vol[i] = (float)((double)vol[i] / exp((double)f));
+      }
+}
+
 OR_EXPORT int or_real_size(void) { return (int)sizeof(real); }
 OR_EXPORT int or_acc_size(void) { return (int)sizeof(acc_t); }
 OR_EXPORT float or_fast_exp_value(float f) { or_init_tables(); return (float)or_fast_exp((real)f); }

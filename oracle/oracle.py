@@ -78,6 +78,7 @@ def _lib(kind: str = "fp32"):
     lib.or_fast_exp_value.argtypes = [ctypes.c_float]
     lib.or_fast_exp_value.restype = ctypes.c_float
     lib.or_hypot_int.argtypes = [ctypes.c_int, ctypes.c_int]
+    lib.or_kernel_fix.argtypes = [_F, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float]
     if kind == "omp":
         lib.or_insert_batch_omp.argtypes = [R, R, ctypes.c_int, ctypes.c_int, _F, ctypes.c_int, _F,
                                             _F, ctypes.c_int, _F, ctypes.c_int]
@@ -215,6 +216,23 @@ class OracleVolume:
             real = real.astype(np.float32) * np.float32(1.0 / (N * N * N))
         real = np.roll(real, (N // 2, N // 2, N // 2), axis=(0, 1, 2))
         return real, self.norm
+
+
+def kernel_fix(vol: np.ndarray, gauss_width: float) -> np.ndarray:
+    """math.gausskernelfix on a real volume (a copy)."""
+    v = np.ascontiguousarray(vol, np.float32).copy()
+    nz, ny, nx = v.shape
+    _lib().or_kernel_fix(_fp(v), nx, ny, nz, float(gauss_width))
+    return v
+
+
+def clip_centre(vol: np.ndarray, outsize) -> np.ndarray:
+    """clip_inplace(Region((nx-ox)//2, (ny-oy)//2, (nz-oz)//2, ox, oy, oz))
+    (programs/e2make3dpar.py:430-431) for a region inside the volume."""
+    nz, ny, nx = vol.shape
+    ox, oy, oz = outsize
+    x0, y0, z0 = (nx - ox) // 2, (ny - oy) // 2, (nz - oz) // 2
+    return np.ascontiguousarray(vol[z0:z0 + oz, y0:y0 + oy, x0:x0 + ox])
 
 
 # ------------------------------------------------------------------- prologue

@@ -236,6 +236,55 @@ def test_finish_matches_oracle(gpu):
         assert rel(out, want) < (RTOL_FFT if doift else RTOL_ACC)
 
 
+def test_kernel_fix_matches_oracle(gpu):
+    """math.gausskernelfix on host and device volumes, cubic and not, equals
+    the oracle's restatement (same float distance, double quotient)."""
+    import torch
+    from eman2_b200 import EMData
+    rng = np.random.default_rng(81)
+    for shape, wdt in [((24, 24, 24), 10.4), ((10, 14, 18), 4.0)]:
+        v = rng.normal(size=shape).astype(np.float32)
+        want = oracle.kernel_fix(v, wdt)
+        e = EMData(v.copy())
+        e.process_inplace("math.gausskernelfix", {"gauss_width": wdt})
+        np.testing.assert_array_max_ulp(e.numpy(), want, maxulp=1)
+        d = torch.as_tensor(v, device="cuda")
+        from eman2_b200 import _lib
+        nz, ny, nx = shape
+        _lib.check(_lib.load().fr_kernel_fix(d.data_ptr(), nx, ny, nz, wdt, None))
+        np.testing.assert_array_max_ulp(d.cpu().numpy(), want, maxulp=1)
+
+
+@pytest.mark.parametrize("mode,width,outsize", [("gauss_5", None, 36), ("gauss_2", 4.0, (30, 32, 34)),
+                                                ("nearest_neighbor", None, 40)])
+def test_finish_corrected_matches_oracle(gpu, mode, width, outsize):
+    """finish(True) + math.gausskernelfix + centred clip (programs/e2make3dpar.py:421-431)
+    in one pass equals the oracle's finish, kernel fix and clip, and the
+    GPU's own unfused sequence bit for bit."""
+    from eman2_b200 import Region
+    N, n = 40, 30
+    sl, rt = rand_slices(N, n, 91), rand_rots(n, 92)
+    w = np.ones(n, np.float32)
+    widths = {"gauss_5": 10.4, "gauss_2": 4.0, "nearest_neighbor": 0.0}
+    wd = widths[mode] if width is None else width
+    osz = (outsize,) * 3 if np.isscalar(outsize) else outsize
+    r = recon(N, mode, "d2")
+    r.insert_slices(sl, rt, w)
+    got = r.finish_corrected(width, outsize).numpy()
+    assert got.shape == (osz[2], osz[1], osz[0])
+    o = oracle_insert(N, sl, rt, w, mode, "d2")
+    real, _ = o.finish(True)
+    want = oracle.clip_centre(oracle.kernel_fix(real, wd) if wd > 0 else real, osz)
+    assert rel(got, want) < RTOL_FFT
+    r2 = recon(N, mode, "d2")
+    r2.insert_slices(sl, rt, w)
+    e = r2.finish(True)
+    if wd > 0:
+        e.process_inplace("math.gausskernelfix", {"gauss_width": wd})
+    e.clip_inplace(Region((N - osz[0]) // 2, (N - osz[1]) // 2, (N - osz[2]) // 2, *osz))
+    assert rel(got, e.numpy()) < RTOL_ACC
+
+
 def test_agreement_matches_oracle(gpu):
     N, n = 32, 30
     sl, rt = rand_slices(N, n, 71), rand_rots(n, 72)

@@ -182,6 +182,22 @@ def test_fp32_and_fp64_oracles_agree():
     assert oracle.rel_l2(b.data, c.data) < 1e-4      # FP32 vs FP64 tap arithmetic
 
 
+def test_kernel_fix_known_values():
+    """math.gausskernelfix (libEM/processor.h:4131-4176): the voxel at
+    (floor(nx/2), floor(ny/2), floor(nz/2)) is unchanged; a voxel at squared
+    distance d is multiplied by exp(d * gauss_width / ny^2), with ny (not nx
+    or nz) in the width's scale."""
+    v = np.ones((6, 8, 10), np.float32)          # nz, ny, nx
+    out = oracle.kernel_fix(v, 4.0)
+    assert out[3, 4, 5] == 1.0
+    sv = np.float32(4.0) / np.float32(64)
+    for (z, y, x) in [(3, 4, 6), (0, 0, 0), (5, 7, 9), (3, 1, 5)]:
+        d = np.float32((x - 5) ** 2 + (y - 4) ** 2 + (z - 3) ** 2)
+        assert out[z, y, x] == np.float32(1.0 / math.exp(float(np.float32(-d * sv))))
+    c = oracle.clip_centre(np.arange(8 * 8 * 8, dtype=np.float32).reshape(8, 8, 8), (4, 6, 2))
+    assert c.shape == (2, 6, 4) and c[0, 0, 0] == 3 * 64 + 1 * 8 + 2
+
+
 @pytest.mark.parametrize("N", [16, 20])
 def test_normalize_weights_conjugate_pairs(N):
     """normalize_threed sums conjugate-pair weights on the x=0 and x=N/2
