@@ -366,6 +366,64 @@ def run_finish(dev, wl: dict, reps: int = 3):
             "note": "normalize + c2r 3-D + depad/centre/scale + kernel fix + clip"}
 
 
+# ------------------------------------------------------------------ I/O
+def run_io(dev, wl: dict, n: int = 16384, chunk: int = 4096):
+    """Particles streamed from a .mrcs stack on local disk (page cache) into a
+    reconstruction of the workload, stored as float32 and as float16, against
+    the same particles already in HBM; one warmed reconstructor for all three
+    (setup() re-zeroes it).  The files are written to a temporary directory
+    and removed afterwards."""
+    import shutil
+    import tempfile
+
+    import torch
+
+    from eman2_b200 import FourierReconstructor, io
+    from eman2_b200.particles import particle_meta
+    from eman2_b200.synth import make_particles
+    B, N = wl["box"], wl["N"]
+    ps = make_particles(B, n, seed=77, snr=wl["snr"], shift=wl["shift"], weights=wl["weights"],
+                        ctf=wl["ctf"], device=dev)
+    meta = particle_meta(ps.rots, ps.shifts, ps.weights, defocus=ps.defocus)
+    sz = ctypes.sizeof(type(meta[0]))
+    d_imgs = ps.images if isinstance(ps.images, torch.Tensor) else torch.as_tensor(ps.images, device=dev)
+    host = d_imgs.cpu().numpy()
+    tmp = tempfile.mkdtemp(prefix="fr_io_")
+    out = {"particles": n, "chunk": chunk, "box": B, "pad": N}
+    r = FourierReconstructor({"size": [N] * 3, "sym": wl["sym"], "mode": wl["mode"]})
+    r.setup()
+
+    def from_hbm():
+        for a in range(0, n, chunk):
+            m = (type(meta[0]) * min(chunk, n - a)).from_address(ctypes.addressof(meta) + a * sz)
+            r.insert_particles(d_imgs[a:a + chunk], m)
+
+    def timed(fn):
+        r.setup()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        fn()
+        torch.cuda.synchronize()
+        return time.perf_counter() - t0
+
+    try:
+        from_hbm()                                           # warm-up: plans, scratch
+        out["hbm_resident_particle_slices_per_s"] = n / timed(from_hbm)
+        for mode, name in ((2, "float32"), (12, "float16")):
+            path = os.path.join(tmp, f"ptcl_{name}.mrcs")
+            io.write_mrc(path, host, mode=mode)
+            io.insert_stack(r, path, meta, chunk=chunk)      # warm-up: page cache, pinned buffers
+            dt = timed(lambda: io.insert_stack(r, path, meta, chunk=chunk))
+            fbytes = n * B * B * (4 if mode == 2 else 2)
+            out[name] = {"particle_slices_per_s": n / dt, "file_gbs": fbytes / dt / 1e9,
+                         "file_bytes": fbytes}
+    finally:
+        r.close()
+        shutil.rmtree(tmp, ignore_errors=True)
+    out["source"] = "page cache of local disk; file read by 16 threads into pinned buffers"
+    return out
+
+
 # ------------------------------------------------------------------ batched
 def run_batched(dev, seed: int = 33, pairs: int = 32, reps: int = 5, plain_sample: int = 16):
     """The batched form on a round of SURVEY config 3's shape: 32 even/odd
@@ -641,6 +699,7 @@ def main():
     if not args.no_serve and ws == 1:
         import torch
         line["finish"] = run_finish(torch.device("cuda", local), wl)
+        line["io"] = run_io(torch.device("cuda", local), WORKLOADS["c2"])
         line["batched"] = run_batched(torch.device("cuda", local))
         line["serving"] = run_serving(torch.device("cuda", local))
     if not args.no_cpu and ws == 1:

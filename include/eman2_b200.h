@@ -297,6 +297,14 @@ FR_API int fr_autotune(int N, int mode, int nsym, int nparticles, int *tile_out,
                        float *ms_out);
 FR_API int fr_set_tile(int N, int mode, int nsym, int tile);
 
+/* Decodes n raw image values of MRC mode `mode` (0 unsigned bytes, 17 signed
+ * bytes, 101 packed 4-bit, 1 int16, 6 uint16, 12 float16, 2 float32; swap:
+ * the file's byte order is not the host's) from device bytes into float32,
+ * as MrcIO::read_data converts them (libEM/io/mrcio.cpp:1040-1140), so stacks
+ * cross PCIe in their stored width.  Asynchronous on `stream`. */
+FR_API int fr_decode_images(const void *d_src, int mode, int swap, long long n, float *d_dst,
+                            void *stream);
+
 /* Measured roofs of the scattered accumulation, in taps/s (a tap adds a
  * complex value and a weight to one voxel): conflict-free float4
  * read-modify-write in shared memory (the column kernel's update), FP32
