@@ -19,11 +19,12 @@ from .emdata import EMData, Region
 from .exceptions import (DeviceException, ImageDimensionException, InvalidParameterException,
                          NotExistingObjectException, NullPointerException, StateException,
                          UnsupportedParameterException)
-from .reconstructor import FourierReconstructor, Reconstructors
+from .reconstructor import FourierReconstructor, Reconstructors, WienerFourierReconstructor
 from .transform import Transform
 
 __all__ = [
     "EMData", "Region", "Transform", "Reconstructors", "FourierReconstructor",
+    "WienerFourierReconstructor",
     "InvalidParameterException", "ImageDimensionException", "NullPointerException",
     "NotExistingObjectException", "StateException", "DeviceException",
     "UnsupportedParameterException",

@@ -84,6 +84,9 @@ SIGNATURES = {
                     ctypes.c_int),
     "fr_set_tile": ([ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int),
     "fr_update_peaks": ([_P, _P, _P], ctypes.c_int),
+    "fr_set_wiener": ([_P, ctypes.c_int], ctypes.c_int),
+    "fr_insert_slices_wiener": ([_P, _P, ctypes.c_int, _P, _P, _P, ctypes.c_int, _P, _P],
+                                ctypes.c_int),
     "fr_decode_images": ([_P, ctypes.c_int, ctypes.c_int, ctypes.c_longlong, _P, _P], ctypes.c_int),
     "fr_finish_corrected": ([_P, ctypes.c_float, ctypes.c_int, ctypes.c_int, ctypes.c_int, _P, _P],
                             ctypes.c_int),

@@ -159,8 +159,15 @@ Geom *get_geom(int N, int corners) {
   for (int y = -n2; y < n2; y++) {
     int xm = -1;
     for (int x = 0; x <= n2; x++) {
-      const int r = hypot_fast_int(x, y);
-      if (!corners && r > n2) continue;   // (r > iny/2 && abs(inx-iny) < 3): square input
+      if (corners == 2) {
+        // WienerFourierReconstructor: rn = (float)hypot(x/(inx-2), y/iny) < .5
+        // (libEM/reconstructor.cpp:1703-1707)
+        const float rx = (float)x / (float)N, ry = (float)y / (float)N;
+        if ((float)std::hypot((double)rx, (double)ry) >= 0.5f) continue;
+      } else {
+        const int r = hypot_fast_int(x, y);
+        if (!corners && r > n2) continue;   // (r > iny/2 && abs(inx-iny) < 3): square input
+      }
       xm = x;                              // kept pixels form a prefix of the row
       npix++;
       // Pixels that can reach a cube face (|i|, |j| or |k| = N/2): their
@@ -313,6 +320,9 @@ InsertJob make_job(fr_recon *r, const float2 *slices, const float *t3d, const fl
   j.rtab = r->geom->d_rtab;
   j.rim = r->geom->d_rim;
   j.nrim = r->geom->nrim;
+  j.wsnr = nullptr;
+  j.wundo = nullptr;
+  j.nwsnr = 0;
   j.ssnr = nullptr;
   j.nssnr = 0;
   j.sscale = 1.0f;
@@ -334,6 +344,8 @@ int run_scatter(const InsertJob &j0, bool edge_only, cudaStream_t st) {
     j.t3d = j0.t3d + (size_t)p0 * j0.nsym * 9;
     j.pw = j0.pw + p0;
     if (j0.ssnr) j.ssnr = j0.ssnr + (size_t)p0 * j0.nssnr;
+    if (j0.wsnr) j.wsnr = j0.wsnr + (size_t)p0 * j0.nwsnr;
+    if (j0.wundo) j.wundo = j0.wundo + p0;
     CU(edge_only ? launch_edge(j, st) : launch_scatter(j, st));
   }
   return FR_OK;
@@ -850,6 +862,62 @@ int fr_insert_slices(fr_recon *r, const float *slices, int n, const float *rot, 
   return FR_OK;
 }
 
+int fr_set_wiener(fr_recon *r, int on) {
+  if (!r) return fail(FR_ENULL, "null handle");
+  std::lock_guard<std::mutex> lk(r->mu);
+  r->wfilt = on ? 1.0f : 0.0f;
+  return FR_OK;
+}
+
+int fr_insert_slices_wiener(fr_recon *r, const float *slices, int n, const float *rot,
+                            const float *weights, const float *snr, int nsnr, const int *undo,
+                            int *status_out) {
+  TRY(check_state(r));
+  if (n < 0) return fail(FR_EINVAL_PARAM, "negative count");
+  if (n == 0) return FR_OK;
+  if (!slices || !rot || !weights) return fail(FR_ENULL, "EMData pointer (input image) is NULL");
+  if (!snr || nsnr < 1)
+    return fail(FR_ENOTEXIST, "The requested key does not exist: ctf_snr_total (No SNR "
+                "information present in class-average. Must use the ctf.auto or ctfw.auto averager.)");
+  std::lock_guard<std::mutex> lk(r->mu);
+  TRY(stream_enter(r, r->stream));
+  const int N = r->N;
+  cudaStream_t st = r->stream;
+  if (!r->wgeom) r->wgeom = get_geom(N, 2);
+  // WienerFourierReconstructor::insert_slice (libEM/reconstructor.cpp:1643-1677)
+  // inserts every slice (a zero weight still enters through the SNR weights);
+  // the sign of the weight selects subtraction.
+  std::vector<float> w(n);
+  if (is_device_ptr(weights)) CU(cudaMemcpy(w.data(), weights, sizeof(float) * n, cudaMemcpyDeviceToHost));
+  else memcpy(w.data(), weights, sizeof(float) * n);
+  for (int i = 0; i < n; i++) {
+    w[i] = w[i] < 0.0f ? -1.0f : 1.0f;
+    if (status_out) status_out[i] = 0;
+  }
+  const void *d_sl = nullptr, *d_rot = nullptr, *d_snr = nullptr, *d_undo = nullptr;
+  TRY(to_device(slices, sizeof(float) * slice_floats(N) * n, r->s_in, st, &d_sl));
+  TRY(to_device(rot, sizeof(float) * 9 * n, r->s_rot, st, &d_rot));
+  TRY(to_device(snr, sizeof(float) * (size_t)nsnr * n, r->s_ssnr, st, &d_snr));
+  if (undo) TRY(to_device(undo, sizeof(int) * n, r->s_txy, st, &d_undo));
+  TRY(r->s_w.ensure(sizeof(float) * n));
+  CU(cudaMemcpyAsync(r->s_w.p, w.data(), sizeof(float) * n, cudaMemcpyHostToDevice, st));
+  TRY(r->s_t3d.ensure(sizeof(float) * 9 * (size_t)n * r->nsym));
+  CU(launch_compose((const float *)d_rot, r->d_sym.as<float>(), n, r->nsym, r->s_t3d.as<float>(),
+                    st));
+  InsertJob j = make_job(r, (const float2 *)d_sl, r->s_t3d.as<float>(), r->s_w.as<float>(), n);
+  j.xmax = r->wgeom->d_xmax;
+  j.wsnr = (const float *)d_snr;
+  j.nwsnr = nsnr;
+  j.wundo = (const int *)d_undo;
+  g_ins_launches++;
+  g_slices += (long long)n * r->nsym;
+  TRY(run_scatter(j, false, st));
+  TRY(stream_leave(r, st));
+  if (d_sl != slices || d_rot != rot || d_snr != snr || (undo && d_undo != undo))
+    CU(cudaStreamSynchronize(st));
+  return FR_OK;
+}
+
 int fr_insert_particles(fr_recon *r, const float *imgs, int n, int box, const fr_particle *meta,
                         int schedule) {
   TRY(check_state(r));
@@ -949,7 +1017,8 @@ int fr_finish(fr_recon *r, int doift, float *out, float *normout) {
   const int N = r->N;
   cudaStream_t st = r->stream;
   TRY(check_device_error(r));
-  CU(launch_normalize(r->vol_data.as<float>(), r->vol_norm.as<float>(), N, r->p.sqrtnorm, st));
+  CU(launch_normalize(r->vol_data.as<float>(), r->vol_norm.as<float>(), N, r->p.sqrtnorm, st,
+                      r->wfilt));
   if (normout) TRY(from_device(normout, r->vol_norm.p, norm_floats(N) * sizeof(float), st));
   if (doift) {
     cufftHandle plan;
@@ -986,7 +1055,8 @@ int fr_finish_corrected(fr_recon *r, float gauss_width, int outx, int outy, int 
   TRY(stream_enter(r, r->stream));
   cudaStream_t st = r->stream;
   TRY(check_device_error(r));
-  CU(launch_normalize(r->vol_data.as<float>(), r->vol_norm.as<float>(), N, r->p.sqrtnorm, st));
+  CU(launch_normalize(r->vol_data.as<float>(), r->vol_norm.as<float>(), N, r->p.sqrtnorm, st,
+                      r->wfilt));
   if (normout) TRY(from_device(normout, r->vol_norm.p, norm_floats(N) * sizeof(float), st));
   cufftHandle plan;
   TRY(r->plans.get3d(N, st, &plan));

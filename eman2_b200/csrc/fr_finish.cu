@@ -47,26 +47,33 @@ __global__ void k_norm_pairs(float *__restrict__ norm, int N) {
 }
 
 // Stage 2: data /= norm (or sqrt(norm)); zero where the weight is 0.
+// wfilt: 1 for the Wiener reconstructor (normalize_threed(sqrtnorm, true),
+// libEM/reconstructor.cpp:376-390): data / (d + 1), still 0 where d == 0.
 __global__ void k_divide(float2 *__restrict__ data, const float *__restrict__ norm, long n,
-                         int sqrtnorm) {
+                         int sqrtnorm, float wfilt) {
   const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   float d = norm[i];
   if (sqrtnorm) d = __fsqrt_rn(d);
   float2 v = data[i];
   if (d == 0.0f) { v.x = 0.f; v.y = 0.f; }
-  else { v.x = __fdiv_rn(v.x, d); v.y = __fdiv_rn(v.y, d); }
+  else {
+    const float dd = __fadd_rn(d, wfilt);
+    v.x = __fdiv_rn(v.x, dd);
+    v.y = __fdiv_rn(v.y, dd);
+  }
   data[i] = v;
 }
 
-cudaError_t launch_normalize(float *d_data, float *d_norm, int N, int sqrtnorm, cudaStream_t st) {
+cudaError_t launch_normalize(float *d_data, float *d_norm, int N, int sqrtnorm, cudaStream_t st,
+                             float wfilt) {
   const int np = N * (N / 2 + 1) + 5;
   note_launch();
   k_norm_pairs<<<(np + 255) / 256, 256, 0, st>>>(d_norm, N);
   const long n = (long)N * N * (N / 2 + 1);
   note_launch();
   k_divide<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(reinterpret_cast<float2 *>(d_data), d_norm,
-                                                         n, sqrtnorm);
+                                                         n, sqrtnorm, wfilt);
   return cudaGetLastError();
 }
 

@@ -148,6 +148,8 @@ struct fr_recon {
   int state = 0;              // 0 created, 1 accumulating, 2 finished
   cudaStream_t own = nullptr, stream = nullptr;
   fr::Geom *geom = nullptr;
+  fr::Geom *wgeom = nullptr;  // the Wiener reconstructor's pixel disk (looked up on first use)
+  float wfilt = 0.0f;         // 1: Wiener normalisation, data / (weight + 1)
   fr::DevBuf vol_data, vol_norm, d_sym;
   // scratch
   fr::DevBuf s_in, s_slices, s_rot, s_w, s_t3d, s_img, s_img2, s_spec, s_ctf, s_mean, s_txy, s_out,

@@ -104,6 +104,32 @@ __device__ __forceinline__ void insert_pixel_atomic(float *__restrict__ data, fl
 // Per-pixel weight: the particle weight, or with usessnr the slice's
 // class_ssnr table at the pixel radius, max(0, ssnr[int(r*sscale)])
 // (libEM/reconstructor.cpp:1170-1184).
+// WienerFourierReconstructor::do_insert_slice_work (libEM/reconstructor.cpp:1679-1731):
+// the weight at the pixel's radius, rn = |(x,y)|/N scaled by 2*len, linearly
+// interpolated in the slice's ctf_snr_total (or its last entry, times the
+// sign of the insert weight, past the end); the value is scaled by
+// (weight+1)/weight when the slice was Wiener filtered.  Returns
+// weight*sign, the weight insert_pixel gets.
+__device__ __forceinline__ float wiener_weight(const InsertJob &J, int p, int x, int y, float w,
+                                               float &vscale) {
+  const float sub = w < 0.0f ? -1.0f : 1.0f;
+  const float rx = __fdiv_rn((float)x, (float)J.N);
+  const float ry = __fdiv_rn((float)y, (float)J.N);
+  float rn = (float)hypot((double)rx, (double)ry);
+  rn = __fmul_rn(rn, __fmul_rn((float)J.nwsnr, 2.0f));
+  const int rni = (int)floorf(rn);
+  const float *snr = J.wsnr + (size_t)p * J.nwsnr;
+  float weight;
+  if ((unsigned)rni >= (unsigned)(J.nwsnr - 1)) {
+    weight = __fmul_rn(snr[J.nwsnr - 1], sub);
+  } else {
+    const float t = __fsub_rn(rn, (float)rni);   // Util::linear_interpolate (libEM/util.h:518-521)
+    weight = __fadd_rn(__fmul_rn(__fsub_rn(1.0f, t), snr[rni]), __fmul_rn(t, snr[rni + 1]));
+  }
+  vscale = (J.wundo && J.wundo[p]) ? __fdiv_rn(__fadd_rn(weight, 1.0f), weight) : 1.0f;
+  return __fmul_rn(weight, sub);
+}
+
 __device__ __forceinline__ float pixel_weight(const InsertJob &J, int p, int x, int y, float w) {
   if (!J.ssnr) return w;
   const int r = (int)__fadd_rn((float)sqrt((double)(x * x + y * y)), 0.5f);
@@ -130,9 +156,16 @@ __global__ void __launch_bounds__(256) k_scatter(InsertJob J, const float *__res
   for (int i = 0; i < 6; i++) M[i] = __ldg(&J.t3d[9 * s + i]);
   float xx, yy, zz;
   pixel_coords(__ldg(&J.rtab[x + n2]), __ldg(&J.rtab[y + n2]), M, (float)N, xx, yy, zz);
-  const float2 v = slice_value(J.slices + (size_t)p * N * w2, N, x, y);
-  insert_pixel_atomic<MODE>(J.data, J.norm, N, xx, yy, zz, v.x, v.y, pixel_weight(J, p, x, y, w),
-                            h, table, false);
+  float2 v = slice_value(J.slices + (size_t)p * N * w2, N, x, y);
+  float pw;
+  if (J.wsnr) {
+    float vs;
+    pw = wiener_weight(J, p, x, y, w, vs);
+    if (vs != 1.0f) { v.x = __fmul_rn(v.x, vs); v.y = __fmul_rn(v.y, vs); }
+  } else {
+    pw = pixel_weight(J, p, x, y, w);
+  }
+  insert_pixel_atomic<MODE>(J.data, J.norm, N, xx, yy, zz, v.x, v.y, pw, h, table, false);
 }
 
 // Face taps of rim pixels: grid.x covers the rim list, grid.y = slice.

@@ -466,10 +466,63 @@ class FourierReconstructor:
                              "finish() was called; call setup() again")
 
 
+class WienerFourierReconstructor(FourierReconstructor):
+    """WienerFourierReconstructor ("wiener_fourier", libEM/reconstructor.cpp:1643-1731,
+    1921-1947): each slice's pixels are weighted by its ctf_snr_total curve at
+    the pixel's radius (inside the rn < 0.5 disk) and finish divides by the
+    summed weight plus one (a Wiener filter)."""
+
+    NAME = "wiener_fourier"
+
+    def _ensure_handle(self):
+        super()._ensure_handle()
+        _lib.check(_lib.load().fr_set_wiener(self._h, 1))
+
+    def insert_slice(self, img, xform, weight: float = 1.0) -> int:
+        """WienerFourierReconstructor::insert_slice: requires the slice's
+        ctf_snr_total; ctf_wiener_filtered undoes a Wiener filter; a negative
+        weight subtracts.  Returns 0."""
+        if img is None:
+            raise NullPointerException("EMData pointer (input image) is NULL")
+        if self._state != 1:
+            self._require_setup()
+        if not (isinstance(img, EMData) and img.has_attr("ctf_snr_total")):
+            raise NotExistingObjectException(
+                "ctf_snr_total: No SNR information present in class-average. Must use the "
+                "ctf.auto or ctfw.auto averager.")
+        snr = np.ascontiguousarray(img.get_attr("ctf_snr_total"), np.float32)
+        undo = np.array([int(img.get_attr_default("ctf_wiener_filtered", 0))], np.int32)
+        sl = self._slice_of(img, xform)
+        rot = _rot_of(xform)
+        w = np.array([weight], np.float32)
+        status = (ctypes.c_int * 1)()
+        _lib.check(_lib.load().fr_insert_slices_wiener(
+            self._h, _lib.ptr(sl), 1, _lib.ptr(rot), _lib.ptr(w), _lib.ptr(snr), int(snr.size),
+            _lib.ptr(undo), status))
+        return 0
+
+    def insert_slices_wiener(self, slices, rots, weights, snr, undo=None):
+        """n preprocessed slices with their SNR curves snr (n, nsnr)."""
+        if self._state != 1:
+            self._require_setup()
+        s = _host_or_device(slices)
+        n = int(s.shape[0])
+        r, w = _host_or_device(rots), _host_or_device(weights)
+        c = np.ascontiguousarray(snr, np.float32).reshape(n, -1)
+        u = np.zeros(n, np.int32) if undo is None else np.ascontiguousarray(undo, np.int32)
+        _lib.check(_lib.load().fr_insert_slices_wiener(
+            self._h, _lib.ptr(s), n, _lib.ptr(r), _lib.ptr(w), _lib.ptr(c), int(c.shape[1]),
+            _lib.ptr(u), None))
+
+    def determine_slice_agreement(self, img, xform, weight: float = 1.0, sub: bool = True) -> int:
+        raise UnsupportedParameterException(
+            "determine_slice_agreement of wiener_fourier is not built")
+
+
 class Reconstructors:
     """Factory<Reconstructor> (libpyEM/libpyReconstructor2.cpp:221-226)."""
 
-    _known = {"fourier": FourierReconstructor}
+    _known = {"fourier": FourierReconstructor, "wiener_fourier": WienerFourierReconstructor}
 
     @staticmethod
     def get(name: str, params: dict | None = None):

@@ -226,6 +226,20 @@ FR_API int fr_insert_slices_noalloc(const float *d_slices, int n, int N, int mod
                                     const float *d_weights, float *d_data, float *d_norm,
                                     void *stream);
 
+/* WienerFourierReconstructor ("wiener_fourier", libEM/reconstructor.cpp:1643-1731,
+ * 1921-1947).  fr_set_wiener(r, 1) makes finish divide by (weight + 1)
+ * (normalize_threed(sqrtnorm, true), libEM/reconstructor.cpp:376-390).
+ * fr_insert_slices_wiener inserts n preprocessed slices whose per-pixel
+ * weight is their ctf_snr_total curve (snr[n][nsnr]) interpolated at the
+ * pixel radius, inside the rn < 0.5 disk; weights[i] < 0 subtracts;
+ * undo[i] != 0 (ctf_wiener_filtered) scales the values by (w+1)/w.
+ * Without a curve: FR_ENOTEXIST, as the reference's
+ * NotExistingObjectException. */
+FR_API int fr_set_wiener(fr_recon *r, int on);
+FR_API int fr_insert_slices_wiener(fr_recon *r, const float *slices, int n, const float *rot,
+                                   const float *weights, const float *snr, int nsnr,
+                                   const int *undo, int *status_out);
+
 /* Last error message of the calling thread. */
 FR_API const char *fr_last_error(void);
 

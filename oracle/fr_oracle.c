@@ -347,6 +347,66 @@ OR_EXPORT int or_insert_slice(acc_t *vol_data, acc_t *vol_norm, int N, int mode,
   return 0;
 }
 
+/* WienerFourierReconstructor::do_insert_slice_work (libEM/reconstructor.cpp:1679-1731)
+ * for one slice: pixels with rn = |(x/(inx-2), y/iny)| < .5, weight = the
+ * slice's ctf_snr_total (snr[nsnr]) linearly interpolated at rn*2*nsnr (its
+ * last entry times the insert weight's sign past the end), the value scaled
+ * by (w+1)/w for a Wiener-filtered slice, inserted with weight*sign. */
+OR_EXPORT int or_insert_slice_wiener(acc_t *vol_data, acc_t *vol_norm, int N, int mode,
+                                     const float *slice, const float *t3d, int nsym,
+                                     float inweight, const float *snr, int nsnr, int undo) {
+  or_init_tables();
+  or_vol v;
+  v.data = vol_data; v.norm = vol_norm;
+  v.nx = N + 2; v.ny = N; v.nz = N;
+  v.nxyz = (long)v.nx * v.ny * v.nz;
+  const float inx = (float)(N + 2), iny = (float)N;
+  const int nx = N + 2, ny = N, nz = N;
+  if (!snr || nsnr < 1) return -1;
+  const float sub = inweight < 0 ? -1.0f : 1.0f;
+  for (int s = 0; s < nsym; s++) {
+    const float *M = t3d + 9 * s;
+    for (int y = (int)(-iny / 2); y < iny / 2; y++) {
+      for (int x = 0; x <= inx / 2; x++) {
+        const float rx = (float)x / (inx - 2.0f);
+        const float ry = (float)y / iny;
+        float rn = (float)hypot(rx, ry);
+        if (rn >= .5) continue;
+        rn *= nsnr * 2.0f;
+        const int rni = (int)floor(rn);
+        float weight;
+        if ((unsigned int)rni >= (unsigned int)(nsnr - 1)) weight = snr[nsnr - 1] * sub;
+        else {
+          rn -= rni;
+          weight = (1 - rn) * snr[rni] + rn * snr[rni + 1];
+        }
+        real xx = (real)rx * (real)M[0] + (real)ry * (real)M[3];
+        real yy = (real)rx * (real)M[1] + (real)ry * (real)M[4];
+        real zz = (real)rx * (real)M[2] + (real)ry * (real)M[5];
+        xx = xx * (real)(nx - 2);
+        yy = yy * (real)ny;
+        zz = zz * (real)nz;
+        real dre, dim;
+        or_slice_at(slice, nx, ny, x, y, &dre, &dim);
+        if (undo) {
+          const float f = (weight + 1.0f) / weight;
+          dre = (real)((float)dre * f);
+          dim = (real)((float)dim * f);
+        }
+        const real w = (real)(weight * sub);
+        switch (mode) {
+          case MODE_NEAREST: or_insert_nearest(&v, xx, yy, zz, dre, dim, w); break;
+          case MODE_GAUSS2: or_insert_gauss2(&v, xx, yy, zz, dre, dim, w); break;
+          case MODE_GAUSS5: or_insert_gauss5(&v, xx, yy, zz, dre, dim, w); break;
+          case MODE_TRILINEAR: or_insert_trilinear(&v, xx, yy, zz, dre, dim, w); break;
+          default: return -2;
+        }
+      }
+    }
+  }
+  return 0;
+}
+
 /* Convenience for tests: insert n slices with per-slice orientation blocks
  * arg[n*9] composed with the symmetry operators sym[nsym*9]. */
 OR_EXPORT int or_insert_batch(acc_t *vol_data, acc_t *vol_norm, int N, int mode,
@@ -366,8 +426,8 @@ OR_EXPORT int or_insert_batch(acc_t *vol_data, acc_t *vol_norm, int N, int mode,
 }
 
 /* ReconstructorVolumeData::normalize_threed (libEM/reconstructor.cpp:315-390),
- * full-volume case, wiener off. */
-OR_EXPORT void or_normalize(acc_t *rdata, acc_t *norm, int N, int sqrtnorm) {
+ * full-volume case; wiener adds 1 to each nonzero denominator (:376-390). */
+OR_EXPORT void or_normalize_w(acc_t *rdata, acc_t *norm, int N, int sqrtnorm, int wiener) {
   const int nx = N + 2, ny = N, nz = N;
   const long nnx = nx / 2, nnxy = (long)ny * nnx;
   for (int z = -nz / 2; z < nz / 2; z++) {
@@ -394,8 +454,16 @@ OR_EXPORT void or_normalize(acc_t *rdata, acc_t *norm, int N, int sqrtnorm) {
     acc_t d = norm[i / 2];
     if (sqrtnorm) d = (sizeof(acc_t) == sizeof(float)) ? (acc_t)sqrtf((float)d) : (acc_t)sqrt((double)d);
     if (d == 0) { rdata[i] = 0; rdata[i + 1] = 0; }
-    else { rdata[i] /= d; rdata[i + 1] /= d; }
+    else {
+      const acc_t dd = d + (acc_t)(wiener ? 1.0f : 0.0f);
+      rdata[i] /= dd;
+      rdata[i + 1] /= dd;
+    }
   }
+}
+
+OR_EXPORT void or_normalize(acc_t *rdata, acc_t *norm, int N, int sqrtnorm) {
+  or_normalize_w(rdata, norm, N, sqrtnorm, 0);
 }
 
 /* FourierReconstructor::pixel_at (libEM/reconstructor.cpp:1448-1462) with

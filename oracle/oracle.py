@@ -64,6 +64,9 @@ def _lib(kind: str = "fp32"):
                                     ctypes.c_int, _F, ctypes.c_int]
     lib.or_insert_pixels.argtypes = [ctypes.c_int, R, R, ctypes.c_int, _F, ctypes.c_long]
     lib.or_normalize.argtypes = [R, R, ctypes.c_int, ctypes.c_int]
+    lib.or_normalize_w.argtypes = [R, R, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    lib.or_insert_slice_wiener.argtypes = [R, R, ctypes.c_int, ctypes.c_int, _F, _F, ctypes.c_int,
+                                           ctypes.c_float, _F, ctypes.c_int, ctypes.c_int]
     lib.or_compare_slice.argtypes = [R, R, ctypes.c_int, _F, _F, ctypes.c_int, ctypes.c_float,
                                      ctypes.c_float, _F]
     lib.or_sym_ops.argtypes = [ctypes.c_char, ctypes.c_int, _F, ctypes.c_int]
@@ -161,6 +164,25 @@ class OracleVolume:
         if rc:
             raise RuntimeError(f"oracle insert failed rc={rc}")
 
+    def insert_wiener(self, slices, rots, weights, snr, undo=None, mode="gauss_2", sym="c1"):
+        """WienerFourierReconstructor insert_slice for n slices with their
+        ctf_snr_total curves snr (n, nsnr) and Wiener-filtered flags undo (n,)."""
+        slices = np.ascontiguousarray(slices, np.float32).reshape(-1, self.N, self.N + 2)
+        n = slices.shape[0]
+        rots = np.ascontiguousarray(rots, np.float32).reshape(n, 9)
+        snr = np.ascontiguousarray(snr, np.float32).reshape(n, -1)
+        ops = np.ascontiguousarray(sym_ops(sym)).reshape(-1, 9)
+        t3d = np.empty((ops.shape[0], 9), np.float32)
+        for p in range(n):
+            for s in range(ops.shape[0]):
+                t3d[s] = compose(rots[p].reshape(3, 3), ops[s].reshape(3, 3)).reshape(9)
+            rc = self.lib.or_insert_slice_wiener(
+                _rp(self.data), _rp(self.norm), self.N, MODES[mode], _fp(slices[p]), _fp(t3d),
+                ops.shape[0], float(weights[p]), _fp(snr[p]), snr.shape[1],
+                int(bool(undo[p])) if undo is not None else 0)
+            if rc:
+                raise RuntimeError(f"oracle insert failed rc={rc}")
+
     def insert_omp(self, slices, rots, weights, mode="gauss_2", sym="c1", threads=0):
         assert self.kind == "omp"
         slices = np.ascontiguousarray(slices, np.float32).reshape(-1, self.N, self.N + 2)
@@ -197,14 +219,15 @@ class OracleVolume:
         o.data, o.norm = self.data.copy(), self.norm.copy()
         return o
 
-    def normalize(self, sqrtnorm=False):
-        self.lib.or_normalize(_rp(self.data), _rp(self.norm), self.N, int(bool(sqrtnorm)))
+    def normalize(self, sqrtnorm=False, wiener=False):
+        self.lib.or_normalize_w(_rp(self.data), _rp(self.norm), self.N, int(bool(sqrtnorm)),
+                                int(bool(wiener)))
 
-    def finish(self, doift=True, sqrtnorm=False):
+    def finish(self, doift=True, sqrtnorm=False, wiener=False):
         """FourierReconstructor::finish (libEM/reconstructor.cpp:1552-1641):
         normalise; optionally inverse FFT (x 1/N^3), depad, phase-origin to
         centre.  Returns (volume, norm) like finish() + normout."""
-        self.normalize(sqrtnorm)
+        self.normalize(sqrtnorm, wiener)
         if not doift:
             return self.data, self.norm
         N = self.N

@@ -285,6 +285,53 @@ def test_finish_corrected_matches_oracle(gpu, mode, width, outsize):
     assert rel(got, e.numpy()) < RTOL_ACC
 
 
+@pytest.mark.parametrize("mode,sym", [("gauss_2", "c1"), ("nearest_neighbor", "d2"),
+                                      ("gauss_5", "c2"), ("trilinear", "d1")])
+def test_wiener_matches_oracle(gpu, mode, sym):
+    """wiener_fourier: SNR-weighted pixels on the rn < 0.5 disk, some slices
+    Wiener filtered (undone), one subtracted, and the (weight + 1) finish."""
+    from eman2_b200 import EMData, Reconstructors
+    from eman2_b200.exceptions import NotExistingObjectException
+    N, n = 24, 12
+    sl, rt = rand_slices(N, n, 101), rand_rots(n, 102)
+    rng = np.random.default_rng(103)
+    snr = rng.uniform(0.2, 5.0, (n, 13)).astype(np.float32)
+    undo = (np.arange(n) % 3 == 0).astype(np.int32)
+    w = np.ones(n, np.float32)
+    w[5] = -1.0
+    r = Reconstructors.get("wiener_fourier", {"size": [N] * 3, "sym": sym, "mode": mode})
+    r.setup()
+    r.insert_slices_wiener(sl, rt, w, snr, undo)
+    d, nrm = r.get_accumulators()
+    o = oracle.OracleVolume(N, "fp32")
+    o.insert_wiener(sl, rt, w, snr, undo, mode, sym)
+    assert rel(nrm, o.norm) < RTOL_ACC and rel(d, o.data) < RTOL_ACC
+    # finish on a reconstruction without the subtracted slice: with it, some
+    # summed weights approach -1 and weight + 1 amplifies summation-order noise
+    w[5] = 1.0
+    r.setup()
+    r.insert_slices_wiener(sl, rt, w, snr, undo)
+    o = oracle.OracleVolume(N, "fp32")
+    o.insert_wiener(sl, rt, w, snr, undo, mode, sym)
+    out = r.finish(True).numpy()
+    want, _ = o.finish(True, wiener=True)
+    assert rel(out, want) < RTOL_FFT
+    # the single-slice API and the missing-curve error
+    r2 = Reconstructors.get("wiener_fourier", {"size": [N] * 3, "sym": sym, "mode": mode})
+    r2.setup()
+    img = EMData(sl[0], is_complex=True, attrs={"reconstruct_preproc": 1,
+                                                "ctf_snr_total": snr[0].tolist()})
+    from eman2_b200 import Transform
+    assert r2.insert_slice(img, Transform(rt[0].reshape(-1)), 1.0) == 0
+    o2 = oracle.OracleVolume(N, "fp32")
+    o2.insert_wiener(sl[:1], rt[:1], np.ones(1, np.float32), snr[:1], None, mode, sym)
+    d2, n2 = r2.get_accumulators()
+    assert rel(n2, o2.norm) < RTOL_ACC and rel(d2, o2.data) < RTOL_ACC
+    with pytest.raises(NotExistingObjectException):
+        r2.insert_slice(EMData(sl[1], is_complex=True, attrs={"reconstruct_preproc": 1}),
+                        Transform(rt[1].reshape(-1)), 1.0)
+
+
 def test_agreement_matches_oracle(gpu):
     N, n = 32, 30
     sl, rt = rand_slices(N, n, 71), rand_rots(n, 72)

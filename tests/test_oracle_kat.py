@@ -198,6 +198,36 @@ def test_kernel_fix_known_values():
     assert c.shape == (2, 6, 4) and c[0, 0, 0] == 3 * 64 + 1 * 8 + 2
 
 
+def test_wiener_pixel_weight_and_disk():
+    """WienerFourierReconstructor (libEM/reconstructor.cpp:1679-1731): each
+    pixel of an identity-oriented slice adds, at its own voxel (nearest), the
+    SNR curve interpolated at rn = |(x, y)|/N * 2*len as weight; pixels at
+    rn >= .5 add nothing; the Wiener finish divides by weight + 1."""
+    N = 16
+    snr = np.linspace(4.0, 1.0, 8).astype(np.float32)          # 8 entries
+    for (x, y) in [(3, 2), (0, 5), (6, -3), (7, 4)]:
+        sl = np.zeros((N, N + 2), np.float32)
+        sl[y % N, 2 * x] = 1.0
+        v = oracle.OracleVolume(N, "fp32")
+        v.insert_wiener(sl[None], np.eye(3, dtype=np.float32)[None], np.ones(1, np.float32),
+                        snr[None], mode="nearest_neighbor")
+        rx, ry = np.float32(x) / np.float32(N), np.float32(y) / np.float32(N)
+        rn = np.float32(math.hypot(rx, ry))
+        if rn >= 0.5:                      # every disk pixel adds its weight; this one is outside
+            assert v.norm[0, y % N, x] == 0.0
+            continue
+        rn = np.float32(rn * np.float32(16.0))
+        k = int(math.floor(rn))
+        t = np.float32(rn - np.float32(k))
+        want = np.float32((np.float32(1) - t) * snr[k] + t * snr[k + 1])
+        got = v.norm[0, y % N, x]          # volumes are [z][y][x]; identity: voxel (x, y, 0)
+        assert got == want
+        d = v.data[0, y % N, 2 * x]
+        v.normalize(wiener=True)
+        if x:
+            assert v.data[0, y % N, 2 * x] == np.float32(d / (want + np.float32(1)))
+
+
 @pytest.mark.parametrize("N", [16, 20])
 def test_normalize_weights_conjugate_pairs(N):
     """normalize_threed sums conjugate-pair weights on the x=0 and x=N/2
