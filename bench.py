@@ -612,7 +612,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-serve", action="store_true", help="skip the batched and serving legs")
     ap.add_argument("--tile", type=int, default=-1,
-                    help="pin the insertion kernel (0-3 register tiles, 4 staged column, "
+                    help="pin the insertion kernel (0-3 register tiles, 4 staged column, 6 pixel-major, "
                          "5 barrier-free column, -2 scatter); default: library choice")
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]

@@ -36,7 +36,7 @@ def insert_particles_multi(recons, images, metas, stream=None):
 
 
 TILE_NAMES = {0: "gather 8x8x8", 1: "gather 16x8x8", 2: "gather 8x8x4", 3: "gather 16x16x4",
-              4: "column (staged)", 5: "column (barrier-free)", -2: "scatter"}
+              4: "column (staged)", 5: "column (barrier-free)", 6: "pixel-major", -2: "scatter"}
 
 
 def autotune(N: int, mode: str, nsym: int, nparticles: int = 256):
@@ -45,10 +45,10 @@ def autotune(N: int, mode: str, nsym: int, nparticles: int = 256):
     from then on.  Returns (tile id, {schedule name: ms})."""
     lib = _lib.load()
     tile = ctypes.c_int()
-    ms = (ctypes.c_float * 7)()
+    ms = (ctypes.c_float * 8)()
     _lib.check(lib.fr_autotune(int(N), _lib.MODE_IDS[mode], int(nsym), int(nparticles),
                                ctypes.byref(tile), ms))
-    names = [TILE_NAMES[i] for i in range(6)] + [TILE_NAMES[-2]]
+    names = [TILE_NAMES[i] for i in range(7)] + [TILE_NAMES[-2]]
     return tile.value, dict(zip(names, list(ms)))
 
 

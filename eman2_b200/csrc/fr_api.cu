@@ -394,8 +394,9 @@ int insert_device(fr_recon *r, const float2 *d_slices, const float *d_t3d, const
     return FR_OK;
   }
   int tile = r->tile >= 0 ? r->tile : (tuned >= 0 ? tuned : default_tile(r->mode, r->N, r->nsym, np));
+  tile = effective_tile(tile, r->mode);
   if (r->tiles_tile != tile) {
-    if (tile == kColumnTile || tile == kColumn3Tile)
+    if (is_column_tile(tile))
       column_tiles(r->N, r->mode, r->p.corners, r->tiles, r->tx, r->ty, r->tz, &r->tile_dist);
     else gather_tiles(r->N, r->mode, tile, r->p.corners, r->tiles, r->tx, r->ty, r->tz);
     r->tiles_tile = tile;
@@ -406,7 +407,7 @@ int insert_device(fr_recon *r, const float2 *d_slices, const float *d_t3d, const
   j.tiles_z = r->tz;
   const int nsl = np * r->nsym;
   int nwork = 0;
-  const bool column = tile == kColumnTile || tile == kColumn3Tile;
+  const bool column = is_column_tile(tile);
   if (column) {
     // work items (job 0, tile, first slice of the block)
     if (r->work_np != nsl) {
@@ -443,7 +444,10 @@ int insert_device(fr_recon *r, const float2 *d_slices, const float *d_t3d, const
   TRY(r->s_counter.ensure(sizeof(int)));
   CU(cudaMemcpyAsync(r->s_jobs.p, &j, sizeof(InsertJob), cudaMemcpyHostToDevice, st));
   if (prof) CU(cudaEventRecord(ev[0], st));
-  if (tile == kColumn3Tile)
+  if (tile == kPixelTile)
+    CU(launch_pixel(r->s_jobs.as<InsertJob>(), r->s_work.as<int4>(), nwork, kColumnBlock,
+                    r->s_counter.as<int>(), r->N, st));
+  else if (tile == kColumn3Tile)
     CU(launch_column3(r->s_jobs.as<InsertJob>(), r->s_work.as<int4>(), nwork, kColumnBlock,
                       r->s_counter.as<int>(), r->N, st));
   else if (tile == kColumnTile)

@@ -37,7 +37,9 @@ int tuned_tile(int N, int mode, int nsym) {
 
 int default_tile(int mode, int N, int nsym, int np) {
   (void)nsym; (void)np; (void)N; (void)mode;
-  return kColumn3Tile;   // the barrier-free column kernel unless the autotuner measured otherwise
+  // unless the autotuner measured otherwise: the pixel-major kernel for the
+  // narrow windows, the barrier-free column kernel for gauss_5
+  return mode == FR_MODE_GAUSS5 ? kColumn3Tile : kPixelTile;
 }
 
 }  // namespace fr
@@ -139,15 +141,15 @@ struct RoundPlan {
   std::vector<unsigned char> work;   // every group's items, 16-byte aligned
 };
 
-static bool is_column(int tile) { return tile == kColumnTile || tile == kColumn3Tile; }
+static bool is_column(int tile) { return is_column_tile(tile); }
 
 // Each job's schedule: the caller's pin, else the autotuner's measurement for
 // its (N, mode, nsym), else the barrier-free column kernel.  Jobs that share
 // a schedule share one persistent launch per round.
 static int job_tile(const fr_recon *r, int tile_pref) {
-  if (tile_pref != -1) return tile_pref;
+  if (tile_pref != -1) return effective_tile(tile_pref, r->mode);
   const int t = tuned_tile(r->N, r->mode, r->nsym);
-  return t != -1 ? t : default_tile(r->mode, r->N, r->nsym, 0);
+  return effective_tile(t != -1 ? t : default_tile(r->mode, r->N, r->nsym, 0), r->mode);
 }
 
 // Adds job r's InsertJob (its chunk's slices, rotations and weights in its
@@ -253,7 +255,10 @@ static int plan_launch(const RoundPlan &P, BatchScratch &bs, cudaStream_t st) {
       continue;
     }
     const void *w = (const unsigned char *)bs.d_work.p + g.off;
-    if (g.tile == kColumn3Tile)
+    if (g.tile == kPixelTile)
+      CU(launch_pixel(d_jobs, (const int4 *)w, (int)g.nwork, kColumnBlock, bs.d_counter.as<int>(),
+                      g.maxN, st));
+    else if (g.tile == kColumn3Tile)
       CU(launch_column3(d_jobs, (const int4 *)w, (int)g.nwork, kColumnBlock, bs.d_counter.as<int>(),
                         g.maxN, st));
     else if (g.tile == kColumnTile)
@@ -634,7 +639,7 @@ int fr_batch_get_accumulators(fr_batch *b, int job, float *data, float *norm) {
 }
 
 int fr_set_tile(int N, int mode, int nsym, int tile) {
-  if (tile != kTunedScatter && (tile < -1 || tile > kColumn3Tile))
+  if (tile != kTunedScatter && (tile < -1 || tile > kPixelTile))
     return fail(FR_EINVAL_PARAM, "tile %d out of range", tile);
   std::lock_guard<std::mutex> lk(g_tune_mu);
   if (tile == -1) g_tuned.erase(std::make_tuple(N, mode, nsym));
@@ -645,8 +650,9 @@ int fr_set_tile(int N, int mode, int nsym, int tile) {
 // Measures the gather schedule with every tile shape, and the scatter
 // schedule, on random slices of size N through random orientations; records
 // the fastest for (N, mode, nsym).  tile_out: chosen tile (-2 = scatter);
-// ms_out[kColumn3Tile+2]: per-candidate milliseconds (register tiles 0-3,
-// staged column 4, barrier-free column 5, then scatter).
+// ms_out[kPixelTile+2]: per-candidate milliseconds (register tiles 0-3,
+// staged column 4, barrier-free column 5, pixel-major 6 (gauss_5: -1), then
+// scatter).
 int fr_autotune(int N, int mode, int nsym, int nparticles, int *tile_out, float *ms_out) {
   if (nparticles <= 0) return fail(FR_EINVAL_PARAM, "nparticles must be positive");
   fr_params p;
@@ -695,8 +701,12 @@ int fr_autotune(int N, int mode, int nsym, int nparticles, int *tile_out, float 
        cudaMemcpy(dw.p, w.data(), sizeof(float) * w.size(), cudaMemcpyHostToDevice) != cudaSuccess))
     rc = fail(FR_ECUDA, "autotune: staging failed");
   int measured = 0;
-  for (int cand = 0; cand <= kColumn3Tile + 1 && rc == FR_OK; cand++) {
-    const bool scatter = cand == kColumn3Tile + 1;
+  for (int cand = 0; cand <= kPixelTile + 1 && rc == FR_OK; cand++) {
+    const bool scatter = cand == kPixelTile + 1;
+    if (!scatter && effective_tile(cand, mode) != cand) {   // no pixel-major gauss_5
+      if (ms_out) ms_out[cand] = -1.0f;
+      continue;
+    }
     r->tile = scatter ? -1 : cand;
     const int sched = scatter ? FR_SCHED_SCATTER : FR_SCHED_GATHER;
     // one warm-up call, then one timed call; a schedule that cannot run this

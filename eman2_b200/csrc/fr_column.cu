@@ -662,6 +662,274 @@ __device__ void tile_item3(const InsertJob &J, int tile, int s0, int s1, const S
   __syncthreads();
 }
 
+
+// ------------------------------------------------------------------ v4
+// Pixel-major variant for the windows one or two taps wide (nearest,
+// gauss_2, trilinear), where walking columns spends most of its
+// instructions finding candidate pixels for two taps.  Each warp takes
+// whole hit slices and, for each, bounds the slice's pixels whose window can
+// meet the tile (or its mirror): rows from the projection of the tile box on
+// the slice's y axis, x ranges per row, a warp prefix sum.  Its lanes then run
+// over those pixels with the reference's exact coordinate and tap arithmetic
+// and add every tap that lands in the tile to the shared-memory
+// accumulators with shared atomics.  No block barriers between slices.
+constexpr int PROWS = 32;   // rows per row batch of a pass
+
+struct Smem4 {
+  float *are, *aim, *awt, *aflag;   // accumulators, one array per component [NV]
+  float4 *steps;
+  float *rtab;
+  int *xmax;
+  int *hits;
+  int *tmp;
+  int *rowc0;                  // [NT/32][PROWS]
+  int *rowoff;                 // [NT/32][PROWS + 1]
+  int *wcount;
+  int *next;                   // next (slice, pass) unit of the work item
+  unsigned long long *state;   // [0] step table loaded (mode), [1] xmax table loaded (address)
+};
+
+// Slot of local cell (lx, ly, lz) in the component arrays: the bank is set by
+// lx and bit 0 of ly, so lx is XORed with the other coordinates' low bits to
+// spread a warp's atomics whichever direction its pixels step the cells in.
+__device__ __forceinline__ int cell_slot(int lx, int ly, int lz) {
+  return (lz * T + ly) * T + (lx ^ (((ly >> 1) + lz) & (T - 1)));
+}
+
+// Adds one tap's contribution to cell (i,j,k) of the window under the
+// placement rules of add_complex_at_fast (libEM/emdata_core.h:368-410):
+// pass sg = +1 takes the direct cells (i >= 0), pass sg = -1 the conjugate
+// cells (-i,-j,-k) of taps with i <= 0; the x = 0 plane's conjugate copy
+// carries no weight and the origin keeps only its real part.
+__device__ __forceinline__ void tile_tap(const Smem4 &S, int sg, int i, int j, int k,
+                                         const int *base, const int *ext, float vre, float vim,
+                                         float vw) {
+  int ti = i, tj = j, tk = k;
+  if (sg < 0) { ti = -i; tj = -j; tk = -k; }
+  if (ti < base[0] || ti > ext[0] || tj < base[1] || tj > ext[1] || tk < base[2] || tk > ext[2])
+    return;
+  const bool origin = (i == 0 && j == 0 && k == 0);
+  const int c = cell_slot(ti - base[0], tj - base[1], tk - base[2]);
+  if (sg > 0) {
+    atomicAdd(&S.are[c], vre);
+    if (origin) S.aflag[c] = 1.0f;
+    else atomicAdd(&S.aim[c], vim);
+    atomicAdd(&S.awt[c], vw);
+  } else {
+    if (origin) return;
+    atomicAdd(&S.are[c], vre);
+    atomicAdd(&S.aim[c], -vim);
+    if (i != 0) atomicAdd(&S.awt[c], vw);
+  }
+}
+
+template <int MODE>
+__device__ __forceinline__ void pixel_pass(const InsertJob &J, const Smem4 &S, const float *M,
+                                           int sg, const int *base, const int *ext,
+                                           const float2 *__restrict__ sl, float w, float h,
+                                           const ExpSteps &steps) {
+  constexpr float RLO = Win<MODE>::lo, RHI = Win<MODE>::hi;
+  const int N = J.N, n2 = N >> 1;
+  const float Nf = (float)N;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int *c0s = S.rowc0 + warp * PROWS;
+  int *offs = S.rowoff + warp * (PROWS + 1);
+  float lo[3], hi[3];
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    lo[a] = (sg > 0 ? base[a] : -ext[a]) - RLO - kDel;
+    hi[a] = (sg > 0 ? ext[a] : -base[a]) + RHI + kDel;
+  }
+  // mapped point of pixel (x, y) ~ x*u + y*v with u, v the first two rows of
+  // M (orthonormal), so y ~ p.v: rows from the box's extent along v
+  const float *u = M, *v = M + 3;
+  float ymn, ymx;
+  box_dot(v, lo, hi, ymn, ymx);
+  const int r0 = max(-n2, (int)ceilf(ymn - 0.05f)), r1 = min(n2 - 1, (int)floorf(ymx + 0.05f));
+  for (int rb = r0; rb <= r1; rb += PROWS) {
+    // ---- this row batch's x ranges and prefix offsets
+    const int y = rb + lane;
+    int c0 = 0, cnt = 0;
+    if (y <= r1) {
+      float xlo = 0.0f, xhi = (float)S.xmax[y + n2];
+#pragma unroll
+      for (int a = 0; a < 3; a++) {
+        if (fabsf(u[a]) > 0.05f) {
+          const float c = v[a] * (float)y;
+          const float L = (lo[a] - c) / u[a], U = (hi[a] - c) / u[a];
+          xlo = fmaxf(xlo, fminf(L, U) - 0.05f);
+          xhi = fminf(xhi, fmaxf(L, U) + 0.05f);
+        }
+      }
+      c0 = max(0, (int)ceilf(xlo));
+      const int c1 = min(S.xmax[y + n2], (int)floorf(xhi));
+      cnt = max(0, c1 - c0 + 1);
+    }
+    int incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += t;
+    }
+    const int total = __shfl_sync(0xffffffffu, incl, 31);
+    c0s[lane] = c0;
+    offs[lane] = incl - cnt;
+    if (lane == 31) offs[PROWS] = total;
+    __syncwarp();
+    // ---- the pixels of the batch, one per lane
+    for (int idx = lane; idx < total; idx += 32) {
+      int row = 0;
+#pragma unroll
+      for (int step = 16; step > 0; step >>= 1)
+        if (offs[row + step] <= idx) row += step;
+      const int x = c0s[row] + (idx - offs[row]);
+      const int py = rb + row;
+      float xx, yy, zz;
+      pixel_coords(S.rtab[x + n2], S.rtab[py + n2], M, Nf, xx, yy, zz);
+      const float2 val = slice_value(sl, N, x, py);
+      if (MODE == MODE_NEAREST) {
+        // FourierInserter3DMode1 (libEM/reconstructor_tools.cpp:113-126)
+        const int i = (int)floorf(__fadd_rn(xx, 0.5f)), j = (int)floorf(__fadd_rn(yy, 0.5f)),
+                  k = (int)floorf(__fadd_rn(zz, 0.5f));
+        tile_tap(S, sg, i, j, k, base, ext, __fmul_rn(val.x, w), __fmul_rn(val.y, w), w);
+      } else {
+        const int x0 = (int)floorf(xx), y0 = (int)floorf(yy), z0 = (int)floorf(zz);
+        float dxx[2], dyy[2], dzz[2];
+#pragma unroll
+        for (int q = 0; q < 2; q++) {
+          const float dx = __fsub_rn((float)(x0 + q), xx), dy = __fsub_rn((float)(y0 + q), yy),
+                      dz = __fsub_rn((float)(z0 + q), zz);
+          dxx[q] = __fmul_rn(dx, dx);
+          dyy[q] = __fmul_rn(dy, dy);
+          dzz[q] = __fmul_rn(dz, dz);
+        }
+#pragma unroll
+        for (int c = 0; c < 2; c++)
+#pragma unroll
+          for (int b = 0; b < 2; b++)
+#pragma unroll
+            for (int a = 0; a < 2; a++) {
+              float vre, vim, vw;
+              if (MODE == MODE_GAUSS2) {
+                const float r = __fadd_rn(__fadd_rn(dxx[a], dyy[b]), dzz[c]);
+                const float gg = __fmul_rn(step_exp(r, h, steps, S.steps), w);
+                vre = __fmul_rn(val.x, gg);
+                vim = __fmul_rn(val.y, gg);
+                vw = gg;
+              } else {
+                tap_value<MODE>(x0 + a, y0 + b, z0 + c, xx, yy, zz, val.x, val.y, w, h, nullptr,
+                                vre, vim, vw);
+              }
+              tile_tap(S, sg, x0 + a, y0 + b, z0 + c, base, ext, vre, vim, vw);
+            }
+      }
+    }
+    __syncwarp();
+  }
+}
+
+template <int MODE>
+__device__ void tile_item4(const InsertJob &J, int tile, int s0, int s1, const Smem4 &S, float h,
+                           const ExpSteps &steps, int *err) {
+  constexpr float RLO = Win<MODE>::lo, RHI = Win<MODE>::hi;
+  const int N = J.N, n2 = N >> 1;
+  const int tix = tile % J.tiles_x, tiy = (tile / J.tiles_x) % J.tiles_y,
+            tiz = tile / (J.tiles_x * J.tiles_y);
+  const int base[3] = {tix * T, -n2 + 1 + tiy * T, -n2 + 1 + tiz * T};
+  const int ext[3] = {min(base[0] + T - 1, n2 - 1), min(base[1] + T - 1, n2 - 1),
+                      min(base[2] + T - 1, n2 - 1)};
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int NW = NT / 32;
+  // ---- cull: slices whose plane passes the tile (and so its mirror)
+  int nhit = 0;
+  for (int r = s0; r < s1; r += NT) {
+    const int s = r + threadIdx.x;
+    bool hit = false;
+    if (s < s1 && __ldg(&J.pw[s / J.nsym]) != 0.0f) {
+      const float n[3] = {__ldg(&J.t3d[9 * s + 6]), __ldg(&J.t3d[9 * s + 7]), __ldg(&J.t3d[9 * s + 8])};
+      const float lo[3] = {base[0] - RLO - kDel, base[1] - RLO - kDel, base[2] - RLO - kDel};
+      const float hi[3] = {ext[0] + RHI + kDel, ext[1] + RHI + kDel, ext[2] + RHI + kDel};
+      float mn, mx;
+      box_dot(n, lo, hi, mn, mx);
+      hit = mn <= kPlaneTol && mx >= -kPlaneTol;
+    }
+    const unsigned b = __ballot_sync(0xffffffffu, hit);
+    if (lane == 0) S.wcount[warp] = __popc(b);
+    __syncthreads();
+    int off = 0, tot = 0;
+#pragma unroll
+    for (int i = 0; i < NW; i++) {
+      const int c = S.wcount[i];
+      off += (i < warp) ? c : 0;
+      tot += c;
+    }
+    if (hit) S.hits[nhit + off + __popc(b & ((1u << lane) - 1u))] = s;
+    nhit += tot;
+    __syncthreads();
+  }
+  if (nhit == 0) return;
+  // ---- per-job tables and this mode's step table
+  if (S.state[1] != (unsigned long long)J.xmax) {
+    for (int i = threadIdx.x; i < N + 2; i += NT) S.rtab[i] = __ldg(&J.rtab[i]);
+    for (int i = threadIdx.x; i < N; i += NT) S.xmax[i] = __ldg(&J.xmax[i]);
+  }
+  if (MODE == MODE_GAUSS2 && S.state[0] != (unsigned long long)MODE) {
+    const int nb = min(steps.nbins, STEP2CAP);
+    for (int i = threadIdx.x; i < nb; i += NT) S.steps[i] = __ldg(&steps.d_bins[i]);
+    if (threadIdx.x == 0 && steps.nbins > STEP2CAP) atomicOr(err, 8);
+  }
+  for (int i = threadIdx.x; i < NV; i += NT) {
+    S.are[i] = 0.f;
+    S.aim[i] = 0.f;
+    S.awt[i] = 0.f;
+    S.aflag[i] = 0.f;
+  }
+  if (threadIdx.x == 0) *S.next = 0;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (MODE == MODE_GAUSS2) S.state[0] = (unsigned long long)MODE;
+    S.state[1] = (unsigned long long)J.xmax;
+  }
+  // ---- warps take (slice, pass) units as they come free
+  const int w2 = n2 + 1;
+  while (true) {
+    int u = 0;
+    if (lane == 0) u = atomicAdd(S.next, 1);
+    u = __shfl_sync(0xffffffffu, u, 0);
+    if (u >= 2 * nhit) break;
+    const int s = S.hits[u >> 1];
+    const int p = s / J.nsym;
+    float M[9];
+#pragma unroll
+    for (int i = 0; i < 9; i++) M[i] = __ldg(&J.t3d[9 * s + i]);
+    const float w = __ldg(&J.pw[p]);
+    const float2 *sl = J.slices + (size_t)p * N * w2;
+    pixel_pass<MODE>(J, S, M, (u & 1) ? -1 : 1, base, ext, sl, w, h, steps);
+  }
+  __syncthreads();
+  // ---- flush (as tile_item3)
+  const size_t nxf = (size_t)N + 2;
+  for (int i = threadIdx.x; i < NV; i += NT) {
+    const int lz = i >> 8, ly = (i >> 4) & 15, lx = i & 15;
+    const int c = cell_slot(lx, ly, lz);
+    const float4 v = make_float4(S.are[c], S.aim[c], S.awt[c], S.aflag[c]);
+    if (v.x == 0.f && v.y == 0.f && v.z == 0.f && v.w == 0.f) continue;
+    const int vx = base[0] + lx, vy = base[1] + ly, vz = base[2] + lz;
+    if (vx > ext[0] || vy > ext[1] || vz > ext[2]) continue;
+    const size_t row = (size_t)(vy < 0 ? N + vy : vy);
+    const size_t slab = (size_t)(vz < 0 ? N + vz : vz);
+    const size_t di = (size_t)vx * 2 + row * nxf + slab * nxf * (size_t)N;
+    const size_t ni = (size_t)vx + row * (size_t)w2 + slab * (size_t)w2 * (size_t)N;
+    if (v.w != 0.f) {
+      atomicAdd(&J.data[di], v.x);
+      J.data[di + 1] = 0.0f;
+    } else {
+      atomicAdd(reinterpret_cast<float2 *>(&J.data[di]), make_float2(v.x, v.y));
+    }
+    if (v.z != 0.f) atomicAdd(&J.norm[ni], v.z);
+  }
+  __syncthreads();
+}
 }  // namespace col
 
 // work[i] = (job, tile, first slice, end slice); blocks are at most `block`.
@@ -767,6 +1035,74 @@ cudaError_t launch_column3(const InsertJob *d_jobs, const int4 *d_work, int nwor
   note_launch();
   k_column3<<<grid, col::NT, smem, st>>>(d_jobs, d_work, nwork, block, d_counter, c.d_exp, c.h2,
                                          c.h5, c.steps2, c.steps5, maxN, c.d_err);
+  return cudaGetLastError();
+}
+
+__global__ void __launch_bounds__(col::NT, 2)
+    k_pixel(const InsertJob *__restrict__ jobs, const int4 *__restrict__ work, int nwork,
+            int block, int *counter, float h2, ExpSteps st2, int maxN, int *err) {
+  extern __shared__ float4 s_dyn[];
+  __shared__ int s_work;
+  __shared__ int s_wcount[col::NT / 32];
+  __shared__ unsigned long long s_state[2];
+  __shared__ int s_next;
+  col::Smem4 S;
+  S.are = reinterpret_cast<float *>(s_dyn);
+  S.aim = S.are + col::NV;
+  S.awt = S.aim + col::NV;
+  S.aflag = S.awt + col::NV;
+  S.steps = s_dyn + col::NV;
+  S.rtab = reinterpret_cast<float *>(S.steps + col::STEP2CAP);
+  S.xmax = reinterpret_cast<int *>(S.rtab + maxN + 2);
+  S.hits = S.xmax + maxN;
+  S.rowc0 = S.hits + block;
+  S.rowoff = S.rowc0 + (col::NT / 32) * col::PROWS;
+  S.wcount = s_wcount;
+  S.next = &s_next;
+  S.state = s_state;
+  if (threadIdx.x == 0) { s_state[0] = ~0ull; s_state[1] = 0ull; }
+  while (true) {
+    __syncthreads();
+    if (threadIdx.x == 0) s_work = atomicAdd(counter, 1);
+    __syncthreads();
+    const int wi = s_work;
+    if (wi >= nwork) break;
+    const int4 wk = work[wi];
+    const InsertJob J = jobs[wk.x];
+    const int s0 = wk.z, s1 = min(min(wk.w, wk.z + block), J.np * J.nsym);
+    switch (J.mode) {
+      case MODE_GAUSS2: col::tile_item4<MODE_GAUSS2>(J, wk.y, s0, s1, S, h2, st2, err); break;
+      case MODE_NEAREST: col::tile_item4<MODE_NEAREST>(J, wk.y, s0, s1, S, h2, st2, err); break;
+      case MODE_TRILINEAR: col::tile_item4<MODE_TRILINEAR>(J, wk.y, s0, s1, S, h2, st2, err); break;
+      default:
+        if (threadIdx.x == 0) atomicOr(err, 4);   // gauss_5 takes the column kernel
+    }
+  }
+}
+
+cudaError_t launch_pixel(const InsertJob *d_jobs, const int4 *d_work, int nwork, int block,
+                         int *d_counter, int maxN, cudaStream_t st) {
+  if (nwork == 0) return cudaSuccess;
+  const Consts &c = consts();
+  const size_t smem = sizeof(float4) * (col::NV + col::STEP2CAP) + sizeof(float) * (maxN + 2) +
+                      sizeof(int) * maxN + sizeof(int) * block +
+                      sizeof(int) * (col::NT / 32) * (2 * col::PROWS + 1);
+  static size_t configured = 0;
+  if (configured < smem) {
+    cudaFuncSetAttribute(k_pixel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    configured = smem;
+  }
+  cudaError_t e = cudaMemsetAsync(d_counter, 0, sizeof(int), st);
+  if (e != cudaSuccess) return e;
+  int dev = 0, sms = 148, per_sm = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pixel, col::NT, smem);
+  if (per_sm < 1) per_sm = 1;
+  const int grid = std::max(1, std::min(nwork, sms * per_sm));
+  note_launch();
+  k_pixel<<<grid, col::NT, smem, st>>>(d_jobs, d_work, nwork, block, d_counter, c.h2, c.steps2,
+                                       maxN, c.d_err);
   return cudaGetLastError();
 }
 

@@ -118,6 +118,18 @@ void column_tiles(int N, int mode, int corners, std::vector<int> &out, int &tx, 
                   std::vector<float> *dist = nullptr);
 // The barrier-free column kernel (no patch staging; hits grouped by axis).
 constexpr int kColumn3Tile = kNumTiles + 1;
+// The pixel-major kernel for windows one or two taps wide (nearest,
+// gauss_2, trilinear); gauss_5 jobs given this id take k_column3.
+constexpr int kPixelTile = kNumTiles + 2;
+cudaError_t launch_pixel(const InsertJob *d_jobs, const int4 *d_work, int nwork, int block,
+                         int *d_counter, int maxN, cudaStream_t st);
+// The kernel a job of this mode runs for a requested tile id.
+inline int effective_tile(int tile, int mode) {
+  return (tile == kPixelTile && mode == 5 /* gauss_5 */) ? kColumn3Tile : tile;
+}
+inline bool is_column_tile(int tile) {
+  return tile == kColumnTile || tile == kColumn3Tile || tile == kPixelTile;
+}
 cudaError_t launch_column3(const InsertJob *d_jobs, const int4 *d_work, int nwork, int block,
                            int *d_counter, int maxN, cudaStream_t st);
 // Ordered work list (tile ids of a job that can receive interior taps).

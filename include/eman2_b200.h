@@ -304,8 +304,9 @@ FR_API int fr_batch_get_accumulators(fr_batch *b, int job, float *data, float *n
 /* Schedule selection for the insertion, measured on the device with
  * nparticles random slices and cached per (N, mode, nsym): candidates are the
  * register-tile gather shapes 0-3, the staged column kernel (4), the
- * barrier-free column kernel (5) and the atomic scatter (tile_out = -2).
- * ms_out, if not NULL, receives 7 timings in that order.  fr_set_tile pins a
+ * barrier-free column kernel (5), the pixel-major kernel for windows one or
+ * two taps wide (6; not for gauss_5) and the atomic scatter (tile_out = -2).
+ * ms_out, if not NULL, receives 8 timings in that order (-1: not run).  fr_set_tile pins a
  * choice (-1 clears it).  No counterpart in the reference. */
 FR_API int fr_autotune(int N, int mode, int nsym, int nparticles, int *tile_out,
                        float *ms_out);

@@ -61,11 +61,11 @@ def test_autotune_and_mixed_schedules_in_one_batch(gpu):
     different one, the batch still gives every job its alone result."""
     from eman2_b200.batch import BatchReconstructor, autotune, set_tile
     tile, ms = autotune(48, "gauss_2", 1, nparticles=64)
-    assert tile in (0, 1, 2, 3, 4, 5, -2) and len(ms) == 7 and all(v > 0 for v in ms.values())
+    assert tile in (0, 1, 2, 3, 4, 5, 6, -2) and len(ms) == 8 and all(v > 0 for v in ms.values())
     set_tile(48, "gauss_2", 1, -1)
     jobs = _jobs()
     nsym = {"c1": 1, "d2": 4, "c3": 3}
-    pins = [-2, 1, 5, 4]
+    pins = [6, 1, 5, -2]
     try:
         for (params, _, _), t in zip(jobs, pins):
             set_tile(params["size"][0], params["mode"], nsym[params["sym"]], t)

@@ -34,7 +34,8 @@ def rand_rots(n, seed):
 def use_tile(N, mode, sym, tile):
     """Pin the gather schedule's kernel for (N, mode, sym): 0-3 the per-voxel
     register tiles, 4 the staged column-owner kernel, 5 the barrier-free
-    column kernel, -1 back to the default."""
+    column kernel, 6 the pixel-major kernel (gauss_5: 5), -1 back to the
+    default."""
     from eman2_b200 import _lib
     from oracle.oracle import sym_ops
     _lib.check(_lib.load().fr_set_tile(N, _lib.MODE_IDS[mode], len(sym_ops(sym)), tile))
@@ -59,7 +60,8 @@ def rel(a, b):
     return oracle.rel_l2(a, b)
 
 
-@pytest.mark.parametrize("sched", ["scatter", "gather_v1", "gather_column", "gather_column3"])
+@pytest.mark.parametrize("sched", ["scatter", "gather_v1", "gather_column", "gather_column3",
+                                   "gather_pixel"])
 @pytest.mark.parametrize("mode", ["nearest_neighbor", "gauss_2", "gauss_5", "trilinear"])
 @pytest.mark.parametrize("N,sym", [(16, "c1"), (22, "d2"), (32, "c3"), (40, "d1")])
 def test_insert_schedules_match_oracle(gpu, sched, mode, N, sym):
@@ -68,7 +70,8 @@ def test_insert_schedules_match_oracle(gpu, sched, mode, N, sym):
     w = np.random.default_rng(N + 2).uniform(0.5, 1.0, n).astype(np.float32)
     r = recon(N, mode, sym)
     if sched != "scatter":
-        use_tile(N, mode, sym, {"gather_v1": 0, "gather_column": 4, "gather_column3": 5}[sched])
+        use_tile(N, mode, sym, {"gather_v1": 0, "gather_column": 4, "gather_column3": 5,
+                                "gather_pixel": 6}[sched])
     try:
         st = r.insert_slices(sl, rt, w, schedule="scatter" if sched == "scatter" else "gather")
     finally:
