@@ -311,6 +311,7 @@ int stream_leave(fr_recon *r, cudaStream_t st) {
 InsertJob make_job(fr_recon *r, const float2 *slices, const float *t3d, const float *pw,
                           int np) {
   InsertJob j;
+  memset(&j, 0, sizeof j);   // padding too: jobs are compared bytewise for reuse
   j.data = r->vol_data.as<float>();
   j.norm = r->vol_norm.as<float>();
   j.slices = slices;
@@ -426,8 +427,7 @@ int insert_device(fr_recon *r, const float2 *d_slices, const float *d_t3d, const
             work.push_back(make_int4(0, r->tiles[ti], s0, std::min(b1, s0 + blk)));
         }
       TRY(r->s_work.ensure(sizeof(int4) * std::max<size_t>(1, work.size())));
-      CU(cudaMemcpyAsync(r->s_work.p, work.data(), sizeof(int4) * work.size(),
-                         cudaMemcpyHostToDevice, st));
+      TRY(r->ring_small.upload(r->s_work.p, work.data(), sizeof(int4) * work.size(), st));
       r->work_np = nsl;
       r->nwork = (int)work.size();
     }
@@ -436,25 +436,38 @@ int insert_device(fr_recon *r, const float2 *d_slices, const float *d_t3d, const
     std::vector<int2> work(r->tiles.size());
     for (size_t i = 0; i < work.size(); i++) work[i] = make_int2(0, r->tiles[i]);
     TRY(r->s_work.ensure(sizeof(int2) * std::max<size_t>(1, work.size())));
-    CU(cudaMemcpyAsync(r->s_work.p, work.data(), sizeof(int2) * work.size(),
-                       cudaMemcpyHostToDevice, st));
+    TRY(r->ring_small.upload(r->s_work.p, work.data(), sizeof(int2) * work.size(), st));
     r->work_np = -2;
   }
-  TRY(r->s_jobs.ensure(sizeof(InsertJob)));
+  // the job in device memory: one of the last two uploaded when unchanged (an
+  // upload queued behind a large copy would hold the stream up)
+  const void *jobs_before = r->s_jobs.p;
+  TRY(r->s_jobs.ensure(2 * sizeof(InsertJob)));
+  if (r->s_jobs.p != jobs_before) r->job_valid[0] = r->job_valid[1] = false;
   TRY(r->s_counter.ensure(sizeof(int)));
-  CU(cudaMemcpyAsync(r->s_jobs.p, &j, sizeof(InsertJob), cudaMemcpyHostToDevice, st));
+  int jslot = -1;
+  for (int q = 0; q < 2; q++)
+    if (r->job_valid[q] && memcmp(&r->job_cache[q], &j, sizeof j) == 0) jslot = q;
+  if (jslot < 0) {
+    jslot = r->job_next;
+    r->job_next ^= 1;
+    TRY(r->ring_small.upload(r->s_jobs.as<InsertJob>() + jslot, &j, sizeof(InsertJob), st));
+    r->job_cache[jslot] = j;
+    r->job_valid[jslot] = true;
+  }
+  const InsertJob *d_job = r->s_jobs.as<InsertJob>() + jslot;
   if (prof) CU(cudaEventRecord(ev[0], st));
   if (tile == kPixelTile)
-    CU(launch_pixel(r->s_jobs.as<InsertJob>(), r->s_work.as<int4>(), nwork, kColumnBlock,
+    CU(launch_pixel(d_job, r->s_work.as<int4>(), nwork, kColumnBlock,
                     r->s_counter.as<int>(), r->N, st));
   else if (tile == kColumn3Tile)
-    CU(launch_column3(r->s_jobs.as<InsertJob>(), r->s_work.as<int4>(), nwork, kColumnBlock,
+    CU(launch_column3(d_job, r->s_work.as<int4>(), nwork, kColumnBlock,
                       r->s_counter.as<int>(), r->N, st));
   else if (tile == kColumnTile)
-    CU(launch_column(r->s_jobs.as<InsertJob>(), r->s_work.as<int4>(), nwork, kColumnBlock,
+    CU(launch_column(d_job, r->s_work.as<int4>(), nwork, kColumnBlock,
                      r->s_counter.as<int>(), r->mode, st));
   else
-    CU(launch_gather(r->s_jobs.as<InsertJob>(), &j, 1, r->s_work.as<int2>(), (int)r->tiles.size(),
+    CU(launch_gather(d_job, &j, 1, r->s_work.as<int2>(), (int)r->tiles.size(),
                      tile, r->s_counter.as<int>(), r->mode, st));
   if (prof) CU(cudaEventRecord(ev[1], st));
   TRY(run_scatter(j, true, st));
@@ -528,20 +541,21 @@ bool prologue_meta(int N, int n, const fr_particle *meta, unsigned char *blk) {
   return any_ctf;
 }
 
-// Copies a metadata block into the handle's per-particle device arrays.
+MetaView meta_view(const unsigned char *d_meta, int n) {
+  MetaView v;
+  v.ctf = d_meta;
+  v.txy = reinterpret_cast<const float *>(d_meta + ctf_dev_size() * (size_t)n);
+  v.w = v.txy + 2 * (size_t)n;
+  v.rot = v.w + n;
+  return v;
+}
+
+// Copies a metadata block to the handle's device block (s_meta).
 int prologue_upload(fr_recon *r, int n, const unsigned char *blk, cudaStream_t st) {
-  const size_t cs = ctf_dev_size();
-  TRY(r->s_ctf.ensure(cs * n));
-  TRY(r->s_txy.ensure(sizeof(float) * 2 * n));
-  TRY(r->s_w.ensure(sizeof(float) * n));
-  TRY(r->s_rot.ensure(sizeof(float) * 9 * n));
-  const unsigned char *txy = blk + cs * n;
-  const unsigned char *w = txy + sizeof(float) * 2 * n;
-  const unsigned char *rot = w + sizeof(float) * n;
-  CU(cudaMemcpyAsync(r->s_ctf.p, blk, cs * n, cudaMemcpyHostToDevice, st));
-  CU(cudaMemcpyAsync(r->s_txy.p, txy, sizeof(float) * 2 * n, cudaMemcpyHostToDevice, st));
-  CU(cudaMemcpyAsync(r->s_w.p, w, sizeof(float) * n, cudaMemcpyHostToDevice, st));
-  CU(cudaMemcpyAsync(r->s_rot.p, rot, sizeof(float) * 9 * n, cudaMemcpyHostToDevice, st));
+  const size_t bytes = prologue_meta_bytes(n);
+  TRY(r->s_meta.ensure(bytes));
+  CU(cudaMemcpyAsync(r->s_meta.p, blk, bytes, cudaMemcpyHostToDevice, st));
+  r->d_meta = r->s_meta.as<unsigned char>();
   return FR_OK;
 }
 
@@ -549,6 +563,7 @@ int prologue_device(fr_recon *r, const float *d_raw, int n, int box, bool any_ct
   const int N = r->N;
   cudaStream_t st = r->stream;
   const size_t img = (size_t)N * N, spec = (size_t)N * (N / 2 + 1);
+  const MetaView mv = meta_view(r->d_meta, n);
   TRY(r->s_img.ensure(sizeof(float) * img * n));
   TRY(r->s_slices.ensure(sizeof(float) * slice_floats(N) * n));
   TRY(r->s_mean.ensure(sizeof(float) * n));
@@ -559,36 +574,38 @@ int prologue_device(fr_recon *r, const float *d_raw, int n, int box, bool any_ct
   const float *img_on = nullptr;
   if (any_ctf) {
     TRY(r->plans.exec2d(true, N, n, r->s_img.p, r->s_spec.p, st));
-    CU(launch_ctf_flip_dev(r->s_spec.as<cufftComplex>(), r->s_ctf.p, n, N, st));
+    CU(launch_ctf_flip_dev(r->s_spec.as<cufftComplex>(), mv.ctf, n, N, st));
     TRY(r->plans.exec2d(false, N, n, r->s_spec.p, r->s_img2.p, st));
     img_on = r->s_img2.as<float>();
   }
-  CU(launch_edge_mean(r->s_img.as<float>(), img_on, any_ctf ? r->s_ctf.p : nullptr, n, N,
+  CU(launch_edge_mean(r->s_img.as<float>(), img_on, any_ctf ? mv.ctf : nullptr, n, N,
                       r->s_mean.as<float>(), st));
   // preprocess_slice: shift, phase origin to corner, x sqrt((N+2)/N), r2c.
   // s_spec is the real staging for the r2c input.
   volatile float inv = 1.0f / (float)N;
   const float scale = sqrtf(inv * (float)(N + 2));
-  CU(launch_shift_corner(r->s_img.as<float>(), img_on, any_ctf ? r->s_ctf.p : nullptr,
-                         r->s_mean.as<float>(), r->s_txy.as<float>(), 2, n, N, scale,
+  CU(launch_shift_corner(r->s_img.as<float>(), img_on, any_ctf ? mv.ctf : nullptr,
+                         r->s_mean.as<float>(), mv.txy, 2, n, N, scale,
                          r->s_spec.as<float>(), st));
   TRY(r->plans.exec2d(true, N, n, r->s_spec.p, r->s_slices.p, st));
-  CU(launch_compose(r->s_rot.as<float>(), r->d_sym.as<float>(), n, r->nsym, r->s_t3d.as<float>(),
-                    st));
+  CU(launch_compose(mv.rot, r->d_sym.as<float>(), n, r->nsym, r->s_t3d.as<float>(), st));
   return FR_OK;
 }
 
 int prologue_chunk(fr_recon *r, const float *d_raw, int n, int box, const fr_particle *meta) {
-  std::vector<unsigned char> blk(prologue_meta_bytes(n));
-  const bool any_ctf = prologue_meta(r->N, n, meta, blk.data());
-  TRY(prologue_upload(r, n, blk.data(), r->stream));
+  int k;
+  unsigned char *blk;
+  TRY(r->ring_meta.acquire(prologue_meta_bytes(n), &k, &blk));
+  const bool any_ctf = prologue_meta(r->N, n, meta, blk);
+  TRY(prologue_upload(r, n, blk, r->stream));
+  TRY(r->ring_meta.done(k, r->stream));
   return prologue_device(r, d_raw, n, box, any_ctf);
 }
 
 int particles_chunk(fr_recon *r, const float *d_raw, int n, int box, const fr_particle *meta,
                     int schedule) {
   TRY(prologue_chunk(r, d_raw, n, box, meta));
-  return insert_device(r, r->s_slices.as<float2>(), r->s_t3d.as<float>(), r->s_w.as<float>(), n,
+  return insert_device(r, r->s_slices.as<float2>(), r->s_t3d.as<float>(), meta_view(r->d_meta, n).w, n,
                        schedule, nullptr, 0);
 }
 
@@ -689,10 +706,22 @@ int fr_destroy(fr_recon *r) {
     if (r->last) cudaEventSynchronize(r->done);
     if (r->stream) cudaStreamSynchronize(r->stream);
     DevBuf *bufs[] = {&r->vol_data, &r->vol_norm, &r->d_sym, &r->s_in, &r->s_slices, &r->s_rot,
+                      &r->s_meta,
                       &r->s_w, &r->s_t3d, &r->s_img, &r->s_img2, &r->s_spec, &r->s_ctf,
                       &r->s_mean, &r->s_txy, &r->s_out, &r->s_ssnr, &r->s_jobs, &r->s_work,
                       &r->s_counter};
     for (DevBuf *b : bufs) b->release();
+    for (int k = 0; k < 2; k++) {
+      r->s_stage[k].release();
+      if (r->staged[k]) cudaEventDestroy(r->staged[k]);
+      if (r->consumed[k]) cudaEventDestroy(r->consumed[k]);
+    }
+    r->ring_meta.release();
+    r->ring_small.release();
+    if (r->copy_st) {
+      cudaStreamSynchronize(r->copy_st);
+      cudaStreamDestroy(r->copy_st);
+    }
     if (r->done) cudaEventDestroy(r->done);
     if (r->own) cudaStreamDestroy(r->own);
   }
@@ -853,7 +882,7 @@ int fr_insert_slices(fr_recon *r, const float *slices, int n, const float *rot, 
   if (use_ssnr)
     TRY(to_device(ssnr, sizeof(float) * (size_t)nssnr * n, r->s_ssnr, st, &d_ss));
   TRY(r->s_w.ensure(sizeof(float) * n));
-  CU(cudaMemcpyAsync(r->s_w.p, w.data(), sizeof(float) * n, cudaMemcpyHostToDevice, st));
+  TRY(r->ring_small.upload(r->s_w.p, w.data(), sizeof(float) * n, st));
   TRY(r->s_t3d.ensure(sizeof(float) * 9 * (size_t)n * r->nsym));
   CU(launch_compose((const float *)d_rot, r->d_sym.as<float>(), n, r->nsym, r->s_t3d.as<float>(),
                     st));
@@ -904,7 +933,7 @@ int fr_insert_slices_wiener(fr_recon *r, const float *slices, int n, const float
   TRY(to_device(snr, sizeof(float) * (size_t)nsnr * n, r->s_ssnr, st, &d_snr));
   if (undo) TRY(to_device(undo, sizeof(int) * n, r->s_txy, st, &d_undo));
   TRY(r->s_w.ensure(sizeof(float) * n));
-  CU(cudaMemcpyAsync(r->s_w.p, w.data(), sizeof(float) * n, cudaMemcpyHostToDevice, st));
+  TRY(r->ring_small.upload(r->s_w.p, w.data(), sizeof(float) * n, st));
   TRY(r->s_t3d.ensure(sizeof(float) * 9 * (size_t)n * r->nsym));
   CU(launch_compose((const float *)d_rot, r->d_sym.as<float>(), n, r->nsym, r->s_t3d.as<float>(),
                     st));
@@ -935,20 +964,56 @@ int fr_insert_particles(fr_recon *r, const float *imgs, int n, int box, const fr
   const size_t per = (size_t)N * N * 4 * 5 + (size_t)box * box * 4;
   const int chunk = (int)std::max<size_t>(1, std::min<size_t>(8192, (8ull << 30) / per));
   const bool dev = is_device_ptr(imgs);
+  if (!dev && !r->copy_st) {
+    CU(cudaStreamCreateWithFlags(&r->copy_st, cudaStreamNonBlocking));
+    for (int k = 0; k < 2; k++) {
+      CU(cudaEventCreateWithFlags(&r->staged[k], cudaEventDisableTiming));
+      CU(cudaEventCreateWithFlags(&r->consumed[k], cudaEventDisableTiming));
+    }
+  }
+  int last = -1;
   for (int p0 = 0; p0 < n; p0 += chunk) {
     const int c = std::min(chunk, n - p0);
     const float *src = imgs + (size_t)p0 * box * box;
-    const float *d_raw = src;
-    if (!dev) {
-      TRY(r->s_in.ensure(sizeof(float) * (size_t)c * box * box));
-      CU(cudaMemcpyAsync(r->s_in.p, src, sizeof(float) * (size_t)c * box * box,
-                         cudaMemcpyHostToDevice, r->stream));
-      d_raw = r->s_in.as<float>();
+    if (dev) {
+      TRY(particles_chunk(r, src, c, box, meta + p0, schedule));
+      continue;
     }
-    TRY(particles_chunk(r, d_raw, c, box, meta + p0, schedule));
+    // Host images: the chunk's images and its metadata block go, on the copy
+    // stream, into the staging buffer the chunk before last used, once the
+    // work that read it is done.  Nothing is uploaded on the compute stream,
+    // where it would queue behind this copy on the copy engine.
+    const int k = r->stage_next;
+    r->stage_next ^= 1;
+    const size_t ibytes = sizeof(float) * (size_t)c * box * box;
+    const size_t moff = (ibytes + 255) & ~(size_t)255;
+    const size_t bytes = moff + prologue_meta_bytes(c);
+    if (r->s_stage[k].cap < bytes) {
+      if (r->consumed_set[k]) CU(cudaEventSynchronize(r->consumed[k]));
+      TRY(r->s_stage[k].ensure(bytes));
+    }
+    int slot;
+    unsigned char *blk;
+    TRY(r->ring_meta.acquire(prologue_meta_bytes(c), &slot, &blk));
+    const bool any_ctf = prologue_meta(r->N, c, meta + p0, blk);
+    if (r->consumed_set[k]) CU(cudaStreamWaitEvent(r->copy_st, r->consumed[k], 0));
+    unsigned char *stage = r->s_stage[k].as<unsigned char>();
+    CU(cudaMemcpyAsync(stage + moff, blk, prologue_meta_bytes(c), cudaMemcpyHostToDevice, r->copy_st));
+    TRY(r->ring_meta.done(slot, r->copy_st));
+    CU(cudaMemcpyAsync(stage, src, ibytes, cudaMemcpyHostToDevice, r->copy_st));
+    CU(cudaEventRecord(r->staged[k], r->copy_st));
+    CU(cudaStreamWaitEvent(r->stream, r->staged[k], 0));
+    last = k;
+    r->d_meta = stage + moff;
+    TRY(prologue_device(r, (const float *)stage, c, box, any_ctf));
+    TRY(insert_device(r, r->s_slices.as<float2>(), r->s_t3d.as<float>(), meta_view(r->d_meta, c).w,
+                      c, schedule, nullptr, 0));
+    CU(cudaEventRecord(r->consumed[k], r->stream));
+    r->consumed_set[k] = true;
   }
   TRY(stream_leave(r, r->stream));
-  if (!dev) CU(cudaStreamSynchronize(r->stream));   // host images: see fr_insert_slices
+  // host images may be pinned: return once they are read, not once inserted
+  if (last >= 0) CU(cudaEventSynchronize(r->staged[last]));
   return FR_OK;
 }
 

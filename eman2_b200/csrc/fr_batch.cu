@@ -49,10 +49,12 @@ namespace fr {
 // Device copies of a batched launch's job table and work list.
 struct BatchScratch {
   DevBuf d_jobs, d_work, d_counter;
+  PinnedRing ring;
   cudaEvent_t done = nullptr;     // after the last launch that read this scratch
   cudaStream_t last = nullptr;
   ~BatchScratch() {
     if (done) { cudaEventSynchronize(done); cudaEventDestroy(done); }
+    ring.release();
   }
 };
 }  // namespace fr
@@ -155,7 +157,8 @@ static int job_tile(const fr_recon *r, int tile_pref) {
 // Adds job r's InsertJob (its chunk's slices, rotations and weights in its
 // scratch) to the plan, with the tile list of its schedule.
 static void plan_add(RoundPlan &P, fr_recon *r, int owner, int np, int tile_pref) {
-  InsertJob J = make_job(r, r->s_slices.as<float2>(), r->s_t3d.as<float>(), r->s_w.as<float>(), np);
+  InsertJob J = make_job(r, r->s_slices.as<float2>(), r->s_t3d.as<float>(), meta_view(r->d_meta, np).w,
+                         np);
   const int tile = job_tile(r, tile_pref);
   if (tile != kTunedScatter && r->tiles_tile != tile) {
     if (is_column(tile))
@@ -237,10 +240,8 @@ static int plan_upload(const RoundPlan &P, BatchScratch &bs, cudaStream_t st) {
   TRY(bs.d_jobs.ensure(sizeof(InsertJob) * std::max<size_t>(1, P.hj.size())));
   TRY(bs.d_counter.ensure(sizeof(int)));
   TRY(bs.d_work.ensure(std::max<size_t>(16, P.work.size())));
-  CU(cudaMemcpyAsync(bs.d_jobs.p, P.hj.data(), sizeof(InsertJob) * P.hj.size(),
-                     cudaMemcpyHostToDevice, st));
-  if (!P.work.empty())
-    CU(cudaMemcpyAsync(bs.d_work.p, P.work.data(), P.work.size(), cudaMemcpyHostToDevice, st));
+  TRY(bs.ring.upload(bs.d_jobs.p, P.hj.data(), sizeof(InsertJob) * P.hj.size(), st));
+  if (!P.work.empty()) TRY(bs.ring.upload(bs.d_work.p, P.work.data(), P.work.size(), st));
   return FR_OK;
 }
 
@@ -367,7 +368,7 @@ int fr_insert_particles_multi(fr_recon *const *handles, int nh, const float *con
 
 namespace fr {
 struct JobBufs {
-  DevBuf img, slices, mean, spec, t3d, img2, ctf, txy, w, rot;
+  DevBuf img, slices, mean, spec, t3d, img2, meta;
   void swap_with(fr_recon *r) {
     std::swap(img, r->s_img);
     std::swap(slices, r->s_slices);
@@ -375,13 +376,10 @@ struct JobBufs {
     std::swap(spec, r->s_spec);
     std::swap(t3d, r->s_t3d);
     std::swap(img2, r->s_img2);
-    std::swap(ctf, r->s_ctf);
-    std::swap(txy, r->s_txy);
-    std::swap(w, r->s_w);
-    std::swap(rot, r->s_rot);
+    std::swap(meta, r->s_meta);
   }
   void release() {
-    for (DevBuf *b : {&img, &slices, &mean, &spec, &t3d, &img2, &ctf, &txy, &w, &rot}) b->release();
+    for (DevBuf *b : {&img, &slices, &mean, &spec, &t3d, &img2, &meta}) b->release();
   }
 };
 }  // namespace fr
@@ -497,8 +495,10 @@ static int graph_create(const std::vector<fr_recon *> &jobs, cudaStream_t st, in
     } else {
       const long long noted = launches_noted();
       for (int j = 0; j < nj && rc == FR_OK; j++)
-        if (counts[j] > 0)
+        if (counts[j] > 0) {
+          jobs[j]->d_meta = jobs[j]->s_meta.as<unsigned char>();   // the graph's block
           rc = prologue_device(jobs[j], g->slots[j].as<float>(), counts[j], boxes[j], g->ctf[j]);
+        }
       if (rc == FR_OK) rc = plan_launch(g->plan, g->bs, st);
       const cudaError_t e = cudaStreamEndCapture(st, &g->graph);
       if (rc == FR_OK && e != cudaSuccess)
@@ -573,7 +573,6 @@ int fr_graph_launch(fr_graph *g, const float *const *imgs, const fr_particle *co
   const int k = g->next;
   // this staging block was last read by the copies two replays ago
   if (g->staged_used[k]) CU(cudaEventSynchronize(g->staged[k]));
-  const size_t cs = ctf_dev_size();
   for (int j = 0; j < nj; j++) {
     const int n = g->counts[j];
     if (n == 0) continue;
@@ -590,15 +589,8 @@ int fr_graph_launch(fr_graph *g, const float *const *imgs, const fr_particle *co
   for (int j = 0; j < nj; j++) {
     const int n = g->counts[j];
     if (n == 0) continue;
-    const unsigned char *blk = g->pinned[k] + g->meta_off[j];
-    const unsigned char *txy = blk + cs * n;
-    const unsigned char *w = txy + sizeof(float) * 2 * n;
-    const unsigned char *rot = w + sizeof(float) * n;
-    fr::JobBufs &jb = g->bufs[j];
-    CU(cudaMemcpyAsync(jb.ctf.p, blk, cs * n, cudaMemcpyHostToDevice, st));
-    CU(cudaMemcpyAsync(jb.txy.p, txy, sizeof(float) * 2 * n, cudaMemcpyHostToDevice, st));
-    CU(cudaMemcpyAsync(jb.w.p, w, sizeof(float) * n, cudaMemcpyHostToDevice, st));
-    CU(cudaMemcpyAsync(jb.rot.p, rot, sizeof(float) * 9 * n, cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(g->bufs[j].meta.p, g->pinned[k] + g->meta_off[j], prologue_meta_bytes(n),
+                       cudaMemcpyHostToDevice, st));
   }
   CU(cudaEventRecord(g->staged[k], st));
   g->staged_used[k] = true;

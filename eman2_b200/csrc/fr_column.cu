@@ -1024,7 +1024,7 @@ cudaError_t launch_column3(const InsertJob *d_jobs, const int4 *d_work, int nwor
     cudaFuncSetAttribute(k_column3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     configured = smem;
   }
-  cudaError_t e = cudaMemsetAsync(d_counter, 0, sizeof(int), st);
+  cudaError_t e = zero_counter(d_counter, st);
   if (e != cudaSuccess) return e;
   int dev = 0, sms = 148, per_sm = 1;
   cudaGetDevice(&dev);
@@ -1092,7 +1092,7 @@ cudaError_t launch_pixel(const InsertJob *d_jobs, const int4 *d_work, int nwork,
     cudaFuncSetAttribute(k_pixel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     configured = smem;
   }
-  cudaError_t e = cudaMemsetAsync(d_counter, 0, sizeof(int), st);
+  cudaError_t e = zero_counter(d_counter, st);
   if (e != cudaSuccess) return e;
   int dev = 0, sms = 148, per_sm = 1;
   cudaGetDevice(&dev);
@@ -1130,7 +1130,7 @@ cudaError_t launch_column(const InsertJob *d_jobs, const int4 *d_work, int nwork
     cudaFuncSetAttribute(k_column, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     configured = smem;
   }
-  cudaError_t e = cudaMemsetAsync(d_counter, 0, sizeof(int), st);
+  cudaError_t e = zero_counter(d_counter, st);
   if (e != cudaSuccess) return e;
   int dev = 0, sms = 148, per_sm = 1;
   cudaGetDevice(&dev);

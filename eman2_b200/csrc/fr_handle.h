@@ -61,6 +61,73 @@ struct DevBuf {
 };
 
 
+// Pinned host staging for per-call uploads (metadata blocks, job tables,
+// work lists).  A pageable source would make cudaMemcpyAsync wait for the
+// stream to drain; from pinned memory the upload is queued and the host runs
+// ahead.  Slots are used in turn; a slot is rewritten only after the upload
+// that read it has completed.
+struct PinnedRing {
+  static constexpr int kSlots = 4;
+  unsigned char *buf[kSlots] = {};
+  size_t cap[kSlots] = {};
+  cudaEvent_t ev[kSlots] = {};
+  bool pending[kSlots] = {};
+  int next = 0;
+  // A pinned block of `bytes` for the caller to fill; *slot names it for done().
+  int acquire(size_t bytes, int *slot, unsigned char **out) {
+    const int k = next;
+    next = (next + 1) % kSlots;
+    if (pending[k]) {
+      if (cudaEventSynchronize(ev[k]) != cudaSuccess) return fail(FR_ECUDA, "staging wait failed");
+      pending[k] = false;
+    } else if (!ev[k] && cudaEventCreateWithFlags(&ev[k], cudaEventDisableTiming) != cudaSuccess) {
+      return fail(FR_ECUDA, "cudaEventCreate failed");
+    }
+    if (cap[k] < bytes) {
+      if (buf[k]) cudaFreeHost(buf[k]);
+      buf[k] = nullptr;
+      cap[k] = 0;
+      if (cudaHostAlloc((void **)&buf[k], bytes, cudaHostAllocDefault) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(FR_ENOMEM, "pinned host allocation of %zu bytes failed", bytes);
+      }
+      cap[k] = bytes;
+    }
+    *slot = k;
+    *out = buf[k];
+    return FR_OK;
+  }
+  // Marks the end of the uploads that read `slot` (queued on st).
+  int done(int slot, cudaStream_t st) {
+    if (cudaEventRecord(ev[slot], st) != cudaSuccess) return fail(FR_ECUDA, "cudaEventRecord failed");
+    pending[slot] = true;
+    return FR_OK;
+  }
+  // One upload of a host block through the ring.
+  int upload(void *dst, const void *src, size_t bytes, cudaStream_t st) {
+    if (bytes == 0) return FR_OK;
+    int k;
+    unsigned char *p;
+    int rc = acquire(bytes, &k, &p);
+    if (rc != FR_OK) return rc;
+    memcpy(p, src, bytes);
+    if (cudaMemcpyAsync(dst, p, bytes, cudaMemcpyHostToDevice, st) != cudaSuccess)
+      return fail(FR_ECUDA, "upload failed: %s", cudaGetErrorString(cudaGetLastError()));
+    return done(k, st);
+  }
+  void release() {
+    for (int k = 0; k < kSlots; k++) {
+      if (pending[k]) cudaEventSynchronize(ev[k]);
+      if (buf[k]) cudaFreeHost(buf[k]);
+      if (ev[k]) cudaEventDestroy(ev[k]);
+      buf[k] = nullptr;
+      ev[k] = nullptr;
+      cap[k] = 0;
+      pending[k] = false;
+    }
+  }
+};
+
 bool is_device_ptr(const void *p);
 int to_device(const void *src, size_t bytes, DevBuf &stage, cudaStream_t st, const void **out);
 int from_device(void *dst, const void *dsrc, size_t bytes, cudaStream_t st);
@@ -165,6 +232,23 @@ struct fr_recon {
   // stream first makes that stream wait for it.
   cudaEvent_t done = nullptr;
   cudaStream_t last = nullptr;
+  // Host particle chunks go through two device staging buffers filled on a
+  // copy stream: the upload of one chunk overlaps the work on the one before.
+  cudaStream_t copy_st = nullptr;
+  fr::DevBuf s_stage[2];
+  cudaEvent_t staged[2] = {nullptr, nullptr}, consumed[2] = {nullptr, nullptr};
+  bool consumed_set[2] = {false, false};
+  int stage_next = 0;
+  // pinned staging of the per-call uploads: chunk metadata, job and work lists
+  fr::PinnedRing ring_meta, ring_small;
+  // The current chunk's metadata block on the device (prologue_meta layout):
+  // s_meta for device inputs, or the tail of the chunk's staging buffer.
+  fr::DevBuf s_meta;
+  const unsigned char *d_meta = nullptr;
+  // Device copies of the last two insertion jobs, reused while unchanged.
+  fr::InsertJob job_cache[2];
+  bool job_valid[2] = {false, false};
+  int job_next = 0;
   std::mutex mu;
 };
 
@@ -188,6 +272,12 @@ int prologue_chunk(fr_recon *r, const float *d_raw, int n, int box, const fr_par
 size_t prologue_meta_bytes(int n);
 bool prologue_meta(int N, int n, const fr_particle *meta, unsigned char *blk);
 int prologue_upload(fr_recon *r, int n, const unsigned char *blk, cudaStream_t st);
+// The arrays of a metadata block of n particles (prologue_meta's layout).
+struct MetaView {
+  const void *ctf;
+  const float *txy, *w, *rot;
+};
+MetaView meta_view(const unsigned char *d_meta, int n);
 int prologue_device(fr_recon *r, const float *d_raw, int n, int box, bool any_ctf);
 int particles_chunk(fr_recon *r, const float *d_raw, int n, int box, const fr_particle *meta,
                     int schedule);

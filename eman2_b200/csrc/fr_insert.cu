@@ -138,6 +138,15 @@ __device__ __forceinline__ float pixel_weight(const InsertJob &J, int p, int x, 
   return sv > 0.0f ? sv : 0.0f;
 }
 
+// Resets a persistent launch's work counter.  A kernel rather than a memset:
+// on the copy engine a memset would queue behind uploads of other streams.
+__global__ void k_zero_int(int *p) { *p = 0; }
+
+cudaError_t zero_counter(int *d_counter, cudaStream_t st) {
+  k_zero_int<<<1, 1, 0, st>>>(d_counter);
+  return cudaGetLastError();
+}
+
 // grid.x covers the N*(N/2+1) pixel grid, grid.y = slice (particle*nsym+sym).
 template <int MODE>
 __global__ void __launch_bounds__(256) k_scatter(InsertJob J, const float *__restrict__ table,
@@ -607,7 +616,7 @@ cudaError_t launch_gather(const InsertJob *d_jobs, const InsertJob *h_jobs, int 
                           cudaStream_t st) {
   (void)h_jobs; (void)njobs;
   if (nwork == 0) return cudaSuccess;
-  cudaError_t e = cudaMemsetAsync(d_counter, 0, sizeof(int), st);
+  cudaError_t e = zero_counter(d_counter, st);
   if (e != cudaSuccess) return e;
   const int side = patch_side(tile, max_mode);
   switch (tile) {

@@ -55,6 +55,7 @@ struct InsertJob {
 
 // Launch accounting (fr_api.cu).
 void note_launch(int n = 1);
+cudaError_t zero_counter(int *d_counter, cudaStream_t st);
 long long launches_noted();
 
 // fast_exp(-r*h) as a function of r: the table index is monotone in r, so
