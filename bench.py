@@ -597,7 +597,27 @@ def run_gpu(args, wl, ws, rank, local):
         g1.record(stream)
         g1.synchronize()
         plain = args.plain / (g0.elapsed_time(g1) / 1e3)
-    return ms_max, e2e_ms, st, clk.summary(), plain
+    # agreement pass (determine_slice_agreement, sub=False) against the volume
+    # just built: n slices through the batched call, device-timed
+    agree = None
+    if rank == 0 and args.agree > 0:
+        g = torch.Generator(device=dev).manual_seed(11)
+        na = args.agree
+        sl = torch.randn((na, N, N + 2), device=dev, generator=g)
+        rots = torch.as_tensor(ps.rots[:na], device=dev) if not isinstance(ps.rots, torch.Tensor) \
+            else ps.rots[:na].contiguous()
+        wts = torch.ones(na, device=dev)
+        torch.cuda.synchronize()
+        r.slice_agreement(sl[:4], rots[:4], wts[:4])
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record(stream)
+        r.slice_agreement(sl, rots, wts)
+        a1.record(stream)
+        a1.synchronize()
+        ams = a0.elapsed_time(a1)
+        agree = {"slices": na, "ms": ams, "particle_slices_per_s": na / (ams / 1e3),
+                 "note": "sub=False, FP64 sums, every symmetry copy of every slice"}
+    return ms_max, e2e_ms, st, clk.summary(), plain, agree
 
 
 def main():
@@ -609,6 +629,8 @@ def main():
     ap.add_argument("--workload", default="c4", choices=sorted(WORKLOADS))
     ap.add_argument("--batch", type=int, default=2048, help="particles per step")
     ap.add_argument("--plain", type=int, default=64, help="particles timed on the plain path")
+    ap.add_argument("--agree", type=int, default=256,
+                    help="slices timed through the agreement pass (0: skip)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-serve", action="store_true", help="skip the batched and serving legs")
     ap.add_argument("--tile", type=int, default=-1,
@@ -648,7 +670,7 @@ def main():
         print(json.dumps(line))
         return
 
-    ms, e2e_ms, st, clk, plain = run_gpu(args, wl, ws, rank, local)
+    ms, e2e_ms, st, clk, plain, agree = run_gpu(args, wl, ws, rank, local)
     if rank != 0:
         return
     value = ws * args.steps * args.batch / (ms / 1e3)
@@ -693,6 +715,8 @@ def main():
                       "l2_red": "L2 red.global.add.f32 (3 per tap)"}[key],
             "achieved": taps_s, "peak": upd[key], "unit": "taps/s", "frac": taps_s / upd[key],
             "peaks_measured": upd, "taps": "upper bound S*p(N)*window"}
+    if agree is not None:
+        line["agreement"] = agree
     if plain is not None:
         line["plain_gpu"] = {"value": plain, "unit": "particle-slices/s", "sample": args.plain,
                              "speedup_batched_vs_plain": value / plain}
