@@ -19,12 +19,13 @@ from .emdata import EMData, Region
 from .exceptions import (DeviceException, ImageDimensionException, InvalidParameterException,
                          NotExistingObjectException, NullPointerException, StateException,
                          UnsupportedParameterException)
-from .reconstructor import FourierReconstructor, Reconstructors, WienerFourierReconstructor
+from .reconstructor import (FourierIterReconstructor, FourierReconstructor, Reconstructors,
+                            WienerFourierReconstructor)
 from .transform import Transform
 
 __all__ = [
     "EMData", "Region", "Transform", "Reconstructors", "FourierReconstructor",
-    "WienerFourierReconstructor",
+    "WienerFourierReconstructor", "FourierIterReconstructor",
     "InvalidParameterException", "ImageDimensionException", "NullPointerException",
     "NotExistingObjectException", "StateException", "DeviceException",
     "UnsupportedParameterException",

@@ -16,6 +16,7 @@ LIB_PATH = os.path.join(HERE, "libeman2_b200.so")
 
 FR_OK = 0
 MODE_IDS = {"nearest_neighbor": 1, "gauss_2": 2, "gauss_5": 5, "trilinear": 6}
+MODE_ITER = 7   # FourierIterReconstructor's inserter
 SCHED = {"auto": 0, "scatter": 1, "gather": 2}
 
 _P = ctypes.c_void_p
@@ -85,6 +86,7 @@ SIGNATURES = {
     "fr_set_tile": ([ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int),
     "fr_update_peaks": ([_P, _P, _P], ctypes.c_int),
     "fr_set_wiener": ([_P, ctypes.c_int], ctypes.c_int),
+    "fr_set_reference": ([_P, _P, ctypes.c_int], ctypes.c_int),
     "fr_insert_slices_wiener": ([_P, _P, ctypes.c_int, _P, _P, _P, ctypes.c_int, _P, _P],
                                 ctypes.c_int),
     "fr_decode_images": ([_P, ctypes.c_int, ctypes.c_int, ctypes.c_longlong, _P, _P], ctypes.c_int),

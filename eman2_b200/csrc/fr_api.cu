@@ -159,7 +159,10 @@ Geom *get_geom(int N, int corners) {
   for (int y = -n2; y < n2; y++) {
     int xm = -1;
     for (int x = 0; x <= n2; x++) {
-      if (corners == 2) {
+      if (corners == 3) {
+        // FourierIterReconstructor: r > iny/2+3 skipped (libEM/reconstructor.cpp:544-545)
+        if (hypot_fast_int(x, y) > n2 + 3) continue;
+      } else if (corners == 2) {
         // WienerFourierReconstructor: rn = (float)hypot(x/(inx-2), y/iny) < .5
         // (libEM/reconstructor.cpp:1703-1707)
         const float rx = (float)x / (float)N, ry = (float)y / (float)N;
@@ -321,6 +324,7 @@ InsertJob make_job(fr_recon *r, const float2 *slices, const float *t3d, const fl
   j.rtab = r->geom->d_rtab;
   j.rim = r->geom->d_rim;
   j.nrim = r->geom->nrim;
+  j.ref = r->has_ref ? r->ref.as<float>() : nullptr;
   j.wsnr = nullptr;
   j.wundo = nullptr;
   j.nwsnr = 0;
@@ -364,7 +368,7 @@ int insert_device(fr_recon *r, const float2 *d_slices, const float *d_t3d, const
     j.sscale = (float)(2.0 * (nssnr - 1) / (float)r->N);
   }
   const int tuned = tuned_tile(r->N, r->mode, r->nsym);
-  int sched = schedule;
+  int sched = r->mode == FR_MODE_ITER ? FR_SCHED_SCATTER : schedule;   // its inserter: scatter only
   if (sched == FR_SCHED_AUTO) {
     // Few slices: the per-tile culling and the volume read/write of the gather
     // pass are not amortised, so atomics win; a measured choice overrides.
@@ -672,7 +676,7 @@ int fr_create(const fr_params *p, fr_recon **out) {
     return fail(FR_EUNSUPPORTED, "odd sizes (fftodd volumes) are not supported (size %d)", p->nx);
   if (p->nx < 4 || p->nx > 4094) return fail(FR_EUNSUPPORTED, "size %d outside [4, 4094]", p->nx);
   if (p->mode != FR_MODE_NEAREST && p->mode != FR_MODE_GAUSS2 && p->mode != FR_MODE_GAUSS5 &&
-      p->mode != FR_MODE_TRILINEAR)
+      p->mode != FR_MODE_TRILINEAR && p->mode != FR_MODE_ITER)
     return fail(FR_EUNSUPPORTED, "inserter mode %d is not built", p->mode);
   std::vector<float> ops;
   const int ns = sym_ops(p->sym, ops);
@@ -694,7 +698,7 @@ int fr_create(const fr_params *p, fr_recon **out) {
     return fail(FR_ECUDA, "cudaEventCreate failed: %s", cudaGetErrorString(cudaGetLastError()));
   }
   consts();
-  r->geom = get_geom(r->N, p->corners);
+  r->geom = get_geom(r->N, p->mode == FR_MODE_ITER ? 3 : p->corners);
   *out = r;
   return FR_OK;
 }
@@ -706,7 +710,7 @@ int fr_destroy(fr_recon *r) {
     if (r->last) cudaEventSynchronize(r->done);
     if (r->stream) cudaStreamSynchronize(r->stream);
     DevBuf *bufs[] = {&r->vol_data, &r->vol_norm, &r->d_sym, &r->s_in, &r->s_slices, &r->s_rot,
-                      &r->s_meta,
+                      &r->s_meta, &r->ref,
                       &r->s_w, &r->s_t3d, &r->s_img, &r->s_img2, &r->s_spec, &r->s_ctf,
                       &r->s_mean, &r->s_txy, &r->s_out, &r->s_ssnr, &r->s_jobs, &r->s_work,
                       &r->s_counter};
@@ -756,6 +760,7 @@ int fr_setup(fr_recon *r) {
   CU(cudaMemsetAsync(r->vol_data.p, 0, vol_floats(r->N) * sizeof(float), r->stream));
   CU(cudaMemsetAsync(r->vol_norm.p, 0, norm_floats(r->N) * sizeof(float), r->stream));
   CU(cudaStreamSynchronize(r->stream));
+  r->has_ref = false;   // FourierIterReconstructor::setup drops the reference volume
   if (r->p.verbose) {
     printf("3D Fourier dimensions are %d %d %d\n", r->N + 2, r->N, r->N);
     printf("You will require approximately %1.3g GB of memory to reconstruct this volume\n",
@@ -870,6 +875,7 @@ int fr_insert_slices(fr_recon *r, const float *slices, int n, const float *rot, 
   // throws NotExistingObjectException (libEM/emdata_metadata.cpp:1142).
   bool any_neg = false;
   for (int i = 0; i < n; i++) any_neg |= w[i] < 0.0f;
+  if (r->mode == FR_MODE_ITER) any_neg = false;   // its insert_slice takes any weight as is
   if (any_neg && !have_ssnr)
     return fail(FR_ENOTEXIST, "The requested key does not exist: class_ssnr (a negative weight "
                 "selects the SSNR insertion path)");
@@ -892,6 +898,36 @@ int fr_insert_slices(fr_recon *r, const float *slices, int n, const float *rot, 
   // Host sources may be pinned, read by DMA after the call returns: finish
   // those reads before handing the buffers back to the caller.
   if (d_sl != slices || d_rot != rot || (use_ssnr && d_ss != ssnr)) CU(cudaStreamSynchronize(st));
+  return FR_OK;
+}
+
+int fr_set_reference(fr_recon *r, const float *vol, int is_complex) {
+  TRY(check_state(r));
+  if (!vol) return fail(FR_ENULL, "null reference volume");
+  if (r->mode != FR_MODE_ITER)
+    return fail(FR_EINVAL_PARAM, "a reference volume belongs to the iterative reconstructor");
+  std::lock_guard<std::mutex> lk(r->mu);
+  TRY(stream_enter(r, r->stream));
+  const int N = r->N;
+  cudaStream_t st = r->stream;
+  TRY(r->ref.ensure(vol_floats(N) * sizeof(float)));
+  if (is_complex) {
+    const cudaMemcpyKind k = is_device_ptr(vol) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    CU(cudaMemcpyAsync(r->ref.p, vol, vol_floats(N) * sizeof(float), k, st));
+  } else {
+    // seed->do_fft() after xform.phaseorigin.tocorner (libEM/reconstructor.cpp:481-488)
+    const size_t n3 = (size_t)N * N * N;
+    const void *d = nullptr;
+    TRY(to_device(vol, n3 * sizeof(float), r->s_in, st, &d));
+    TRY(r->s_out.ensure(n3 * sizeof(float)));
+    CU(launch_tocorner3(static_cast<const float *>(d), N, r->s_out.as<float>(), st));
+    cufftHandle plan;
+    TRY(r->plans.get3d_r2c(N, st, &plan));
+    CUFFT(cufftExecR2C(plan, r->s_out.as<cufftReal>(), r->ref.as<cufftComplex>()));
+  }
+  CU(cudaStreamSynchronize(st));
+  r->has_ref = true;
+  r->job_valid[0] = r->job_valid[1] = false;
   return FR_OK;
 }
 

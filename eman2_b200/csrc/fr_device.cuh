@@ -8,7 +8,7 @@
 
 namespace fr {
 
-enum { MODE_NEAREST = 1, MODE_GAUSS2 = 2, MODE_GAUSS5 = 5, MODE_TRILINEAR = 6 };
+enum { MODE_NEAREST = 1, MODE_GAUSS2 = 2, MODE_GAUSS5 = 5, MODE_TRILINEAR = 6, MODE_ITER = 7 };
 
 // Util::fast_exp (libEM/util.cpp:788-800): table of exp(-i/50) indexed by
 // (int)(-f*50.0 + 0.5) in double arithmetic; exp() outside [-19.98, 0].

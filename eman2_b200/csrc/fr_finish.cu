@@ -163,6 +163,24 @@ cudaError_t launch_finish_out(const float *d_real_padded, int N, float scale, fl
   return cudaGetLastError();
 }
 
+// xform.phaseorigin.tocorner of a real N^3 volume (even N): a circular shift
+// by N/2 along each axis.
+__global__ void k_tocorner3(const float *__restrict__ in, int N, float *__restrict__ out) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long n3 = (long)N * N * N;
+  if (i >= n3) return;
+  const int x = (int)(i % N), y = (int)((i / N) % N), z = (int)(i / ((long)N * N));
+  const int h = N / 2;
+  out[i] = in[((long)((z + h) % N) * N + (y + h) % N) * N + (x + h) % N];
+}
+
+cudaError_t launch_tocorner3(const float *d_in, int N, float *d_out, cudaStream_t st) {
+  const long n3 = (long)N * N * N;
+  note_launch();
+  k_tocorner3<<<(unsigned)((n3 + 255) / 256), 256, 0, st>>>(d_in, N, d_out);
+  return cudaGetLastError();
+}
+
 // FourierReconstructor::setup_seed (libEM/reconstructor.cpp:865-895):
 // data = seed * w (mult skips f == 1), norm = w, with the x=0 and x=N/2
 // planes at w/2 and four cells restored to w.

@@ -135,12 +135,24 @@ int from_device(void *dst, const void *dsrc, size_t bytes, cudaStream_t st);
 // ------------------------------------------------------------- cuFFT plans
 struct PlanCache {
   std::map<std::pair<int, int>, cufftHandle> r2c, c2r;   // key (N, batch)
-  cufftHandle c2r3 = 0;
-  int c2r3_N = 0;
+  cufftHandle c2r3 = 0, r2c3 = 0;
+  int c2r3_N = 0, r2c3_N = 0;
   ~PlanCache() {
     for (auto &kv : r2c) cufftDestroy(kv.second);
     for (auto &kv : c2r) cufftDestroy(kv.second);
     if (c2r3) cufftDestroy(c2r3);
+    if (r2c3) cufftDestroy(r2c3);
+  }
+  int get3d_r2c(int N, cudaStream_t st, cufftHandle *out) {
+    if (!r2c3 || r2c3_N != N) {
+      if (r2c3) cufftDestroy(r2c3);
+      r2c3 = 0;
+      CUFFT(cufftPlan3d(&r2c3, N, N, N, CUFFT_R2C));
+      r2c3_N = N;
+    }
+    CUFFT(cufftSetStream(r2c3, st));
+    *out = r2c3;
+    return FR_OK;
   }
   int get2d(bool forward, int N, int batch, cudaStream_t st, cufftHandle *out) {
     auto &m = forward ? r2c : c2r;
@@ -216,6 +228,8 @@ struct fr_recon {
   cudaStream_t own = nullptr, stream = nullptr;
   fr::Geom *geom = nullptr;
   fr::Geom *wgeom = nullptr;  // the Wiener reconstructor's pixel disk (looked up on first use)
+  fr::DevBuf ref;             // the iterative reconstructor's reference volume [N][N][N+2]
+  bool has_ref = false;
   float wfilt = 0.0f;         // 1: Wiener normalisation, data / (weight + 1)
   fr::DevBuf vol_data, vol_norm, d_sym;
   // scratch

@@ -101,6 +101,86 @@ __device__ __forceinline__ void insert_pixel_atomic(float *__restrict__ data, fl
   }
 }
 
+// EMData::get_complex_at(x, y, z) of a complex volume [N][N][N+2]
+// (libEM/emdata_core.cpp:134-144): 0 outside, the conjugate for x < 0.
+__device__ __forceinline__ float2 volume_at(const float *__restrict__ v, int N, int x, int y, int z) {
+  if (abs(x) >= (N + 2) / 2 || abs(y) > N / 2 || abs(z) > N / 2) return make_float2(0.f, 0.f);
+  const size_t nxf = (size_t)N + 2, nxy = nxf * (size_t)N;
+  if (x < 0) {
+    const size_t idx = (size_t)(-x * 2) + (size_t)(y <= 0 ? -y : N - y) * nxf +
+                       (size_t)(z <= 0 ? -z : N - z) * nxy;
+    return make_float2(__ldg(&v[idx]), -__ldg(&v[idx + 1]));
+  }
+  const size_t idx = (size_t)x * 2 + (size_t)(y < 0 ? N + y : y) * nxf + (size_t)(z < 0 ? N + z : z) * nxy;
+  return make_float2(__ldg(&v[idx]), __ldg(&v[idx + 1]));
+}
+
+// FourierIterReconstructor::insert_slice's per-pixel insertion
+// (libEM/reconstructor.cpp:555-640): the gauss_5 window (floor(xx-2.5), the
+// same reject rule) clamped with nx2 = nx/2-2 = N/2-1 along x; without a
+// reference volume a Gaussian of width h = 1/(|p|^2/4000 + .15) (at least
+// 0.1) and the pixel's value; with one, h = 1/2, cells past radius N/2
+// skipped, and the value dt + ref(i,j,k) - ref(p) (ref(p) trilinear).
+__device__ __forceinline__ void insert_pixel_iter(const InsertJob &J, float xx, float yy, float zz,
+                                                  float re, float im, float w,
+                                                  const float *__restrict__ table) {
+  const int N = J.N, n2 = N >> 1;
+  const int nx2 = n2 - 1, ny2 = n2, nz2 = n2;
+  int x0 = floor_minus_2p5(xx), y0 = floor_minus_2p5(yy), z0 = floor_minus_2p5(zz);
+  if (x0 < -nx2 - 4 || y0 < -ny2 - 4 || z0 < -nz2 - 4 || x0 > nx2 + 3 || y0 > ny2 + 3 || z0 > nz2 + 3)
+    return;
+  int x1 = x0 + 5, y1 = y0 + 5, z1 = z0 + 5;
+  x0 = max(x0, -nx2); x1 = min(x1, nx2);
+  y0 = max(y0, -ny2); y1 = min(y1, ny2);
+  z0 = max(z0, -nz2); z1 = min(z1, nz2);
+  float h;
+  float2 nodt = make_float2(0.f, 0.f);
+  if (J.ref) {
+    // Util::trilinear_interpolate_complex (libEM/util.h:645-654) of the 8
+    // cells around p, in its order of products and sums
+    const float fx = floorf(xx), fy = floorf(yy), fz = floorf(zz);
+    const float t = __fsub_rn(xx, fx), u = __fsub_rn(yy, fy), v = __fsub_rn(zz, fz);
+    const int ix = (int)fx, iy = (int)fy, iz = (int)fz;
+    const float t1 = __fsub_rn(1.0f, t), u1 = __fsub_rn(1.0f, u), v1 = __fsub_rn(1.0f, v);
+    const float c[8] = {__fmul_rn(__fmul_rn(t1, u1), v1), __fmul_rn(__fmul_rn(t, u1), v1),
+                        __fmul_rn(__fmul_rn(t1, u), v1),  __fmul_rn(__fmul_rn(t, u), v1),
+                        __fmul_rn(__fmul_rn(t1, u1), v),  __fmul_rn(__fmul_rn(t, u1), v),
+                        __fmul_rn(__fmul_rn(t1, u), v),   __fmul_rn(__fmul_rn(t, u), v)};
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      const float2 pq = volume_at(J.ref, N, ix + (q & 1), iy + ((q >> 1) & 1), iz + (q >> 2));
+      nodt.x = q ? __fadd_rn(nodt.x, __fmul_rn(c[q], pq.x)) : __fmul_rn(c[q], pq.x);
+      nodt.y = q ? __fadd_rn(nodt.y, __fmul_rn(c[q], pq.y)) : __fmul_rn(c[q], pq.y);
+    }
+    h = 0.5f;
+  } else {
+    const float hs = __fadd_rn(__fadd_rn(__fmul_rn(xx, xx), __fmul_rn(yy, yy)), __fmul_rn(zz, zz));
+    float hf = (float)(1.0 / ((double)__fdiv_rn(hs, 4000.0f) + 0.15));
+    if ((double)hf < 0.1) hf = (float)0.1;
+    h = hf;
+  }
+  const int ny2sq = N * N / 4;
+  for (int k = z0; k <= z1; k++)
+    for (int j = y0; j <= y1; j++)
+      for (int i = x0; i <= x1; i++) {
+        if (J.ref && i * i + j * j + k * k > ny2sq) continue;
+        const float r = dist2(i, j, k, xx, yy, zz);
+        const float gg = fast_exp(__fmul_rn(-r, h), table);
+        float vre, vim;
+        if (J.ref) {
+          const float2 nt = volume_at(J.ref, N, i, j, k);
+          const float ure = __fsub_rn(__fadd_rn(re, nt.x), nodt.x);
+          const float uim = __fsub_rn(__fadd_rn(im, nt.y), nodt.y);
+          vre = __fmul_rn(__fmul_rn(ure, gg), w);
+          vim = __fmul_rn(__fmul_rn(uim, gg), w);
+        } else {
+          vre = __fmul_rn(__fmul_rn(re, gg), w);
+          vim = __fmul_rn(__fmul_rn(im, gg), w);
+        }
+        add_tap_atomic(J.data, J.norm, N, i, j, k, vre, vim, __fmul_rn(gg, w));
+      }
+}
+
 // Per-pixel weight: the particle weight, or with usessnr the slice's
 // class_ssnr table at the pixel radius, max(0, ssnr[int(r*sscale)])
 // (libEM/reconstructor.cpp:1170-1184).
@@ -177,6 +257,26 @@ __global__ void __launch_bounds__(256) k_scatter(InsertJob J, const float *__res
   insert_pixel_atomic<MODE>(J.data, J.norm, N, xx, yy, zz, v.x, v.y, pw, h, table, false);
 }
 
+// The iterative reconstructor's insertion: one thread per pixel of its disk.
+__global__ void __launch_bounds__(256) k_scatter_iter(InsertJob J, const float *__restrict__ table) {
+  const int N = J.N, n2 = N >> 1, w2 = n2 + 1;
+  const int s = blockIdx.y;
+  const int p = s / J.nsym;
+  const float w = J.pw[p];
+  if (w == 0.0f) return;
+  const int pix = blockIdx.x * blockDim.x + threadIdx.x;
+  if (pix >= N * w2) return;
+  const int x = pix % w2, y = pix / w2 - n2;
+  if (x > __ldg(&J.xmax[y + n2])) return;
+  float M[6];
+#pragma unroll
+  for (int i = 0; i < 6; i++) M[i] = __ldg(&J.t3d[9 * s + i]);
+  float xx, yy, zz;
+  pixel_coords(__ldg(&J.rtab[x + n2]), __ldg(&J.rtab[y + n2]), M, (float)N, xx, yy, zz);
+  const float2 v = slice_value(J.slices + (size_t)p * N * w2, N, x, y);
+  insert_pixel_iter(J, xx, yy, zz, v.x, v.y, w, table);
+}
+
 // Face taps of rim pixels: grid.x covers the rim list, grid.y = slice.
 template <int MODE>
 __global__ void __launch_bounds__(128) k_edge(InsertJob J, const float *__restrict__ table,
@@ -213,6 +313,10 @@ cudaError_t launch_scatter(const InsertJob &j, cudaStream_t st) {
   const float *tab = consts().d_exp;
   const float h = mode_h(j.mode);
   note_launch();
+  if (j.mode == MODE_ITER) {
+    k_scatter_iter<<<grid, 256, 0, st>>>(j, tab);
+    return cudaGetLastError();
+  }
   switch (j.mode) {
     case MODE_NEAREST: k_scatter<MODE_NEAREST><<<grid, 256, 0, st>>>(j, tab, h); break;
     case MODE_GAUSS2: k_scatter<MODE_GAUSS2><<<grid, 256, 0, st>>>(j, tab, h); break;

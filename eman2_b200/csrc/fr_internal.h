@@ -18,7 +18,8 @@ namespace fr {
 // scalar arithmetic and kept on the device.
 struct Geom {
   int N = 0;
-  int corners = 0;           // 1: no radius cut; 2: the Wiener reconstructor's rn < 0.5 disk
+  int corners = 0;           // 1: no radius cut; 2: the Wiener reconstructor's rn < 0.5 disk;
+                             // 3: the iterative reconstructor's r <= N/2 + 3 disk
   int *d_xmax = nullptr;     // [N]: largest x kept in row y (index y+N/2), -1 none
   float *d_rtab = nullptr;   // [N+2]: (float)i/(float)N for i in [-N/2, N/2+1]
   int *d_rim = nullptr;      // rim pixels (x | (y+N/2)<<16) that can reach the cube faces
@@ -46,6 +47,7 @@ struct InsertJob {
   const float *wsnr;         // optional [np][nwsnr] ctf_snr_total curves (wiener_fourier)
   const int *wundo;          // optional [np]: the slice is Wiener filtered, undo it
   int nwsnr;
+  const float *ref;          // FourierIterReconstructor's reference volume [N][N][N+2] or null
   const float *ssnr;         // optional [np][nssnr] class_ssnr tables (usessnr)
   int nssnr;
   float sscale;              // 2*(nssnr-1)/N (libEM/reconstructor.cpp:1162)
@@ -155,6 +157,7 @@ cudaError_t launch_normalize(float *d_data, float *d_norm, int N, int sqrtnorm, 
                              float wfilt = 0.0f);
 cudaError_t launch_depad_center(const float *d_real_padded, int N, float scale, float *d_out,
                                 cudaStream_t st);
+cudaError_t launch_tocorner3(const float *d_in, int N, float *d_out, cudaStream_t st);
 cudaError_t launch_kernel_fix(float *d_vol, int nx, int ny, int nz, float gauss_width,
                               cudaStream_t st);
 cudaError_t launch_finish_out(const float *d_real_padded, int N, float scale, float gauss_width,

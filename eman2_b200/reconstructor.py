@@ -182,10 +182,12 @@ class FourierReconstructor:
     def _sym(self) -> str:
         return str(self.params.get("sym", "c1"))
 
+    MODE_ID = None   # a fixed inserter (subclasses), else the "mode" parameter's
+
     def _ensure_handle(self):
         size = self._size()
         mode = self._mode()
-        if mode not in _lib.MODE_IDS:
+        if self.MODE_ID is None and mode not in _lib.MODE_IDS:
             raise UnsupportedParameterException(
                 f"mode {mode!r}: the built inserters are {sorted(_lib.MODE_IDS)}")
         if "subvolume" in self.params:
@@ -198,7 +200,7 @@ class FourierReconstructor:
         lib = _lib.load()
         p = _lib.fr_params()
         p.nx, p.ny, p.nz = size
-        p.mode = _lib.MODE_IDS[mode]
+        p.mode = self.MODE_ID if self.MODE_ID is not None else _lib.MODE_IDS[mode]
         p.sym = self._sym().encode()[:15]
         p.corners = int(sig[3])
         p.sqrtnorm = int(sig[4])
@@ -519,10 +521,64 @@ class WienerFourierReconstructor(FourierReconstructor):
             "determine_slice_agreement of wiener_fourier is not built")
 
 
+class FourierIterReconstructor(FourierReconstructor):
+    """FourierIterReconstructor ("fourier_iter", libEM/reconstructor.cpp:430-682):
+    a gauss_5-shaped window whose width grows with resolution on the first
+    pass; given a seed (the previous iteration's map) it inserts the update
+    dt + ref(i,j,k) - ref(p) with a fixed width instead.  finish() normalises
+    without sqrtnorm; determine_slice_agreement does nothing and returns 0."""
+
+    NAME = "fourier_iter"
+    MODE_ID = _lib.MODE_ITER
+
+    def _ensure_handle(self):
+        self.params.pop("sqrtnorm", None)            # finish uses normalize_threed(0)
+        super()._ensure_handle()
+
+    def setup_seed(self, seed, seed_weight: float = 1.0):
+        """FourierIterReconstructor::setup_seed (:481-488): setup(), then the
+        seed (a real N^3 map, or its complex transform) as the reference."""
+        self.setup()
+        s = _host_or_device(seed.numpy() if isinstance(seed, EMData) else seed)
+        N = self.N
+        is_complex = tuple(s.shape[-3:]) == (N, N, N + 2)
+        if not is_complex and tuple(s.shape[-3:]) != (N, N, N):
+            raise ImageDimensionException(
+                "The dimensions of the seed volume do not match the reconstruction size")
+        with join_streams(library_stream(self._h), s):
+            _lib.check(_lib.load().fr_set_reference(self._h, _lib.ptr(s), int(is_complex)))
+
+    def setup_seedandweights(self, seed, weights):
+        """The weights are ignored, as in the reference (:490-499)."""
+        self.setup_seed(seed)
+
+    def clear(self):
+        """FourierIterReconstructor::clear (:501-503): setup() again."""
+        self.setup()
+
+    def insert_slice(self, img, xform, weight: float = 1.0) -> int:
+        """FourierIterReconstructor::insert_slice (:522-648).  Returns 0."""
+        if img is None:
+            raise NullPointerException("EMData pointer (input image) is NULL")
+        if self._state != 1:
+            self._require_setup()
+        sl = self._slice_of(img, xform)
+        rot = _rot_of(xform)
+        w = np.array([weight], np.float32)
+        status = (ctypes.c_int * 1)()
+        _lib.check(_lib.load().fr_insert_slices(self._h, _lib.ptr(sl), 1, _lib.ptr(rot), _lib.ptr(w),
+                                                None, 0, status, _lib.SCHED["scatter"]))
+        return 0
+
+    def determine_slice_agreement(self, img, xform, weight: float = 1.0, sub: bool = True) -> int:
+        return 0
+
+
 class Reconstructors:
     """Factory<Reconstructor> (libpyEM/libpyReconstructor2.cpp:221-226)."""
 
-    _known = {"fourier": FourierReconstructor, "wiener_fourier": WienerFourierReconstructor}
+    _known = {"fourier": FourierReconstructor, "wiener_fourier": WienerFourierReconstructor,
+              "fourier_iter": FourierIterReconstructor}
 
     @staticmethod
     def get(name: str, params: dict | None = None):

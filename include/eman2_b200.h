@@ -49,7 +49,8 @@ enum {
   FR_MODE_NEAREST = 1,   /* "nearest_neighbor" */
   FR_MODE_GAUSS2 = 2,    /* "gauss_2" (default) */
   FR_MODE_GAUSS5 = 5,    /* "gauss_5" */
-  FR_MODE_TRILINEAR = 6  /* "trilinear" */
+  FR_MODE_TRILINEAR = 6, /* "trilinear" */
+  FR_MODE_ITER = 7       /* FourierIterReconstructor ("fourier_iter") insertion */
 };
 
 /* Insertion schedules. */
@@ -225,6 +226,16 @@ FR_API int fr_insert_slices_noalloc(const float *d_slices, int n, int N, int mod
                                     const char *sym, const float *d_rot,
                                     const float *d_weights, float *d_data, float *d_norm,
                                     void *stream);
+
+/* FourierIterReconstructor ("fourier_iter", libEM/reconstructor.cpp:430-682):
+ * a handle created with mode FR_MODE_ITER inserts with that class's
+ * inserter (gauss_5 window clamped to |x| <= N/2-1, the r <= N/2+3 pixel
+ * disk; width 1/(|p|^2/4000+.15) without a reference volume, else width
+ * 1/2 and the update dt + ref(i,j,k) - ref(p)); fr_set_reference sets the
+ * reference from a seed (setup_seed, :481-488): a complex volume as is, or a
+ * real N^3 map after phase origin to corner and an r2c FFT.  fr_setup drops
+ * it. */
+FR_API int fr_set_reference(fr_recon *r, const float *vol, int is_complex);
 
 /* WienerFourierReconstructor ("wiener_fourier", libEM/reconstructor.cpp:1643-1731,
  * 1921-1947).  fr_set_wiener(r, 1) makes finish divide by (weight + 1)

@@ -407,6 +407,110 @@ OR_EXPORT int or_insert_slice_wiener(acc_t *vol_data, acc_t *vol_norm, int N, in
   return 0;
 }
 
+/* EMData::get_complex_at(x,y,z) of a complex volume [N][N][N+2]
+ * (libEM/emdata_core.cpp:134-144). */
+static void or_volume_at(const float *v, int N, int x, int y, int z, float *re, float *im) {
+  const int nx = N + 2, ny = N, nz = N;
+  const long nxy = (long)nx * ny;
+  if (abs(x) >= nx / 2 || abs(y) > ny / 2 || abs(z) > nz / 2) { *re = 0; *im = 0; return; }
+  if (x < 0) {
+    long idx = (long)(-x * 2) + (long)(y <= 0 ? -y : ny - y) * nx + (long)(z <= 0 ? -z : nz - z) * nxy;
+    *re = v[idx]; *im = -v[idx + 1];
+    return;
+  }
+  long idx = (long)x * 2 + (long)(y < 0 ? ny + y : y) * nx + (long)(z < 0 ? nz + z : z) * nxy;
+  *re = v[idx]; *im = v[idx + 1];
+}
+
+/* FourierIterReconstructor::insert_slice (libEM/reconstructor.cpp:522-648)
+ * for one slice with composed blocks t3d[nsym*9]; ref: the reference
+ * volume [N][N][N+2] or NULL.  Single precision as the reference computes. */
+OR_EXPORT int or_insert_slice_iter(acc_t *vol_data, acc_t *vol_norm, int N, const float *slice,
+                                   const float *t3d, int nsym, float weight, const float *ref) {
+  or_init_tables();
+  or_vol v;
+  v.data = vol_data; v.norm = vol_norm;
+  v.nx = N + 2; v.ny = N; v.nz = N;
+  v.nxyz = (long)v.nx * v.ny * v.nz;
+  const float inx = (float)(N + 2), iny = (float)N;
+  const int nx = N + 2, ny = N, nz = N;
+  const int nx2 = nx / 2 - 2, ny2 = ny / 2, nz2 = nz / 2;
+  const long ny2sq = (long)ny * ny / 4;
+  for (int s = 0; s < nsym; s++) {
+    const float *M = t3d + 9 * s;
+    for (int y = (int)(-iny / 2); y < iny / 2; y++) {
+      for (int x = 0; x < inx / 2; x++) {
+        const float rx = (float)x / (inx - 2.0f);
+        const float ry = (float)y / iny;
+        const int r = or_hypot_fast_int(x, y);
+        if (r > iny / 2 + 3 && fabsf(inx - iny) < 3) continue;
+        float xx = rx * M[0] + ry * M[3];
+        float yy = rx * M[1] + ry * M[4];
+        float zz = rx * M[2] + ry * M[5];
+        xx = xx * (float)(nx - 2);
+        yy = yy * (float)ny;
+        zz = zz * (float)nz;
+        int x0 = (int)floor(xx - 2.5), y0 = (int)floor(yy - 2.5), z0 = (int)floor(zz - 2.5);
+        real dre, dim;
+        or_slice_at(slice, nx, ny, x, y, &dre, &dim);
+        if (x0 < -nx2 - 4 || y0 < -ny2 - 4 || z0 < -nz2 - 4 || x0 > nx2 + 3 || y0 > ny2 + 3 || z0 > nz2 + 3)
+          continue;
+        int x1 = x0 + 5, y1 = y0 + 5, z1 = z0 + 5;
+        if (x0 < -nx2) x0 = -nx2;
+        if (x1 > nx2) x1 = nx2;
+        if (y0 < -ny2) y0 = -ny2;
+        if (y1 > ny2) y1 = ny2;
+        if (z0 < -nz2) z0 = -nz2;
+        if (z1 > nz2) z1 = nz2;
+        if (ref) {
+          const float xx0 = floorf(xx), yy0 = floorf(yy), zz0 = floorf(zz);
+          const float t = xx - xx0, u = yy - yy0, w3 = zz - zz0;
+          float pr[8], pi[8];
+          for (int q = 0; q < 8; q++)
+            or_volume_at(ref, N, (int)xx0 + (q & 1), (int)yy0 + ((q >> 1) & 1), (int)zz0 + (q >> 2),
+                         &pr[q], &pi[q]);
+          const float c[8] = {(1 - t) * (1 - u) * (1 - w3), t * (1 - u) * (1 - w3),
+                              (1 - t) * u * (1 - w3),       t * u * (1 - w3),
+                              (1 - t) * (1 - u) * w3,       t * (1 - u) * w3,
+                              (1 - t) * u * w3,             t * u * w3};
+          float nre = c[0] * pr[0], nim = c[0] * pi[0];
+          for (int q = 1; q < 8; q++) { nre = nre + c[q] * pr[q]; nim = nim + c[q] * pi[q]; }
+          const float h = 1.0f / 2.0f;
+          for (int k = z0; k <= z1; k++)
+            for (int j = y0; j <= y1; j++)
+              for (int i = x0; i <= x1; i++) {
+                if ((long)i * i + j * j + k * k > ny2sq) continue;
+                float tre, tim;
+                or_volume_at(ref, N, i, j, k, &tre, &tim);
+                const float ure = ((float)dre + tre) - nre, uim = ((float)dim + tim) - nim;
+                const float dx = (float)i - xx, dy = (float)j - yy, dz = (float)k - zz;
+                const float rl = (dx * dx + dy * dy) + dz * dz;
+                const float gg = (float)or_fast_exp((real)(-rl * h));
+                long off = or_add_complex_at(&v, i, j, k, (real)((ure * gg) * weight),
+                                             (real)((uim * gg) * weight));
+                if (off != v.nxyz) v.norm[off / 2] += (real)(gg * weight);
+              }
+        } else {
+          const float hs = (xx * xx + yy * yy) + zz * zz;
+          float h = (float)(1.0f / ((hs / 4000) + .15));
+          h = h < 0.1 ? (float)0.1 : h;
+          for (int k = z0; k <= z1; k++)
+            for (int j = y0; j <= y1; j++)
+              for (int i = x0; i <= x1; i++) {
+                const float dx = (float)i - xx, dy = (float)j - yy, dz = (float)k - zz;
+                const float rl = (dx * dx + dy * dy) + dz * dz;
+                const float gg = (float)or_fast_exp((real)(-rl * h));
+                long off = or_add_complex_at(&v, i, j, k, (real)(((float)dre * gg) * weight),
+                                             (real)(((float)dim * gg) * weight));
+                if (off != v.nxyz) v.norm[off / 2] += (real)(gg * weight);
+              }
+        }
+      }
+    }
+  }
+  return 0;
+}
+
 /* Convenience for tests: insert n slices with per-slice orientation blocks
  * arg[n*9] composed with the symmetry operators sym[nsym*9]. */
 OR_EXPORT int or_insert_batch(acc_t *vol_data, acc_t *vol_norm, int N, int mode,

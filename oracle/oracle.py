@@ -65,6 +65,8 @@ def _lib(kind: str = "fp32"):
     lib.or_insert_pixels.argtypes = [ctypes.c_int, R, R, ctypes.c_int, _F, ctypes.c_long]
     lib.or_normalize.argtypes = [R, R, ctypes.c_int, ctypes.c_int]
     lib.or_normalize_w.argtypes = [R, R, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    lib.or_insert_slice_iter.argtypes = [R, R, ctypes.c_int, _F, _F, ctypes.c_int, ctypes.c_float,
+                                         _F]
     lib.or_insert_slice_wiener.argtypes = [R, R, ctypes.c_int, ctypes.c_int, _F, _F, ctypes.c_int,
                                            ctypes.c_float, _F, ctypes.c_int, ctypes.c_int]
     lib.or_compare_slice.argtypes = [R, R, ctypes.c_int, _F, _F, ctypes.c_int, ctypes.c_float,
@@ -182,6 +184,22 @@ class OracleVolume:
                 int(bool(undo[p])) if undo is not None else 0)
             if rc:
                 raise RuntimeError(f"oracle insert failed rc={rc}")
+
+    def insert_iter(self, slices, rots, weights, sym="c1", ref=None):
+        """FourierIterReconstructor insert_slice for n slices; ref: the
+        reference volume (N, N, N+2) float32 or None."""
+        slices = np.ascontiguousarray(slices, np.float32).reshape(-1, self.N, self.N + 2)
+        n = slices.shape[0]
+        rots = np.ascontiguousarray(rots, np.float32).reshape(n, 9)
+        ops = np.ascontiguousarray(sym_ops(sym)).reshape(-1, 9)
+        refp = None if ref is None else np.ascontiguousarray(ref, np.float32)
+        t3d = np.empty((ops.shape[0], 9), np.float32)
+        for p in range(n):
+            for s in range(ops.shape[0]):
+                t3d[s] = compose(rots[p].reshape(3, 3), ops[s].reshape(3, 3)).reshape(9)
+            self.lib.or_insert_slice_iter(_rp(self.data), _rp(self.norm), self.N, _fp(slices[p]),
+                                          _fp(t3d), ops.shape[0], float(weights[p]),
+                                          _fp(refp) if refp is not None else None)
 
     def insert_omp(self, slices, rots, weights, mode="gauss_2", sym="c1", threads=0):
         assert self.kind == "omp"

@@ -69,9 +69,9 @@ def test_library_symmetry_matches_oracle(lib, sym):
 def test_params_and_exceptions():
     from eman2_b200 import (InvalidParameterException, NotExistingObjectException,
                             Reconstructors, UnsupportedParameterException)
-    assert Reconstructors.get_list() == ["fourier", "wiener_fourier"]
+    assert Reconstructors.get_list() == ["fourier", "wiener_fourier", "fourier_iter"]
     with pytest.raises(NotExistingObjectException):
-        Reconstructors.get("fourier_iter")        # FourierIterReconstructor is not built
+        Reconstructors.get("nn4")                 # SPARX reconstructors are not built
     with pytest.raises(InvalidParameterException):
         Reconstructors.get("fourier", {"size": [32] * 3, "bogus": 1})
     r = Reconstructors.get("fourier", {"size": [32] * 3, "sym": "d7"})

@@ -228,6 +228,49 @@ def test_wiener_pixel_weight_and_disk():
             assert v.data[0, y % N, 2 * x] == np.float32(d / (want + np.float32(1)))
 
 
+def test_iter_first_pass_width_and_x_clamp():
+    """FourierIterReconstructor without a reference (libEM/reconstructor.cpp:609-628):
+    taps weighted by fast_exp(-r * h), h = 1/(|p|^2/4000 + .15); the window is
+    clamped to |x| <= N/2 - 1 but |y|, |z| <= N/2."""
+    N = 16
+    sl = np.zeros((N, N + 2), np.float32)
+    sl[2, 2 * 3] = 1.0                                   # pixel (3, 2) -> point (3, 2, 0)
+    v = oracle.OracleVolume(N, "fp32")
+    v.insert_iter(sl[None], np.eye(3, dtype=np.float32)[None], np.ones(1, np.float32))
+    hs = np.float32(9 + 4)
+    h = np.float32(1.0 / (float(hs / np.float32(4000)) + 0.15))
+    for (i, j, k) in [(3, 2, 0), (4, 2, 1), (3, 3, -1)]:      # taps inside the exp table
+        r = np.float32((i - 3) ** 2 + (j - 2) ** 2 + k ** 2)
+        g = int(-float(np.float32(-r * h)) * 50.0 + 0.5)
+        want = np.float32(math.exp(-g / 50.0))
+        assert v.data[k % N, j % N, 2 * i] == want                  # the pixel's value * gg
+    # a pixel near x = N/2: no tap at x = N/2 (nx2 = N/2 - 1), taps at y = -N/2 kept
+    sl2 = np.zeros((N, N + 2), np.float32)
+    v2 = oracle.OracleVolume(N, "fp32")
+    v2.insert_iter(sl2[None], np.eye(3, dtype=np.float32)[None], np.ones(1, np.float32))
+    assert v2.norm[:, :, N // 2].max() == 0.0
+    assert v2.norm[:, N // 2, :].max() > 0.0
+
+
+def test_iter_reference_update_rule():
+    """With a reference volume the value inserted is dt + ref(i,j,k) - ref(p)
+    (ref(p) trilinear): a slice equal to the reference's section through a
+    constant reference inserts dt (the update terms cancel), weights
+    unchanged by the reference."""
+    N = 16
+    ref = np.zeros((N, N, N + 2), np.float32)
+    ref[..., 0::2] = 2.0                                # constant real reference
+    sl = np.zeros((N, N + 2), np.float32)
+    sl[1, 2 * 2] = 1.0
+    a = oracle.OracleVolume(N, "fp32")
+    a.insert_iter(sl[None], np.eye(3, dtype=np.float32)[None], np.ones(1, np.float32), ref=ref)
+    b = oracle.OracleVolume(N, "fp32")
+    b.insert_iter(sl[None], np.eye(3, dtype=np.float32)[None], np.ones(1, np.float32), ref=ref * 0)
+    # interior cells: the constant reference cancels; radius > N/2 cells are skipped in both
+    np.testing.assert_allclose(a.data, b.data, atol=1e-6)
+    np.testing.assert_array_equal(a.norm, b.norm)
+
+
 @pytest.mark.parametrize("N", [16, 20])
 def test_normalize_weights_conjugate_pairs(N):
     """normalize_threed sums conjugate-pair weights on the x=0 and x=N/2
