@@ -457,3 +457,33 @@ def insert_stack(recon, path: str, meta, chunk: int = 2048) -> int:
         recon.insert_particles(imgs, m)
         done += n
     return done
+
+
+def reconstruct_lst(recon, path: str, chunk: int = 2048, weights=None) -> int:
+    """e2spa_make3d's reconstruction loop over an #LSX particle list
+    (programs/e2spa_make3d.py:215-345): the records give each particle's
+    image (file and index), xform.projection, CTF and score; weights follow
+    initialize_data's score rule unless given; runs of consecutive images of
+    one .mrcs stack are streamed from disk and inserted in list order into
+    the set-up reconstructor `recon`.  Particles with weight <= 0 are skipped
+    (:303-305).  Returns the number of particles read."""
+    recs = load_lst_params(path)
+    if not recs:
+        return 0
+    meta = records_to_meta(recs, weights)
+    sz = ctypes.sizeof(_lib.fr_particle)
+    runs = []                                   # (src, first index, first record, count)
+    for i, r in enumerate(recs):
+        if runs and runs[-1][0] == r["src"] and runs[-1][1] + runs[-1][3] == r["idx"]:
+            src, first, start, count = runs[-1]
+            runs[-1] = (src, first, start, count + 1)
+        else:
+            runs.append((r["src"], r["idx"], i, 1))
+    done = 0
+    for src, first, start, count in runs:
+        for k0, imgs in StackStream(src, chunk, first=first, count=count):
+            n = imgs.shape[0]
+            m = (_lib.fr_particle * n).from_address(ctypes.addressof(meta) + (start + k0 - first) * sz)
+            recon.insert_particles(imgs, m)
+            done += n
+    return done

@@ -71,3 +71,39 @@ def test_streamed_insertion_equals_memory(gpu, tmp_path):
     assert io.insert_stack(b, p, meta, chunk=32) == 100
     (da, na), (db, nb) = a.get_accumulators(), b.get_accumulators()
     assert oracle.rel_l2(db, da) < 2e-6 and oracle.rel_l2(nb, na) < 2e-6
+
+
+def test_reconstruct_from_lst(gpu, tmp_path):
+    """An #LSX list over two stacks, in shuffled order: the streamed
+    reconstruction equals inserting the same particles, in list order, from
+    memory."""
+    import os
+
+    from eman2_b200 import FourierReconstructor, Transform
+    from eman2_b200.synth import make_particles
+    ps = make_particles(32, 40, seed=31, snr=0.5, shift=2.0, weights=None, ctf=False)
+    a, b = str(tmp_path / "a.mrcs"), str(tmp_path / "b.mrcs")
+    io.write_mrc(a, ps.images[:25])
+    io.write_mrc(b, ps.images[25:])
+    order = [3, 4, 5, 6, 30, 31, 32, 10, 0, 1, 2, 39, 38, 20, 21]
+    lst = io.LSXFile(str(tmp_path / "set.lst"))
+    for i in order:
+        m34 = np.zeros((3, 4), np.float32)
+        m34[:, :3] = ps.rots[i]
+        m34[:2, 3] = ps.shifts[i]
+        f, n = (a, i) if i < 25 else (b, i - 25)
+        lst.write(-1, n, f, {"xform.projection": Transform(m34), "score": -1.0 - 0.01 * i})
+    lst.close()
+    params = {"size": [48] * 3, "sym": "c2", "mode": "gauss_2"}
+    r = FourierReconstructor(params)
+    r.setup()
+    assert io.reconstruct_lst(r, str(tmp_path / "set.lst"), chunk=4) == len(order)
+    # the same records (matrices as the list stores them, 6 significant
+    # digits), the images from memory
+    m = io.records_to_meta(io.load_lst_params(str(tmp_path / "set.lst")))
+    r0 = FourierReconstructor(params)
+    r0.setup()
+    r0.insert_particles(np.ascontiguousarray(ps.images[order], np.float32), m)
+    (d, nr), (d0, n0) = r.get_accumulators(), r0.get_accumulators()
+    assert oracle.rel_l2(d, d0) < 2e-6 and oracle.rel_l2(nr, n0) < 2e-6
+    assert os.path.exists(a)
