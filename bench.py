@@ -735,4 +735,8 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    try:
+        main()
+    finally:
+        from eman2_b200 import replicas
+        replicas.finalize(int(os.environ.get("WORLD_SIZE", "1")))

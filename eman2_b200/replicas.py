@@ -19,6 +19,15 @@ def init(backend: str | None = None, timeout_s: int = 300):
     return ws, rank, local
 
 
+def finalize(ws: int):
+    """Every rank, after its last collective: barrier, then tear the group down."""
+    if ws > 1:
+        import torch.distributed as dist
+        if dist.is_initialized():
+            dist.barrier()
+            dist.destroy_process_group()
+
+
 def barrier(ws: int):
     if ws > 1:
         import torch.distributed as dist

@@ -24,8 +24,9 @@ def _worker(rank, ws, port, out):
     w, r, _ = replicas.init("gloo", timeout_s=60)
     replicas.barrier(w)
     out[r] = (replicas.max_over_ranks(1.5 + r, w), replicas.sum_over_ranks(1.0 + r, w))
+    replicas.finalize(w)
     import torch.distributed as dist
-    dist.destroy_process_group()
+    assert not dist.is_initialized()
 
 
 @pytest.mark.timeout(120)
