@@ -508,6 +508,7 @@ def run_batched(dev, seed: int = 33, pairs: int = 32, reps: int = 5, plain_sampl
         rec.close()
     plain = done / spent
     graph_rate = total / (ms_graph / 1e3)
+    overhead = per_job_overhead(params, boxes, imgs, metas, stream, reps)
     return {"jobs": len(params), "particles_per_round": total,
             "graph": {"ms_per_round": ms_graph, "particle_slices_per_s": graph_rate,
                       "capture_s": capture_s},
@@ -515,7 +516,80 @@ def run_batched(dev, seed: int = 33, pairs: int = 32, reps: int = 5, plain_sampl
             "plain_per_particle": {"particle_slices_per_s": plain,
                                    "sample": f"{plain_sample} particles of every 4th job"},
             "speedup_batched_vs_plain": graph_rate / plain,
+            "per_job_overhead": overhead,
             "autotuned": tuned}
+
+
+def per_job_overhead(params, boxes, imgs, metas, stream, reps: int = 5):
+    """Per-job latency overhead of the plain path against the batched form,
+    on the round's 64 jobs with ONE particle each.  "empty": the particle has
+    weight 0, so every stage runs (host call, metadata, prologue launches,
+    insertion launch, synchronisation) but no tap is added: the job's time is
+    all fixed cost.  "one_particle": weight as drawn, schedules from the
+    autotuner for one particle; a gauss_5 d7 job at N=240 is still ~7e7 taps,
+    so this one is mostly insertion.  Plain: one insert call per job, waited
+    for before the next (the drop-in loop's latency).  Batched: one replay of
+    a graph of all jobs (and one multi-job call without the graph), divided by
+    the job count.  Wall-clock, since the overhead is host and launch time."""
+    import torch
+
+    from eman2_b200 import _lib
+    from eman2_b200.batch import BatchReconstructor, autotune, insert_particles_multi, set_tile
+    nj = len(params)
+    combos = {(p["size"][0], p["mode"], nsym_of(p["sym"])) for p in params}
+    tuned = {f"N{k[0]} {k[1]} nsym{k[2]}": autotune(k[0], k[1], k[2], nparticles=1)[0]
+             for k in combos}
+    one_imgs = [im[:1] for im in imgs]
+
+    def first(m, weight=None):
+        a = (_lib.fr_particle * 1)()
+        ctypes.memmove(a, ctypes.addressof(m), ctypes.sizeof(_lib.fr_particle))
+        if weight is not None:
+            a[0].weight = weight
+        return a
+
+    def wall(fn, n):
+        for _ in range(2):
+            fn()
+        stream.synchronize()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(n):
+            fn()
+        stream.synchronize()
+        torch.cuda.synchronize()
+        return (time.perf_counter() - t0) / n
+
+    def measure(one_metas):
+        bp = BatchReconstructor(params)
+        try:
+            def plain_round():
+                for j in range(nj):
+                    bp.recons[j].insert_particles(one_imgs[j], one_metas[j], schedule="scatter")
+                    torch.cuda.synchronize()
+            plain_s = wall(plain_round, reps)
+            multi_s = wall(lambda: insert_particles_multi(bp.recons, one_imgs, one_metas, stream),
+                           reps)
+        finally:
+            bp.close()
+        bg = BatchReconstructor(params)
+        try:
+            g = bg.capture(boxes, [1] * nj, [True] * nj, stream=stream)
+            graph_s = wall(lambda: g.launch(one_imgs, one_metas), reps * 4)
+            g.close()
+        finally:
+            bg.close()
+        ms = lambda t: t * 1e3 / nj
+        return {"plain_ms_per_job": ms(plain_s), "no_graph_ms_per_job": ms(multi_s),
+                "graph_ms_per_job": ms(graph_s), "removed_x": plain_s / graph_s}
+
+    try:
+        empty = measure([first(m, 0.0) for m in metas])
+        one = measure([first(m) for m in metas])
+    finally:
+        for k in combos:
+            set_tile(k[0], k[1], k[2], -1)
+    return {"jobs": nj, "empty": empty, "one_particle": one, "autotuned_one_particle": tuned}
 
 
 # ------------------------------------------------------------------ GPU run

@@ -10,6 +10,7 @@ first) changes.
 from __future__ import annotations
 
 import ctypes
+import sys
 
 import numpy as np
 
@@ -18,18 +19,48 @@ from .emdata import EMData
 from .reconstructor import FourierReconstructor, _host_or_device, join_streams, library_stream
 
 
+def _meta_address(m):
+    """Address of an fr_particle array (or pointer); None stays None."""
+    if m is None:
+        return None
+    if isinstance(m, ctypes.Array):
+        return ctypes.addressof(m)
+    return ctypes.cast(m, ctypes.c_void_p).value
+
+
+def _particles(images):
+    """Particle arrays of a batched call as the library reads them, and their
+    addresses.  Contiguous float32 tensors pass through untouched: the common
+    case, kept cheap since a call converts one array per job."""
+    torch = sys.modules.get("torch")
+    keep, ptrs = [], []
+    for a in images:
+        if a is None:
+            keep.append(None)
+            ptrs.append(None)
+        elif torch is not None and isinstance(a, torch.Tensor) and a.dtype is torch.float32 \
+                and a.is_contiguous():
+            keep.append(a)
+            ptrs.append(a.data_ptr())
+        else:
+            a = _host_or_device(a)
+            keep.append(a)
+            ptrs.append(_lib.ptr(a))
+    return keep, ptrs
+
+
 def insert_particles_multi(recons, images, metas, stream=None):
     """One batched insertion tick over already set-up reconstructions:
     images[j] (n_j, box_j, box_j) and metas[j] (fr_particle array) go to
     recons[j]."""
     nj = len(recons)
     lib = _lib.load()
-    keep = [_host_or_device(im) for im in images]
+    keep, ptrs = _particles(images)
     handles = (ctypes.c_void_p * nj)(*[r.handle.value for r in recons])
-    imgs = (ctypes.c_void_p * nj)(*[_lib.ptr(a) for a in keep])
+    imgs = (ctypes.c_void_p * nj)(*ptrs)
     boxes = (ctypes.c_int * nj)(*[int(a.shape[-1]) for a in keep])
     counts = (ctypes.c_int * nj)(*[int(a.shape[0]) for a in keep])
-    metas_p = (ctypes.c_void_p * nj)(*[ctypes.cast(m, ctypes.c_void_p).value for m in metas])
+    metas_p = (ctypes.c_void_p * nj)(*[_meta_address(m) for m in metas])
     st = ctypes.c_void_p(stream.cuda_stream) if stream is not None else None
     with join_streams(st.value if st is not None else library_stream(recons[0].handle), *keep):
         _lib.check(lib.fr_insert_particles_multi(handles, nj, imgs, boxes, counts, metas_p, st))
@@ -62,8 +93,9 @@ class InsertGraph:
     (fr_graph_create): every replay inserts counts[j] particles of box
     boxes[j] into recons[j] through the same prologue and persistent launches
     as insert_particles_multi, without per-round host work beyond staging
-    the particles' metadata.  ctf[j]: whether job j's particles carry a CTF
-    (its replays must agree)."""
+    the particles' metadata and image addresses.  ctf[j]: whether job j's
+    particles carry a CTF (replays with CTF particles need it set for a job of
+    the same N, box and symmetry)."""
 
     def __init__(self, recons, boxes, counts, ctf, stream=None):
         lib = _lib.load()
@@ -88,17 +120,16 @@ class InsertGraph:
         return p.value
 
     def launch(self, images, metas):
-        """One replay.  images[j]: (counts[j], box, box) host or device
-        particles, or None to insert what the slots hold; metas[j]: fr_particle
-        arrays of counts[j] entries."""
+        """One replay.  images[j]: (counts[j], box, box) host particles (copied
+        into the slots) or device particles (read in place), or None to insert
+        what the slots hold; metas[j]: fr_particle arrays of counts[j] entries."""
         nj = len(self.recons)
-        metas_p = (ctypes.c_void_p * nj)(*[ctypes.cast(m, ctypes.c_void_p).value if m is not None
-                                          else None for m in metas])
+        metas_p = (ctypes.c_void_p * nj)(*[_meta_address(m) for m in metas])
         if images is None:
             _lib.check(_lib.load().fr_graph_launch(self._g, None, metas_p))
             return
-        keep = [_host_or_device(im) if im is not None else None for im in images]
-        imgs = (ctypes.c_void_p * nj)(*[_lib.ptr(a) if a is not None else None for a in keep])
+        keep, ptrs = _particles(images)
+        imgs = (ctypes.c_void_p * nj)(*ptrs)
         with join_streams(self.stream_ptr, *[a for a in keep if a is not None]):
             _lib.check(_lib.load().fr_graph_launch(self._g, imgs, metas_p))
 

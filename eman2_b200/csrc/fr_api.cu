@@ -300,13 +300,33 @@ int check_state(fr_recon *r) {
 }
 
 int stream_enter(fr_recon *r, cudaStream_t st) {
-  if (r->last && r->last != st) CU(cudaStreamWaitEvent(st, r->done, 0));
+  if (r->last && r->last != st) CU(cudaStreamWaitEvent(st, r->done->ev, 0));
+  return FR_OK;
+}
+
+static int new_event(std::shared_ptr<SharedEvent> &out) {
+  auto e = std::make_shared<SharedEvent>();
+  CU(cudaEventCreateWithFlags(&e->ev, cudaEventDisableTiming));
+  out = std::move(e);
   return FR_OK;
 }
 
 int stream_leave(fr_recon *r, cudaStream_t st) {
-  CU(cudaEventRecord(r->done, st));
+  // a shared event still marks the other handles' point: take a fresh one
+  if (!r->done || r->done.use_count() > 1) TRY(new_event(r->done));
+  CU(cudaEventRecord(r->done->ev, st));
   r->last = st;
+  return FR_OK;
+}
+
+int stream_leave_all(const std::vector<fr_recon *> &rs, cudaStream_t st) {
+  std::shared_ptr<SharedEvent> e;
+  TRY(new_event(e));
+  CU(cudaEventRecord(e->ev, st));
+  for (fr_recon *r : rs) {
+    r->done = e;
+    r->last = st;
+  }
   return FR_OK;
 }
 
@@ -525,13 +545,18 @@ size_t prologue_meta_bytes(int n) {
 // Writes [CTF constants: ctf_dev_size()*n][txy: 2n][w: n][rot: 9n] into blk;
 // returns whether any particle carries a CTF.
 bool prologue_meta(int N, int n, const fr_particle *meta, unsigned char *blk) {
+  return prologue_meta_range(N, n, 0, n, meta, blk);
+}
+
+bool prologue_meta_range(int N, int n, int first, int count, const fr_particle *meta,
+                         unsigned char *blk) {
   const size_t cs = ctf_dev_size();
   float *txy = reinterpret_cast<float *>(blk + cs * n);
   float *w = txy + 2 * (size_t)n;
   float *rot = w + n;
   bool any_ctf = false;
-  for (int i = 0; i < n; i++) {
-    const fr_particle &m = meta[i];
+  for (int i = first; i < first + count; i++) {
+    const fr_particle &m = meta[i - first];
     ctf_constants(m.defocus, m.dfdiff, m.dfang, m.voltage, m.cs, m.apix, m.ampcont, N,
                   blk + cs * i);
     if (std::fabs(m.defocus) > 1e-4f) any_ctf = true;
@@ -563,37 +588,47 @@ int prologue_upload(fr_recon *r, int n, const unsigned char *blk, cudaStream_t s
   return FR_OK;
 }
 
-int prologue_device(fr_recon *r, const float *d_raw, int n, int box, bool any_ctf) {
-  const int N = r->N;
-  cudaStream_t st = r->stream;
+int prologue_run(PlanCache &plans, const ProScratch &b, const unsigned char *d_meta,
+                 const float *d_raw, const float *const *d_src, int n, int box, int N,
+                 const float *d_sym, int nsym, bool any_ctf, cudaStream_t st, bool exact_fft) {
   const size_t img = (size_t)N * N, spec = (size_t)N * (N / 2 + 1);
-  const MetaView mv = meta_view(r->d_meta, n);
-  TRY(r->s_img.ensure(sizeof(float) * img * n));
-  TRY(r->s_slices.ensure(sizeof(float) * slice_floats(N) * n));
-  TRY(r->s_mean.ensure(sizeof(float) * n));
-  TRY(r->s_spec.ensure(std::max(sizeof(cufftComplex) * spec, sizeof(float) * img) * n));
-  TRY(r->s_t3d.ensure(sizeof(float) * 9 * (size_t)n * r->nsym));
-  if (any_ctf) TRY(r->s_img2.ensure(sizeof(float) * img * n));
-  CU(launch_pad(d_raw, n, box, N, r->s_img.as<float>(), st));
+  const MetaView mv = meta_view(d_meta, n);
+  TRY(b.img->ensure(sizeof(float) * img * n));
+  TRY(b.slices->ensure(sizeof(float) * slice_floats(N) * n));
+  TRY(b.mean->ensure(sizeof(float) * n));
+  TRY(b.spec->ensure(std::max(sizeof(cufftComplex) * spec, sizeof(float) * img) * n));
+  TRY(b.t3d->ensure(sizeof(float) * 9 * (size_t)n * nsym));
+  if (any_ctf) TRY(b.img2->ensure(sizeof(float) * img * n));
+  CU(launch_pad_compose(d_raw, d_src, n, box, N, b.img->as<float>(), mv.rot, d_sym, nsym,
+                        b.t3d->as<float>(), st));
   const float *img_on = nullptr;
   if (any_ctf) {
-    TRY(r->plans.exec2d(true, N, n, r->s_img.p, r->s_spec.p, st));
-    CU(launch_ctf_flip_dev(r->s_spec.as<cufftComplex>(), mv.ctf, n, N, st));
-    TRY(r->plans.exec2d(false, N, n, r->s_spec.p, r->s_img2.p, st));
-    img_on = r->s_img2.as<float>();
+    TRY(plans.exec2d(true, N, n, b.img->p, b.spec->p, st, exact_fft));
+    CU(launch_ctf_flip_dev(b.spec->as<cufftComplex>(), mv.ctf, n, N, st));
+    TRY(plans.exec2d(false, N, n, b.spec->p, b.img2->p, st, exact_fft));
+    img_on = b.img2->as<float>();
   }
-  CU(launch_edge_mean(r->s_img.as<float>(), img_on, any_ctf ? mv.ctf : nullptr, n, N,
-                      r->s_mean.as<float>(), st));
-  // preprocess_slice: shift, phase origin to corner, x sqrt((N+2)/N), r2c.
-  // s_spec is the real staging for the r2c input.
+  // edge mean; preprocess_slice: shift, phase origin to corner,
+  // x sqrt((N+2)/N), r2c.  spec is the real staging for the r2c input.
   volatile float inv = 1.0f / (float)N;
   const float scale = sqrtf(inv * (float)(N + 2));
-  CU(launch_shift_corner(r->s_img.as<float>(), img_on, any_ctf ? mv.ctf : nullptr,
-                         r->s_mean.as<float>(), mv.txy, 2, n, N, scale,
-                         r->s_spec.as<float>(), st));
-  TRY(r->plans.exec2d(true, N, n, r->s_spec.p, r->s_slices.p, st));
-  CU(launch_compose(mv.rot, r->d_sym.as<float>(), n, r->nsym, r->s_t3d.as<float>(), st));
+  if (mean_shift_fused(n, N)) {
+    CU(launch_mean_shift_corner(b.img->as<float>(), img_on, any_ctf ? mv.ctf : nullptr, mv.txy, 2,
+                                n, N, scale, b.spec->as<float>(), st));
+  } else {
+    CU(launch_edge_mean(b.img->as<float>(), img_on, any_ctf ? mv.ctf : nullptr, n, N,
+                        b.mean->as<float>(), st));
+    CU(launch_shift_corner(b.img->as<float>(), img_on, any_ctf ? mv.ctf : nullptr,
+                           b.mean->as<float>(), mv.txy, 2, n, N, scale, b.spec->as<float>(), st));
+  }
+  TRY(plans.exec2d(true, N, n, b.spec->p, b.slices->p, st, exact_fft));
   return FR_OK;
+}
+
+int prologue_device(fr_recon *r, const float *d_raw, int n, int box, bool any_ctf) {
+  const ProScratch b{&r->s_img, &r->s_slices, &r->s_mean, &r->s_spec, &r->s_t3d, &r->s_img2};
+  return prologue_run(r->plans, b, r->d_meta, d_raw, nullptr, n, box, r->N, r->d_sym.as<float>(),
+                      r->nsym, any_ctf, r->stream);
 }
 
 int prologue_chunk(fr_recon *r, const float *d_raw, int n, int box, const fr_particle *meta) {
@@ -692,7 +727,7 @@ int fr_create(const fr_params *p, fr_recon **out) {
     return fail(FR_ECUDA, "cudaStreamCreate failed: %s", cudaGetErrorString(cudaGetLastError()));
   }
   r->stream = r->own;
-  if (cudaEventCreateWithFlags(&r->done, cudaEventDisableTiming) != cudaSuccess) {
+  if (new_event(r->done) != FR_OK) {
     cudaStreamDestroy(r->own);
     delete r;
     return fail(FR_ECUDA, "cudaEventCreate failed: %s", cudaGetErrorString(cudaGetLastError()));
@@ -707,7 +742,7 @@ int fr_destroy(fr_recon *r) {
   if (!r) return FR_OK;
   {
     std::lock_guard<std::mutex> lk(r->mu);
-    if (r->last) cudaEventSynchronize(r->done);
+    if (r->last) cudaEventSynchronize(r->done->ev);
     if (r->stream) cudaStreamSynchronize(r->stream);
     DevBuf *bufs[] = {&r->vol_data, &r->vol_norm, &r->d_sym, &r->s_in, &r->s_slices, &r->s_rot,
                       &r->s_meta, &r->ref,
@@ -726,7 +761,7 @@ int fr_destroy(fr_recon *r) {
       cudaStreamSynchronize(r->copy_st);
       cudaStreamDestroy(r->copy_st);
     }
-    if (r->done) cudaEventDestroy(r->done);
+    r->done.reset();
     if (r->own) cudaStreamDestroy(r->own);
   }
   delete r;

@@ -3,9 +3,10 @@
 //
 // A batch holds independent FourierReconstructor states (uneven N, modes and
 // symmetries: even/odd half maps, heterogeneity classes).  Each insert call
-// runs every job's prologue on the batch stream, then ONE persistent insertion
-// launch (k_column) whose work list interleaves all jobs' (tile, slice block)
-// items, heaviest first, then the small face-tap kernels.
+// runs one prologue per group of jobs of equal (N, box, symmetry) on the batch
+// stream, then per schedule ONE persistent insertion launch whose work list
+// interleaves all its jobs' (tile, slice block) items, heaviest first, and one
+// launch of their face taps (or one scatter launch over all its jobs' slices).
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -46,16 +47,31 @@ int default_tile(int mode, int N, int nsym, int np) {
 
 // ------------------------------------------------------------------ batch
 namespace fr {
-// Device copies of a batched launch's job table and work list.
+// Scratch of one prologue group (see ProGroup).
+struct ProBufs {
+  DevBuf img, slices, mean, spec, t3d, img2;
+  ProScratch view() { return {&img, &slices, &mean, &spec, &t3d, &img2}; }
+  void release() {
+    for (DevBuf *b : {&img, &slices, &mean, &spec, &t3d, &img2}) b->release();
+  }
+};
+
+// Device copies of a batched launch's job table and work list, the round's
+// metadata block and the prologue groups' scratch.
 struct BatchScratch {
-  DevBuf d_jobs, d_work, d_counter;
+  DevBuf d_jobs, d_work, d_counter, d_meta;
+  std::vector<ProBufs> gbufs;
   PinnedRing ring;
   cudaEvent_t done = nullptr;     // after the last launch that read this scratch
   cudaStream_t last = nullptr;
-  ~BatchScratch() {
-    if (done) { cudaEventSynchronize(done); cudaEventDestroy(done); }
+  void release() {
+    if (done) { cudaEventSynchronize(done); cudaEventDestroy(done); done = nullptr; }
+    for (DevBuf *b : {&d_jobs, &d_work, &d_counter, &d_meta}) b->release();
+    for (ProBufs &g : gbufs) g.release();
+    gbufs.clear();
     ring.release();
   }
+  ~BatchScratch() { release(); }
 };
 }  // namespace fr
 
@@ -135,6 +151,10 @@ static int lock_handles(const std::vector<fr_recon *> &jobs,
 struct RoundGroup {
   int tile = 0, max_mode = FR_MODE_NEAREST, maxN = 0;
   size_t off = 0, nwork = 0;   // byte offset and item count in the work buffer
+  // (job, slice) units of the group's scatter, or of its face taps after a
+  // gather launch: offset in the work buffer, count, largest pixel (rim) count
+  size_t units_off = 0, nunits = 0;
+  int max_px = 0;
 };
 struct RoundPlan {
   std::vector<InsertJob> hj;
@@ -154,11 +174,11 @@ static int job_tile(const fr_recon *r, int tile_pref) {
   return effective_tile(t != -1 ? t : default_tile(r->mode, r->N, r->nsym, 0), r->mode);
 }
 
-// Adds job r's InsertJob (its chunk's slices, rotations and weights in its
-// scratch) to the plan, with the tile list of its schedule.
-static void plan_add(RoundPlan &P, fr_recon *r, int owner, int np, int tile_pref) {
-  InsertJob J = make_job(r, r->s_slices.as<float2>(), r->s_t3d.as<float>(), meta_view(r->d_meta, np).w,
-                         np);
+// Adds job r's InsertJob (its chunk's np slices, composed rotations and
+// weights) to the plan, with the tile list of its schedule.
+static void plan_add(RoundPlan &P, fr_recon *r, int owner, int np, int tile_pref,
+                     const float2 *slices, const float *t3d, const float *pw) {
+  InsertJob J = make_job(r, slices, t3d, pw, np);
   const int tile = job_tile(r, tile_pref);
   if (tile != kTunedScatter && r->tiles_tile != tile) {
     if (is_column(tile))
@@ -175,6 +195,27 @@ static void plan_add(RoundPlan &P, fr_recon *r, int owner, int np, int tile_pref
   P.jt.push_back(tile);
 }
 
+// Appends the (job, slice) units of group g's jobs to the work buffer: every
+// slice for a scatter group, every slice of a job with rim pixels for the
+// face taps that follow a gather launch.
+static void plan_units(RoundPlan &P, RoundGroup &g, bool edge) {
+  std::vector<int2> u;
+  int mx = 0;
+  for (size_t k = 0; k < P.hj.size(); k++) {
+    if (P.jt[k] != g.tile) continue;
+    const InsertJob &J = P.hj[k];
+    const int px = edge ? J.nrim : J.N * (J.N / 2 + 1);
+    if (px == 0) continue;
+    mx = std::max(mx, px);
+    for (int s = 0; s < J.np * J.nsym; s++) u.push_back(make_int2((int)k, s));
+  }
+  g.units_off = (P.work.size() + 15) & ~(size_t)15;
+  g.nunits = u.size();
+  g.max_px = mx;
+  P.work.resize(g.units_off + sizeof(int2) * u.size());
+  if (!u.empty()) memcpy(&P.work[g.units_off], u.data(), sizeof(int2) * u.size());
+}
+
 // Builds each schedule group's work list.  Column items run slice-bucket-major
 // (slice_bucket per job, so the CTAs in flight share a bucket's slices in L2)
 // and within a bucket by estimated cost, heaviest first: the slices meeting a
@@ -187,7 +228,11 @@ static void plan_groups(const std::vector<fr_recon *> &jobs, RoundPlan &P) {
   for (const int tile : tiles_used) {
     RoundGroup g;
     g.tile = tile;
-    if (tile == kTunedScatter) { P.groups.push_back(g); continue; }
+    if (tile == kTunedScatter) {
+      plan_units(P, g, false);
+      P.groups.push_back(g);
+      continue;
+    }
     const bool column = is_column(tile);
     std::vector<std::pair<double, int4>> items;
     for (size_t k = 0; k < P.hj.size(); k++) {
@@ -230,6 +275,7 @@ static void plan_groups(const std::vector<fr_recon *> &jobs, RoundPlan &P) {
         memcpy(&P.work[g.off + i * isz], &w2, isz);
       }
     }
+    plan_units(P, g, true);
     P.groups.push_back(g);
   }
 }
@@ -250,9 +296,9 @@ static int plan_upload(const RoundPlan &P, BatchScratch &bs, cudaStream_t st) {
 static int plan_launch(const RoundPlan &P, BatchScratch &bs, cudaStream_t st) {
   const InsertJob *d_jobs = bs.d_jobs.as<InsertJob>();
   for (const RoundGroup &g : P.groups) {
+    const int2 *units = (const int2 *)((const unsigned char *)bs.d_work.p + g.units_off);
     if (g.tile == kTunedScatter) {
-      for (size_t k = 0; k < P.hj.size(); k++)
-        if (P.jt[k] == g.tile) TRY(run_scatter(P.hj[k], false, st));
+      CU(launch_scatter_multi(d_jobs, units, (int)g.nunits, g.max_px, false, st));
       continue;
     }
     const void *w = (const unsigned char *)bs.d_work.p + g.off;
@@ -268,15 +314,106 @@ static int plan_launch(const RoundPlan &P, BatchScratch &bs, cudaStream_t st) {
     else
       CU(launch_gather(d_jobs, P.hj.data(), (int)P.hj.size(), (const int2 *)w, (int)g.nwork,
                        g.tile, bs.d_counter.as<int>(), g.max_mode, st));
-    for (size_t k = 0; k < P.hj.size(); k++)
-      if (P.jt[k] == g.tile) TRY(run_scatter(P.hj[k], true, st));
+    CU(launch_scatter_multi(d_jobs, units, (int)g.nunits, g.max_px, true, st));
   }
   return FR_OK;
 }
 
-// Inserts, for every job, counts[j] particles through the caller pipeline;
-// all jobs' insertion work goes through one persistent launch per schedule
-// per round.  Every job runs on `st` for the duration of the call.
+// ------------------------------------------------------------ prologue groups
+// Jobs of a round that share (N, box, symmetry operators) run ONE prologue
+// over their concatenated particles, so each prologue stage is one launch
+// (or one batched FFT) per group rather than per job.  A group's metadata
+// block is the prologue_meta layout for all its particles, then a table of
+// their raw image addresses, so the jobs' images need not be contiguous.
+struct ProGroup {
+  int N = 0, box = 0, nsym = 1, n = 0;
+  bool ctf = false;                     // the group runs the CTF round trip
+  fr_recon *lead = nullptr;             // its FFT plans and symmetry operators serve the group
+  std::vector<int> jobs, first, count;  // job indices, first particle and count of each
+  size_t meta_off = 0;                  // the group's block in the round's block
+};
+
+static size_t align16(size_t b) { return (b + 15) & ~(size_t)15; }
+static size_t group_meta_bytes(int n) {
+  return align16(prologue_meta_bytes(n)) + sizeof(float *) * (size_t)n;
+}
+
+// Groups the jobs with counts[j] > 0 (in job order); returns the bytes of
+// the round's metadata block.
+static size_t make_groups(const std::vector<fr_recon *> &jobs, const int *counts,
+                          const int *boxes, std::vector<ProGroup> &G) {
+  G.clear();
+  for (int j = 0; j < (int)jobs.size(); j++) {
+    if (counts[j] <= 0) continue;
+    fr_recon *r = jobs[j];
+    ProGroup *g = nullptr;
+    for (ProGroup &q : G)
+      if (q.N == r->N && q.box == boxes[j] && q.nsym == r->nsym && q.lead->syms == r->syms) {
+        g = &q;
+        break;
+      }
+    if (!g) {
+      G.emplace_back();
+      g = &G.back();
+      g->N = r->N;
+      g->box = boxes[j];
+      g->nsym = r->nsym;
+      g->lead = r;
+    }
+    g->jobs.push_back(j);
+    g->first.push_back(g->n);
+    g->count.push_back(counts[j]);
+    g->n += counts[j];
+  }
+  size_t off = 0;
+  for (ProGroup &g : G) {
+    g.meta_off = off;
+    off += align16(group_meta_bytes(g.n));
+  }
+  return off;
+}
+
+// Writes group g's block at blk: each job's particle metadata meta[j], then
+// particle i of job j's raw image address src[j] + i * box^2.  Returns
+// whether any particle carries a CTF.
+static bool group_meta(const ProGroup &g, const fr_particle *const *meta,
+                       const float *const *src, unsigned char *blk) {
+  bool any = false;
+  const float **tab = reinterpret_cast<const float **>(blk + align16(prologue_meta_bytes(g.n)));
+  const size_t img = (size_t)g.box * g.box;
+  for (size_t k = 0; k < g.jobs.size(); k++) {
+    const int j = g.jobs[k];
+    any |= prologue_meta_range(g.N, g.n, g.first[k], g.count[k], meta[j], blk);
+    for (int i = 0; i < g.count[k]; i++) tab[g.first[k] + i] = src[j] + (size_t)i * img;
+  }
+  return any;
+}
+
+// The device half of group g's prologue (block at d_blk, scratch b) on st;
+// with P, its jobs' InsertJobs (their parts of the group's slices, rotations
+// and weights) join the plan.
+static int group_run(const std::vector<fr_recon *> &jobs, const ProGroup &g, ProBufs &b,
+                     const unsigned char *d_blk, RoundPlan *P, int tile_pref, cudaStream_t st,
+                     bool exact_fft = false) {
+  const float *const *tab =
+      reinterpret_cast<const float *const *>(d_blk + align16(prologue_meta_bytes(g.n)));
+  TRY(prologue_run(g.lead->plans, b.view(), d_blk, nullptr, tab, g.n, g.box, g.N,
+                   g.lead->d_sym.as<float>(), g.nsym, g.ctf, st, exact_fft));
+  if (!P) return FR_OK;
+  const MetaView mv = meta_view(d_blk, g.n);
+  const size_t sl = (size_t)g.N * (g.N / 2 + 1);
+  for (size_t k = 0; k < g.jobs.size(); k++) {
+    const int j = g.jobs[k], f = g.first[k];
+    plan_add(*P, jobs[j], j, g.count[k], tile_pref, b.slices.as<float2>() + (size_t)f * sl,
+             b.t3d.as<float>() + (size_t)f * g.nsym * 9, mv.w + f);
+  }
+  return FR_OK;
+}
+
+// Inserts, for every job, counts[j] particles through the caller pipeline:
+// per round one prologue per group of jobs of equal (N, box, symmetry), and
+// all jobs' insertion work in one persistent launch per schedule.  Every
+// job runs on `st` for the duration of the call.
 static int batch_insert(std::vector<fr_recon *> &jobs, BatchScratch &bs, int tile_pref,
                         cudaStream_t st, const float *const *imgs, const int *boxes,
                         const int *counts, const fr_particle *const *meta) {
@@ -306,27 +443,42 @@ static int batch_insert(std::vector<fr_recon *> &jobs, BatchScratch &bs, int til
   int rounds = 0;
   for (int j = 0; j < nj; j++) rounds = std::max(rounds, (counts[j] + chunk - 1) / chunk);
   for (int rd = 0; rd < rounds; rd++) {
-    RoundPlan P;
+    std::vector<int> c(nj, 0);
+    std::vector<const float *> src(nj, nullptr);
+    std::vector<const fr_particle *> m(nj, nullptr);
+    const int p0 = rd * chunk;
     for (int j = 0; j < nj; j++) {
-      fr_recon *r = jobs[j];
-      const int p0 = rd * chunk;
-      const int c = std::max(0, std::min(chunk, counts[j] - p0));
-      if (c == 0) continue;
+      c[j] = std::max(0, std::min(chunk, counts[j] - p0));
+      if (c[j] == 0) continue;
       const int box = boxes[j];
       const void *d_raw = nullptr;
-      TRY(to_device(imgs[j] + (size_t)p0 * box * box, sizeof(float) * (size_t)c * box * box,
-                    r->s_in, st, &d_raw));
-      TRY(prologue_chunk(r, (const float *)d_raw, c, box, meta[j] + p0));
-      plan_add(P, r, j, c, tile_pref);
+      TRY(to_device(imgs[j] + (size_t)p0 * box * box, sizeof(float) * (size_t)c[j] * box * box,
+                    jobs[j]->s_in, st, &d_raw));
+      src[j] = (const float *)d_raw;
+      m[j] = meta[j] + p0;
     }
-    if (P.hj.empty()) continue;
+    std::vector<ProGroup> G;
+    const size_t bytes = make_groups(jobs, c.data(), boxes, G);
+    if (G.empty()) continue;
+    int slot;
+    unsigned char *blk;
+    TRY(bs.ring.acquire(bytes, &slot, &blk));
+    for (ProGroup &g : G) g.ctf = group_meta(g, m.data(), src.data(), blk + g.meta_off);
+    TRY(bs.d_meta.ensure(bytes));
+    CU(cudaMemcpyAsync(bs.d_meta.p, blk, bytes, cudaMemcpyHostToDevice, st));
+    TRY(bs.ring.done(slot, st));
+    if (bs.gbufs.size() < G.size()) bs.gbufs.resize(G.size());
+    RoundPlan P;
+    for (size_t gi = 0; gi < G.size(); gi++)
+      TRY(group_run(jobs, G[gi], bs.gbufs[gi], bs.d_meta.as<unsigned char>() + G[gi].meta_off, &P,
+                    tile_pref, st));
     plan_groups(jobs, P);
     TRY(plan_upload(P, bs, st));
     TRY(plan_launch(P, bs, st));
   }
   CU(cudaEventRecord(bs.done, st));
   bs.last = st;
-  for (int j = 0; j < nj; j++) TRY(stream_leave(jobs[j], st));
+  TRY(stream_leave_all(jobs, st));
   if (host_src) CU(cudaStreamSynchronize(st));   // host images may be pinned: read them before returning
   return FR_OK;
 }
@@ -360,42 +512,30 @@ int fr_insert_particles_multi(fr_recon *const *handles, int nh, const float *con
 
 // ------------------------------------------------------------------ graphs
 // A batched insertion round of fixed shapes captured once as a CUDA graph.
-// The graph owns the images' device slots and every job's chunk scratch (so
-// later calls on the same handles cannot move them); a replay writes the
-// particles' metadata into pinned staging, copies it and the images in, and
-// launches the graph.
+// The graph owns the device slots for host images and every prologue
+// group's scratch (so later calls on the same handles cannot move them); a
+// replay writes the particles' metadata and image addresses into pinned
+// staging, copies that one block (and any host images) in, and launches the
+// graph.  Device images are read in place.
 }  // extern "C"
-
-namespace fr {
-struct JobBufs {
-  DevBuf img, slices, mean, spec, t3d, img2, meta;
-  void swap_with(fr_recon *r) {
-    std::swap(img, r->s_img);
-    std::swap(slices, r->s_slices);
-    std::swap(mean, r->s_mean);
-    std::swap(spec, r->s_spec);
-    std::swap(t3d, r->s_t3d);
-    std::swap(img2, r->s_img2);
-    std::swap(meta, r->s_meta);
-  }
-  void release() {
-    for (DevBuf *b : {&img, &slices, &mean, &spec, &t3d, &img2, &meta}) b->release();
-  }
-};
-}  // namespace fr
 
 struct fr_graph {
   std::vector<fr_recon *> jobs;
   cudaStream_t st = nullptr;
-  std::vector<int> boxes, counts, ctf;
-  std::vector<fr::DevBuf> slots;
-  std::vector<fr::JobBufs> bufs;
-  std::vector<size_t> meta_off;
+  std::vector<int> boxes, counts;
+  std::vector<fr::DevBuf> slots;        // device images of host sources (and the caller's own)
+  std::vector<fr::ProGroup> groups;     // prologue groups, fixed at capture
+  std::vector<fr::ProBufs> gbufs;
+  fr::DevBuf d_meta;                    // the round's metadata block
   size_t meta_bytes = 0;
   unsigned char *pinned[2] = {nullptr, nullptr};
   cudaEvent_t staged[2] = {nullptr, nullptr};
   bool staged_used[2] = {false, false};
   int next = 0;
+  // The groups' prologues are captured as parallel branches on side streams.
+  static constexpr int kSide = 8;
+  cudaStream_t side[kSide] = {};
+  cudaEvent_t fork = nullptr, join[kSide] = {};
   long long kernels = 0;          // this library's kernels per replay
   fr::BatchScratch bs;
   fr::RoundPlan plan;
@@ -411,15 +551,41 @@ static void graph_free(fr_graph *g) {
   if (g->exec) cudaGraphExecDestroy(g->exec);
   if (g->graph) cudaGraphDestroy(g->graph);
   for (auto &s : g->slots) s.release();
-  for (auto &jb : g->bufs) jb.release();
-  g->bs.d_jobs.release();
-  g->bs.d_work.release();
-  g->bs.d_counter.release();
+  for (auto &b : g->gbufs) b.release();
+  g->d_meta.release();
+  g->bs.release();
   for (int k = 0; k < 2; k++) {
     if (g->pinned[k]) cudaFreeHost(g->pinned[k]);
     if (g->staged[k]) cudaEventDestroy(g->staged[k]);
   }
+  for (int k = 0; k < fr_graph::kSide; k++) {
+    if (g->side[k]) cudaStreamDestroy(g->side[k]);
+    if (g->join[k]) cudaEventDestroy(g->join[k]);
+  }
+  if (g->fork) cudaEventDestroy(g->fork);
   delete g;
+}
+
+// The graph's device work: the groups' prologues (parallel branches when
+// there are several), then the round's insertion launches on st.
+static int graph_device_work(fr_graph *g, cudaStream_t st) {
+  const int ng = (int)g->groups.size();
+  const int nside = std::min(ng, (int)fr_graph::kSide);
+  if (ng > 1) {
+    CU(cudaEventRecord(g->fork, st));
+    for (int k = 0; k < nside; k++) CU(cudaStreamWaitEvent(g->side[k], g->fork, 0));
+  }
+  for (int gi = 0; gi < ng; gi++) {
+    cudaStream_t s = ng > 1 ? g->side[gi % fr_graph::kSide] : st;
+    TRY(group_run(g->jobs, g->groups[gi], g->gbufs[gi],
+                  g->d_meta.as<unsigned char>() + g->groups[gi].meta_off, nullptr, -1, s, true));
+  }
+  if (ng > 1)
+    for (int k = 0; k < nside; k++) {
+      CU(cudaEventRecord(g->join[k], g->side[k]));
+      CU(cudaStreamWaitEvent(st, g->join[k], 0));
+    }
+  return plan_launch(g->plan, g->bs, st);
 }
 
 static int graph_create(const std::vector<fr_recon *> &jobs, cudaStream_t st, int tile_pref,
@@ -439,26 +605,33 @@ static int graph_create(const std::vector<fr_recon *> &jobs, cudaStream_t st, in
   g->st = st;
   g->boxes.assign(boxes, boxes + nj);
   g->counts.assign(counts, counts + nj);
-  g->ctf.assign(nj, 0);
-  for (int j = 0; ctf && j < nj; j++) g->ctf[j] = ctf[j] ? 1 : 0;
   g->slots.resize(nj);
-  g->bufs.resize(nj);
-  g->meta_off.assign(nj, 0);
-  for (int j = 0; j < nj; j++) {
-    g->meta_off[j] = g->meta_bytes;
-    g->meta_bytes += (prologue_meta_bytes(counts[j]) + 15) & ~(size_t)15;
-  }
-  std::vector<cudaStream_t> saved;
-  for (fr_recon *r : jobs) { saved.push_back(r->stream); r->stream = st; }
-  // Sizing pass on the graph-owned scratch (swapped into the handles): a
-  // prologue of weight-0 particles allocates every buffer and FFT plan the
-  // capture uses, so the captured work allocates nothing.
-  for (int j = 0; j < nj; j++) g->bufs[j].swap_with(jobs[j]);
+  g->meta_bytes = make_groups(jobs, counts, boxes, g->groups);
+  g->gbufs.resize(g->groups.size());
+  // a group runs the CTF round trip when any of its jobs was captured with one
+  for (ProGroup &q : g->groups)
+    for (int j : q.jobs) q.ctf = q.ctf || (ctf && ctf[j]);
   int rc = FR_OK;
+  for (int k = 0; k < 2 && rc == FR_OK; k++)
+    if (cudaHostAlloc((void **)&g->pinned[k], std::max<size_t>(16, g->meta_bytes),
+                      cudaHostAllocDefault) != cudaSuccess ||
+        cudaEventCreateWithFlags(&g->staged[k], cudaEventDisableTiming) != cudaSuccess)
+      rc = fail(FR_ENOMEM, "pinned staging allocation failed");
+  for (int k = 0; k < fr_graph::kSide && rc == FR_OK; k++)
+    if (cudaStreamCreateWithFlags(&g->side[k], cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&g->join[k], cudaEventDisableTiming) != cudaSuccess)
+      rc = fail(FR_ECUDA, "stream creation failed");
+  if (rc == FR_OK && cudaEventCreateWithFlags(&g->fork, cudaEventDisableTiming) != cudaSuccess)
+    rc = fail(FR_ECUDA, "cudaEventCreate failed");
+  if (rc == FR_OK) rc = g->d_meta.ensure(std::max<size_t>(16, g->meta_bytes));
   for (int j = 0; j < nj && rc == FR_OK; j++) rc = stream_enter(jobs[j], st);
-  std::vector<unsigned char> blk(std::max<size_t>(16, g->meta_bytes));
+  // Sizing pass: a prologue of weight-0 particles read from the zeroed slots
+  // allocates every buffer and FFT plan the capture uses, so the captured
+  // work allocates nothing.
+  std::vector<std::vector<fr_particle>> zero(nj);
+  std::vector<const fr_particle *> zmeta(nj, nullptr);
+  std::vector<const float *> src(nj, nullptr);
   for (int j = 0; j < nj && rc == FR_OK; j++) {
-    fr_recon *r = jobs[j];
     const int n = counts[j];
     if (n == 0) continue;
     const size_t bytes = sizeof(float) * (size_t)n * boxes[j] * boxes[j];
@@ -467,21 +640,32 @@ static int graph_create(const std::vector<fr_recon *> &jobs, cudaStream_t st, in
       rc = fail(FR_ECUDA, "memset failed");
       break;
     }
-    std::vector<fr_particle> parts(n);
-    for (fr_particle &m : parts) {
+    src[j] = g->slots[j].as<float>();
+    zero[j].resize(n);
+    for (fr_particle &m : zero[j]) {
       memset(&m, 0, sizeof m);
       m.rot[0] = m.rot[4] = m.rot[8] = 1.0f;
-      m.defocus = g->ctf[j] ? 1.5f : 0.0f;
+      m.defocus = (ctf && ctf[j]) ? 1.5f : 0.0f;
       m.voltage = 300.0f;
       m.cs = 2.7f;
       m.apix = 1.0f;
       m.ampcont = 10.0f;
     }
-    prologue_meta(r->N, n, parts.data(), blk.data() + g->meta_off[j]);
-    if ((rc = prologue_upload(r, n, blk.data() + g->meta_off[j], st)) != FR_OK) break;
-    if ((rc = prologue_device(r, g->slots[j].as<float>(), n, boxes[j], g->ctf[j])) != FR_OK) break;
-    plan_add(g->plan, r, j, n, tile_pref);
+    zmeta[j] = zero[j].data();
   }
+  if (rc == FR_OK) {
+    std::vector<unsigned char> blk(std::max<size_t>(16, g->meta_bytes));
+    for (const ProGroup &q : g->groups) group_meta(q, zmeta.data(), src.data(), blk.data() + q.meta_off);
+    if (cudaMemcpyAsync(g->d_meta.p, blk.data(), g->meta_bytes, cudaMemcpyHostToDevice, st) !=
+        cudaSuccess)
+      rc = fail(FR_ECUDA, "metadata upload failed");
+    if (rc == FR_OK && cudaStreamSynchronize(st) != cudaSuccess)   // blk is pageable
+      rc = fail(FR_ECUDA, "metadata upload failed");
+  }
+  for (size_t gi = 0; gi < g->groups.size() && rc == FR_OK; gi++)
+    rc = group_run(jobs, g->groups[gi], g->gbufs[gi],
+                   g->d_meta.as<unsigned char>() + g->groups[gi].meta_off, &g->plan, tile_pref, st,
+                   true);
   if (rc == FR_OK) {
     plan_groups(jobs, g->plan);
     rc = plan_upload(g->plan, g->bs, st);
@@ -494,12 +678,7 @@ static int graph_create(const std::vector<fr_recon *> &jobs, cudaStream_t st, in
       rc = fail(FR_ECUDA, "cudaStreamBeginCapture failed");
     } else {
       const long long noted = launches_noted();
-      for (int j = 0; j < nj && rc == FR_OK; j++)
-        if (counts[j] > 0) {
-          jobs[j]->d_meta = jobs[j]->s_meta.as<unsigned char>();   // the graph's block
-          rc = prologue_device(jobs[j], g->slots[j].as<float>(), counts[j], boxes[j], g->ctf[j]);
-        }
-      if (rc == FR_OK) rc = plan_launch(g->plan, g->bs, st);
+      rc = graph_device_work(g, st);
       const cudaError_t e = cudaStreamEndCapture(st, &g->graph);
       if (rc == FR_OK && e != cudaSuccess)
         rc = fail(FR_ECUDA, "stream capture failed: %s", cudaGetErrorString(e));
@@ -508,19 +687,10 @@ static int graph_create(const std::vector<fr_recon *> &jobs, cudaStream_t st, in
   }
   if (rc == FR_OK && cudaGraphInstantiate(&g->exec, g->graph, 0) != cudaSuccess)
     rc = fail(FR_ECUDA, "cudaGraphInstantiate failed: %s", cudaGetErrorString(cudaGetLastError()));
-  for (int j = 0; j < nj; j++) g->bufs[j].swap_with(jobs[j]);
-  for (int k = 0; k < 2 && rc == FR_OK; k++) {
-    if (cudaHostAlloc((void **)&g->pinned[k], std::max<size_t>(16, g->meta_bytes),
-                      cudaHostAllocDefault) != cudaSuccess ||
-        cudaEventCreateWithFlags(&g->staged[k], cudaEventDisableTiming) != cudaSuccess)
-      rc = fail(FR_ENOMEM, "pinned staging allocation failed");
-  }
-  for (int j = 0; j < nj; j++) {
-    stream_leave(jobs[j], st);
-    jobs[j]->stream = saved[j];
-  }
+  stream_leave_all(jobs, st);
   if (rc != FR_OK) {
     cudaGetLastError();
+    cudaStreamSynchronize(st);
     graph_free(g);
     return rc;
   }
@@ -570,40 +740,41 @@ int fr_graph_launch(fr_graph *g, const float *const *imgs, const fr_particle *co
   for (fr_recon *r : g->jobs) TRY(check_state(r));
   cudaStream_t st = g->st;
   const int nj = (int)g->counts.size();
-  const int k = g->next;
-  // this staging block was last read by the copies two replays ago
-  if (g->staged_used[k]) CU(cudaEventSynchronize(g->staged[k]));
+  // particle sources: device images in place, host images through the slots
+  std::vector<const float *> src(nj, nullptr);
+  bool host_src = false;
   for (int j = 0; j < nj; j++) {
-    const int n = g->counts[j];
-    if (n == 0) continue;
+    if (g->counts[j] == 0) continue;
     if (!meta[j]) return fail(FR_ENULL, "job %d: null metadata", j);
     if (imgs && !imgs[j]) return fail(FR_ENULL, "job %d: null images", j);
-    const bool any = prologue_meta(g->jobs[j]->N, n, meta[j], g->pinned[k] + g->meta_off[j]);
-    if ((int)any != g->ctf[j])
-      return fail(FR_EINVAL_PARAM, "job %d: the graph was captured %s a CTF phase flip", j,
-                  g->ctf[j] ? "with" : "without");
+    const bool in_place = imgs && is_device_ptr(imgs[j]);
+    src[j] = in_place ? imgs[j] : g->slots[j].as<float>();
+    host_src |= imgs && !in_place;
+  }
+  const int k = g->next;
+  // this staging block was last read by the copy two replays ago
+  if (g->staged_used[k]) CU(cudaEventSynchronize(g->staged[k]));
+  for (const ProGroup &q : g->groups) {
+    const bool any = group_meta(q, meta, src.data(), g->pinned[k] + q.meta_off);
+    if (any && !q.ctf)
+      return fail(FR_EINVAL_PARAM,
+                  "jobs of box %d (N %d) carry a CTF but were captured without the phase flip",
+                  q.box, q.N);
   }
   g->next ^= 1;
   for (fr_recon *r : g->jobs) TRY(stream_enter(r, st));
-  bool host_src = false;
-  for (int j = 0; j < nj; j++) {
-    const int n = g->counts[j];
-    if (n == 0) continue;
-    CU(cudaMemcpyAsync(g->bufs[j].meta.p, g->pinned[k] + g->meta_off[j], prologue_meta_bytes(n),
-                       cudaMemcpyHostToDevice, st));
-  }
+  CU(cudaMemcpyAsync(g->d_meta.p, g->pinned[k], g->meta_bytes, cudaMemcpyHostToDevice, st));
   CU(cudaEventRecord(g->staged[k], st));
   g->staged_used[k] = true;
-  for (int j = 0; imgs && j < nj; j++) {
+  for (int j = 0; host_src && j < nj; j++) {
     const int n = g->counts[j];
-    if (n == 0 || imgs[j] == g->slots[j].as<float>()) continue;
+    if (n == 0 || is_device_ptr(imgs[j])) continue;
     const size_t bytes = sizeof(float) * (size_t)n * g->boxes[j] * g->boxes[j];
-    host_src |= !is_device_ptr(imgs[j]);
-    CU(cudaMemcpyAsync(g->slots[j].p, imgs[j], bytes, cudaMemcpyDefault, st));
+    CU(cudaMemcpyAsync(g->slots[j].p, imgs[j], bytes, cudaMemcpyHostToDevice, st));
   }
   CU(cudaGraphLaunch(g->exec, st));
   note_launch((int)g->kernels);
-  for (fr_recon *r : g->jobs) TRY(stream_leave(r, st));
+  TRY(stream_leave_all(g->jobs, st));
   if (host_src) CU(cudaStreamSynchronize(st));   // host images may be pinned: read them first
   return FR_OK;
 }

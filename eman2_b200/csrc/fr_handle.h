@@ -4,6 +4,7 @@
 #include <cufft.h>
 
 #include <map>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -128,6 +129,16 @@ struct PinnedRing {
   }
 };
 
+// An event marking the end of a handle's last work.  A call over many
+// handles on one stream records ONE event and shares it among them; a handle
+// that leaves alone on another stream gets a fresh event of its own.
+struct SharedEvent {
+  cudaEvent_t ev = nullptr;
+  ~SharedEvent() {
+    if (ev) cudaEventDestroy(ev);
+  }
+};
+
 bool is_device_ptr(const void *p);
 int to_device(const void *src, size_t bytes, DevBuf &stage, cudaStream_t st, const void **out);
 int from_device(void *dst, const void *dsrc, size_t bytes, cudaStream_t st);
@@ -175,12 +186,16 @@ struct PlanCache {
   // n batched 2-D transforms of size N (contiguous, unpadded) run as a
   // binary decomposition into power-of-two batches (at most 1024), so the
   // plans are shared by every chunk length instead of one plan per length.
-  int exec2d(bool forward, int N, int n, const void *in, void *out, cudaStream_t st) {
+  // exact: one plan of batch n (a captured graph's fixed shapes: one launch
+  // sequence instead of one per power of two).
+  int exec2d(bool forward, int N, int n, const void *in, void *out, cudaStream_t st,
+             bool exact = false) {
     const size_t img = (size_t)N * N, spec = (size_t)N * (N / 2 + 1);
     int done = 0;
     while (done < n) {
       int b = 1;
-      while (2 * b <= n - done && 2 * b <= 1024) b *= 2;
+      if (exact) b = n;
+      else while (2 * b <= n - done && 2 * b <= 1024) b *= 2;
       cufftHandle h;
       int rc = get2d(forward, N, b, st, &h);
       if (rc != FR_OK) return rc;
@@ -244,7 +259,7 @@ struct fr_recon {
   // Insertion calls return once their work is enqueued.  `done` is recorded
   // after the handle's last enqueued work on stream `last`; a call on another
   // stream first makes that stream wait for it.
-  cudaEvent_t done = nullptr;
+  std::shared_ptr<fr::SharedEvent> done;
   cudaStream_t last = nullptr;
   // Host particle chunks go through two device staging buffers filled on a
   // copy stream: the upload of one chunk overlaps the work on the one before.
@@ -273,6 +288,8 @@ int check_state(fr_recon *r);
 int stream_enter(fr_recon *r, cudaStream_t st);
 // Marks the end of the handle's work enqueued so far on st.
 int stream_leave(fr_recon *r, cudaStream_t st);
+// The same for many handles whose work went to st: one event for all.
+int stream_leave_all(const std::vector<fr_recon *> &rs, cudaStream_t st);
 InsertJob make_job(fr_recon *r, const float2 *slices, const float *t3d, const float *pw, int np);
 int run_scatter(const InsertJob &j0, bool edge_only, cudaStream_t st);
 int insert_device(fr_recon *r, const float2 *d_slices, const float *d_t3d, const float *d_pw, int np,
@@ -285,6 +302,9 @@ int prologue_chunk(fr_recon *r, const float *d_raw, int n, int box, const fr_par
 // Its halves: metadata block on the host, upload, device work only.
 size_t prologue_meta_bytes(int n);
 bool prologue_meta(int N, int n, const fr_particle *meta, unsigned char *blk);
+// Entries [first, first + count) of the block of n particles.
+bool prologue_meta_range(int N, int n, int first, int count, const fr_particle *meta,
+                         unsigned char *blk);
 int prologue_upload(fr_recon *r, int n, const unsigned char *blk, cudaStream_t st);
 // The arrays of a metadata block of n particles (prologue_meta's layout).
 struct MetaView {
@@ -292,6 +312,19 @@ struct MetaView {
   const float *txy, *w, *rot;
 };
 MetaView meta_view(const unsigned char *d_meta, int n);
+// Scratch of one prologue run: padded images, spectra (and the r2c input),
+// the CTF round trip's images, edge means, slices, composed rotations.
+struct ProScratch {
+  DevBuf *img, *slices, *mean, *spec, *t3d, *img2;
+};
+// The device half of a prologue over n particles of size box into slices of
+// size N: metadata block (prologue_meta layout) at d_meta, raw images at
+// d_raw (contiguous) or through d_src (a device table of per-particle
+// pointers).  Kernels and FFTs only once the scratch and plans exist.
+int prologue_run(PlanCache &plans, const ProScratch &b, const unsigned char *d_meta,
+                 const float *d_raw, const float *const *d_src, int n, int box, int N,
+                 const float *d_sym, int nsym, bool any_ctf, cudaStream_t st,
+                 bool exact_fft = false);
 int prologue_device(fr_recon *r, const float *d_raw, int n, int box, bool any_ctf);
 int particles_chunk(fr_recon *r, const float *d_raw, int n, int box, const fr_particle *meta,
                     int schedule);

@@ -227,16 +227,15 @@ cudaError_t zero_counter(int *d_counter, cudaStream_t st) {
   return cudaGetLastError();
 }
 
-// grid.x covers the N*(N/2+1) pixel grid, grid.y = slice (particle*nsym+sym).
+// One pixel of slice s (particle*nsym+sym) of job J, scattered with atomics.
+// pix indexes the N*(N/2+1) pixel grid.
 template <int MODE>
-__global__ void __launch_bounds__(256) k_scatter(InsertJob J, const float *__restrict__ table,
-                                                 float h) {
+__device__ __forceinline__ void scatter_pixel(const InsertJob &J, int s, int pix,
+                                              const float *__restrict__ table, float h) {
   const int N = J.N, n2 = N >> 1, w2 = n2 + 1;
-  const int s = blockIdx.y;
   const int p = s / J.nsym;
   const float w = J.pw[p];
   if (w == 0.0f) return;
-  const int pix = blockIdx.x * blockDim.x + threadIdx.x;
   if (pix >= N * w2) return;
   const int x = pix % w2, y = pix / w2 - n2;
   if (x > __ldg(&J.xmax[y + n2])) return;
@@ -257,14 +256,13 @@ __global__ void __launch_bounds__(256) k_scatter(InsertJob J, const float *__res
   insert_pixel_atomic<MODE>(J.data, J.norm, N, xx, yy, zz, v.x, v.y, pw, h, table, false);
 }
 
-// The iterative reconstructor's insertion: one thread per pixel of its disk.
-__global__ void __launch_bounds__(256) k_scatter_iter(InsertJob J, const float *__restrict__ table) {
+// The iterative reconstructor's insertion of one pixel of its disk.
+__device__ __forceinline__ void scatter_pixel_iter(const InsertJob &J, int s, int pix,
+                                                   const float *__restrict__ table) {
   const int N = J.N, n2 = N >> 1, w2 = n2 + 1;
-  const int s = blockIdx.y;
   const int p = s / J.nsym;
   const float w = J.pw[p];
   if (w == 0.0f) return;
-  const int pix = blockIdx.x * blockDim.x + threadIdx.x;
   if (pix >= N * w2) return;
   const int x = pix % w2, y = pix / w2 - n2;
   if (x > __ldg(&J.xmax[y + n2])) return;
@@ -277,16 +275,14 @@ __global__ void __launch_bounds__(256) k_scatter_iter(InsertJob J, const float *
   insert_pixel_iter(J, xx, yy, zz, v.x, v.y, w, table);
 }
 
-// Face taps of rim pixels: grid.x covers the rim list, grid.y = slice.
+// Face taps of rim pixel r (index into J.rim) of slice s.
 template <int MODE>
-__global__ void __launch_bounds__(128) k_edge(InsertJob J, const float *__restrict__ table,
-                                              float h) {
+__device__ __forceinline__ void edge_pixel(const InsertJob &J, int s, int r,
+                                           const float *__restrict__ table, float h) {
   const int N = J.N, n2 = N >> 1, w2 = n2 + 1;
-  const int s = blockIdx.y;
   const int p = s / J.nsym;
   const float w = J.pw[p];
   if (w == 0.0f) return;
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= J.nrim) return;
   const int code = __ldg(&J.rim[r]);
   const int x = code & 0xFFFF, y = (code >> 16) - n2;
@@ -298,6 +294,58 @@ __global__ void __launch_bounds__(128) k_edge(InsertJob J, const float *__restri
   const float2 v = slice_value(J.slices + (size_t)p * N * w2, N, x, y);
   insert_pixel_atomic<MODE>(J.data, J.norm, N, xx, yy, zz, v.x, v.y, pixel_weight(J, p, x, y, w),
                             h, table, true);
+}
+
+// grid.x covers the N*(N/2+1) pixel grid, grid.y = slice (particle*nsym+sym).
+template <int MODE>
+__global__ void __launch_bounds__(256) k_scatter(InsertJob J, const float *__restrict__ table,
+                                                 float h) {
+  scatter_pixel<MODE>(J, blockIdx.y, blockIdx.x * blockDim.x + threadIdx.x, table, h);
+}
+
+__global__ void __launch_bounds__(256) k_scatter_iter(InsertJob J, const float *__restrict__ table) {
+  scatter_pixel_iter(J, blockIdx.y, blockIdx.x * blockDim.x + threadIdx.x, table);
+}
+
+// Face taps of rim pixels: grid.x covers the rim list, grid.y = slice.
+template <int MODE>
+__global__ void __launch_bounds__(128) k_edge(InsertJob J, const float *__restrict__ table,
+                                              float h) {
+  edge_pixel<MODE>(J, blockIdx.y, blockIdx.x * blockDim.x + threadIdx.x, table, h);
+}
+
+// Several jobs' scatter (or face taps) in one launch: grid.x = unit
+// (job, slice); the grid.y blocks of a unit stride over its job's pixel grid
+// (or rim list).  A slice of weight 0 costs one check per block.
+__global__ void __launch_bounds__(256) k_scatter_multi(const InsertJob *__restrict__ jobs,
+                                                       const int2 *__restrict__ units,
+                                                       const float *__restrict__ table, float h2,
+                                                       float h5, int edge) {
+  const int2 u = units[blockIdx.x];
+  const InsertJob &J = jobs[u.x];
+  if (J.pw[u.y / J.nsym] == 0.0f) return;
+  const int mode = J.mode;
+  const int npx = edge ? J.nrim : J.N * (J.N / 2 + 1);
+  for (int i = blockIdx.y * blockDim.x + threadIdx.x; i < npx; i += gridDim.y * blockDim.x) {
+    if (edge) {
+      switch (mode) {
+        case MODE_NEAREST: edge_pixel<MODE_NEAREST>(J, u.y, i, table, h2); break;
+        case MODE_GAUSS2: edge_pixel<MODE_GAUSS2>(J, u.y, i, table, h2); break;
+        case MODE_GAUSS5: edge_pixel<MODE_GAUSS5>(J, u.y, i, table, h5); break;
+        case MODE_TRILINEAR: edge_pixel<MODE_TRILINEAR>(J, u.y, i, table, h2); break;
+        default: break;
+      }
+      continue;
+    }
+    switch (mode) {
+      case MODE_NEAREST: scatter_pixel<MODE_NEAREST>(J, u.y, i, table, h2); break;
+      case MODE_GAUSS2: scatter_pixel<MODE_GAUSS2>(J, u.y, i, table, h2); break;
+      case MODE_GAUSS5: scatter_pixel<MODE_GAUSS5>(J, u.y, i, table, h5); break;
+      case MODE_TRILINEAR: scatter_pixel<MODE_TRILINEAR>(J, u.y, i, table, h2); break;
+      case MODE_ITER: scatter_pixel_iter(J, u.y, i, table); break;
+      default: break;
+    }
+  }
 }
 
 static float mode_h(int mode) {
@@ -360,6 +408,23 @@ cudaError_t launch_edge(const InsertJob &j, cudaStream_t st) {
     case MODE_TRILINEAR: k_edge<MODE_TRILINEAR><<<grid, 128, 0, st>>>(j, tab, h); break;
     default: return cudaErrorInvalidValue;
   }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_scatter_multi(const InsertJob *d_jobs, const int2 *d_units, int nunits,
+                                 int max_px, bool edge_only, cudaStream_t st) {
+  if (nunits == 0 || max_px == 0) return cudaSuccess;
+  const Consts &c = consts();
+  // blocks per unit: enough for ~4 waves of resident blocks in all, each
+  // striding over its job's pixels (one pixel per thread at most)
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const long want = (4L * sms * 8 + nunits - 1) / nunits;
+  const int per = (int)std::max(1L, std::min<long>(want, (max_px + 255) / 256));
+  dim3 grid(nunits, per);
+  note_launch();
+  k_scatter_multi<<<grid, 256, 0, st>>>(d_jobs, d_units, c.d_exp, c.h2, c.h5, edge_only ? 1 : 0);
   return cudaGetLastError();
 }
 

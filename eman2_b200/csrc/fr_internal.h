@@ -92,6 +92,11 @@ cudaError_t launch_gather(const InsertJob *d_jobs, const InsertJob *h_jobs, int 
 cudaError_t launch_edge(const InsertJob &j, cudaStream_t st);
 cudaError_t launch_scatter_tables(const InsertJob &j, const float *table, float h,
                                   cudaStream_t st);
+// Scatter (edge_only: face taps of the rim pixels) of several jobs in one
+// launch: units[u] = (job index in d_jobs, slice), max_px = the largest pixel
+// (or rim) count of those jobs.
+cudaError_t launch_scatter_multi(const InsertJob *d_jobs, const int2 *d_units, int nunits,
+                                 int max_px, bool edge_only, cudaStream_t st);
 // Column-owner kernel (fr_column.cu): 16^3 tiles, work items (job, tile,
 // first slice, end slice) over slice blocks of at most kColumnBlock.
 constexpr int kColumnTile = kNumTiles;   // tile id selecting the column kernel
@@ -140,7 +145,12 @@ void gather_tiles(int N, int mode, int tile, int corners, std::vector<int> &out,
                   int &tz);
 
 // Prologue (fr_prologue.cu).
-cudaError_t launch_pad(const float *d_raw, int n, int box, int N, float *d_img, cudaStream_t st);
+// Edge-mean subtraction and zero-pad clip of n raw images of size box to N
+// (from d_raw, or particle p from d_src[p] when a device pointer table is
+// given) and, in the same launch, the rotation composition launch_compose does.
+cudaError_t launch_pad_compose(const float *d_raw, const float *const *d_src, int n, int box, int N,
+                               float *d_img, const float *d_rot, const float *d_sym, int nsym,
+                               float *d_t3d, cudaStream_t st);
 void ctf_constants(float defocus, float dfdiff, float dfang, float voltage, float cs, float apix,
                    float ampcont, int N, void *out);
 size_t ctf_dev_size();
@@ -151,6 +161,13 @@ cudaError_t launch_edge_mean(const float *d_img_off, const float *d_img_on, cons
 cudaError_t launch_shift_corner(const float *d_img_off, const float *d_img_on, const void *d_ctf,
                                 const float *d_mean, const float *d_txy, int txy_stride, int n,
                                 int N, float scale_out, float *d_out, cudaStream_t st);
+// Edge mean and shift in one launch (each block forms its particle's edge
+// mean); chosen by mean_shift_fused(n, N) for launches small enough that the
+// repeated border reads cost less than a kernel.
+bool mean_shift_fused(int n, int N);
+cudaError_t launch_mean_shift_corner(const float *d_img_off, const float *d_img_on,
+                                     const void *d_ctf, const float *d_txy, int txy_stride, int n,
+                                     int N, float scale_out, float *d_out, cudaStream_t st);
 
 // Finish / agreement (fr_finish.cu).
 cudaError_t launch_normalize(float *d_data, float *d_norm, int N, int sqrtnorm, cudaStream_t st,

@@ -10,6 +10,7 @@
 //     r2c FFT, x sqrt((N+2)/N)
 // Here the FFTs are batched cuFFT plans and everything between them is one
 // kernel per stage over all particles of a chunk.
+#include <algorithm>
 #include <cmath>
 
 #include "fr_device.cuh"
@@ -53,16 +54,38 @@ __device__ float edge_mean_dev(const float *img, int nx, int ny, float scale, do
 }
 
 // Edge-mean subtract and zero-padded clip of box x box raw particles to N x N.
-__global__ void __launch_bounds__(256) k_pad(const float *__restrict__ raw, int box, int N,
-                                             float *__restrict__ out) {
+// Particle p's raw image is raw[p] (contiguous images), or src[p] when a
+// per-particle table is given (the particles of several jobs in one launch).
+// grid.x = particle; the grid.y blocks of a particle share its pixels (each
+// forms the same edge mean).  With rot, block (p, 0) also composes the
+// particle's symmetry copies, t3d[p*nsym+q] = rot[p] * sym[q]
+// (libEM/transform.cpp:1384-1395), in float with the products and sums
+// rounded in that order.
+__global__ void __launch_bounds__(256) k_pad(const float *__restrict__ raw,
+                                             const float *const *__restrict__ src_tab, int box,
+                                             int N, float *__restrict__ out,
+                                             const float *__restrict__ rot,
+                                             const float *__restrict__ sym, int nsym,
+                                             float *__restrict__ t3d) {
   __shared__ double s_red[8];
   const int p = blockIdx.x;
-  const float *src = raw + (size_t)p * box * box;
+  if (rot && blockIdx.y == 0) {
+    for (int t = threadIdx.x; t < nsym * 9; t += blockDim.x) {
+      const int q = t / 9, e = t % 9, i = e / 3, j = e % 3;
+      const float *a = rot + 9 * (size_t)p;
+      const float *b = sym + 9 * q;
+      float v = __fmul_rn(a[3 * i + 0], b[j]);
+      v = __fadd_rn(v, __fmul_rn(a[3 * i + 1], b[3 + j]));
+      v = __fadd_rn(v, __fmul_rn(a[3 * i + 2], b[6 + j]));
+      t3d[((size_t)p * nsym + q) * 9 + e] = v;
+    }
+  }
+  const float *src = src_tab ? src_tab[p] : raw + (size_t)p * box * box;
   const float mean = edge_mean_dev(src, box, box, 1.0f, s_red);
   // Region origin (box - N) // 2 (Python floor division).
   const int o = (box - N) >= 0 ? (box - N) / 2 : -((N - box + 1) / 2);
   float *dst = out + (size_t)p * N * N;
-  for (int i = threadIdx.x; i < N * N; i += blockDim.x) {
+  for (int i = blockIdx.y * blockDim.x + threadIdx.x; i < N * N; i += gridDim.y * blockDim.x) {
     const int y = i / N, x = i % N;
     const int sy = y + o, sx = x + o;
     float v = 0.0f;
@@ -71,10 +94,17 @@ __global__ void __launch_bounds__(256) k_pad(const float *__restrict__ raw, int 
   }
 }
 
-cudaError_t launch_pad(const float *d_raw, int n, int box, int N, float *d_img, cudaStream_t st) {
+cudaError_t launch_pad_compose(const float *d_raw, const float *const *d_src, int n, int box, int N,
+                               float *d_img, const float *d_rot, const float *d_sym, int nsym,
+                               float *d_t3d, cudaStream_t st) {
   if (n == 0) return cudaSuccess;
+  // few particles: several blocks each, so the launch still fills the device
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int parts = std::max(1, std::min(16, (16 * sms + n - 1) / n));
   note_launch();
-  k_pad<<<n, 256, 0, st>>>(d_raw, box, N, d_img);
+  k_pad<<<dim3(n, parts), 256, 0, st>>>(d_raw, d_src, box, N, d_img, d_rot, d_sym, nsym, d_t3d);
   return cudaGetLastError();
 }
 
@@ -194,16 +224,20 @@ __device__ __forceinline__ float src_at(const float *img, size_t k, float scale_
 // inverse translation (tx, ty), then phase origin to corner, then x scale_out
 // (the sqrt((N+2)/N) factor, applied before the r2c instead of after it).
 // txy == nullptr or |t| < 1e-6 (Transform::is_identity) copies.
+// fuse_mean: each block forms its particle's edge mean itself (as
+// k_edge_mean does, same partition and order, so the same value): for small
+// launches, where one kernel fewer matters more than the repeated border reads.
 __global__ void __launch_bounds__(256) k_shift_corner(SrcSel sel, const float *__restrict__ mean,
                                                       const float *__restrict__ txy,
                                                       int txy_stride, int N, float scale_out,
-                                                      float *__restrict__ out) {
+                                                      float *__restrict__ out, int fuse_mean) {
+  __shared__ double s_red[8];
   const int p = blockIdx.y;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= N * N) return;
   const float *src = sel.img(p, (size_t)N * N);
   const float scale_in = sel.scale(p);
-  const float m = mean ? mean[p] : 0.0f;
+  const float m = fuse_mean ? edge_mean_dev(src, N, N, scale_in, s_red) : (mean ? mean[p] : 0.0f);
+  if (i >= N * N) return;
   const int yo = i / N, xo = i % N;
   const int h = N / 2;
   // phase origin to corner (even N): out[y][x] = in[(y+N/2)%N][(x+N/2)%N]
@@ -247,7 +281,24 @@ cudaError_t launch_shift_corner(const float *d_img_off, const float *d_img_on, c
              1.0f / ((float)N * (float)N)};
   dim3 grid((N * N + 255) / 256, n);
   note_launch();
-  k_shift_corner<<<grid, 256, 0, st>>>(sel, d_mean, d_txy, txy_stride, N, scale_out, d_out);
+  k_shift_corner<<<grid, 256, 0, st>>>(sel, d_mean, d_txy, txy_stride, N, scale_out, d_out, 0);
+  return cudaGetLastError();
+}
+
+bool mean_shift_fused(int n, int N) {
+  // border floats re-read by all blocks: at most ~16 MB
+  return (double)n * ((N * N + 255) / 256) * 4.0 * N <= 4.0e6;
+}
+
+cudaError_t launch_mean_shift_corner(const float *d_img_off, const float *d_img_on,
+                                     const void *d_ctf, const float *d_txy, int txy_stride, int n,
+                                     int N, float scale_out, float *d_out, cudaStream_t st) {
+  if (n == 0) return cudaSuccess;
+  SrcSel sel{d_img_off, d_img_on, reinterpret_cast<const CtfDev *>(d_ctf),
+             1.0f / ((float)N * (float)N)};
+  dim3 grid((N * N + 255) / 256, n);
+  note_launch();
+  k_shift_corner<<<grid, 256, 0, st>>>(sel, nullptr, d_txy, txy_stride, N, scale_out, d_out, 1);
   return cudaGetLastError();
 }
 

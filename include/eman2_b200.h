@@ -286,11 +286,13 @@ FR_API int fr_insert_particles_multi(fr_recon *const *handles, int nh, const flo
 
 /* A batched insertion round of fixed shapes (counts[j] <= 4096 particles of
  * box boxes[j] for handle j; 0 leaves a job out), captured once as a CUDA
- * graph on `stream` (NULL: the first handle's): every job's prologue (pad,
- * CTF flip pair where ctf[j] is set, edge mean, shift, r2c, rotation
- * composition), the persistent insertion launches and the face taps.  The
- * graph owns the device image slots and the chunk scratch; the handles must
- * outlive it.  No counterpart in the reference. */
+ * graph on `stream` (NULL: the first handle's): the prologue (pad, CTF flip
+ * pair where ctf[j] is set, edge mean, shift, r2c, rotation composition), run
+ * once per group of jobs of equal (N, box, symmetry) over their particles,
+ * the groups as parallel branches; then the insertion launches (per schedule
+ * one persistent launch or one scatter over all its jobs) and the face taps.
+ * The graph owns the device image slots and the prologue scratch; the
+ * handles must outlive it.  No counterpart in the reference. */
 typedef struct fr_graph fr_graph;
 FR_API int fr_graph_create(fr_recon *const *handles, int nh, const int *boxes, const int *counts,
                            const int *ctf, void *stream, fr_graph **out);
@@ -300,11 +302,14 @@ FR_API int fr_batch_graph_create(fr_batch *b, const int *boxes, const int *count
 /* Device slot of job j's images (float[counts[j]][box][box]): a caller may
  * write the particles there and pass imgs = NULL to fr_graph_launch. */
 FR_API int fr_graph_slot(fr_graph *g, int job, float **d_images);
-/* One replay on the batch stream: meta[j] (counts[j] particles each) is
- * staged through pinned memory; imgs[j] (host or device; NULL: the slots as
- * filled) is copied into the slots; then the graph is launched.  Returns once
- * enqueued (after reading host images).  Whether a job's particles carry a
- * CTF must match its ctf[j] at capture (FR_EINVAL_PARAM otherwise). */
+/* One replay on the batch stream: meta[j] (counts[j] particles each) and the
+ * particles' image addresses are staged through pinned memory and uploaded
+ * as one block; device imgs[j] are read in place (unchanged until the replay
+ * has run on the stream), host imgs[j] are copied into the slots, NULL reads
+ * the slots as filled; then the graph is launched.  Returns once enqueued
+ * (after reading host images).  Particles with a CTF need their group to have
+ * been captured with the phase flip (ctf[j] set for one of its jobs;
+ * FR_EINVAL_PARAM otherwise); particles without one are accepted either way. */
 FR_API int fr_graph_launch(fr_graph *g, const float *const *imgs, const fr_particle *const *meta);
 FR_API int fr_graph_destroy(fr_graph *g);
 

@@ -114,6 +114,85 @@ def test_graph_replays_equal_batched_rounds(gpu):
     g.close()
 
 
+def _grouped_jobs():
+    """Jobs that share (N, box, symmetry) and so one prologue launch per
+    stage: with and without a CTF, different inserters (so different
+    schedules), beside a job of its own group."""
+    from eman2_b200.particles import particle_meta
+    from eman2_b200.synth import make_particles
+    specs = [(32, 48, "gauss_2", "c1", 20, True), (32, 48, "gauss_2", "c1", 14, False),
+             (32, 48, "gauss_5", "c1", 9, True), (32, 48, "nearest_neighbor", "c1", 17, False),
+             (40, 60, "gauss_2", "d2", 11, True)]
+    jobs = []
+    for k, (box, N, mode, sym, n, ctf) in enumerate(specs):
+        ps = make_particles(box, n, seed=700 + k, snr=0.5, shift=2.0, weights=(0.5, 1.0), ctf=ctf)
+        meta = particle_meta(ps.rots, ps.shifts, ps.weights, defocus=ps.defocus)
+        jobs.append(({"size": [N] * 3, "sym": sym, "mode": mode}, ps, meta, ctf))
+    return jobs
+
+
+def test_grouped_prologue_equals_each_job_alone(gpu):
+    """Jobs of equal (N, box, symmetry) run one prologue over their
+    concatenated particles (mixed CTF, mixed schedules): each job still gets
+    its alone result, batched and through a graph reading device images in
+    place."""
+    import torch
+
+    from eman2_b200.batch import BatchReconstructor
+    jobs = _grouped_jobs()
+    params = [p for p, _, _, _ in jobs]
+    b = BatchReconstructor(params)
+    b.insert_particles([ps.images for _, ps, _, _ in jobs], [m for _, _, m, _ in jobs])
+    alone = [_alone(p, ps.images, m) for p, ps, m, _ in jobs]
+    for j in range(len(jobs)):
+        d, n = b.get_accumulators(j)
+        assert oracle.rel_l2(d, alone[j][0]) < RTOL and oracle.rel_l2(n, alone[j][1]) < RTOL
+    g_b = BatchReconstructor(params)
+    g = g_b.capture([ps.images.shape[-1] for _, ps, _, _ in jobs],
+                    [len(ps.images) for _, ps, _, _ in jobs], [c for _, _, _, c in jobs])
+    dev = [torch.as_tensor(ps.images, device="cuda") for _, ps, _, _ in jobs]
+    g.launch(dev, [m for _, _, m, _ in jobs])
+    torch.cuda.synchronize()
+    for j in range(len(jobs)):
+        d, n = g_b.get_accumulators(j)
+        assert oracle.rel_l2(d, alone[j][0]) < RTOL and oracle.rel_l2(n, alone[j][1]) < RTOL
+    g.close()
+
+
+def test_graph_of_one_particle_jobs_scatter(gpu):
+    """One particle per job, every job pinned to the scatter schedule: the
+    round's insertion is one multi-job scatter launch, and replays equal the
+    jobs inserted alone."""
+    import torch
+
+    from eman2_b200.batch import BatchReconstructor, set_tile
+    from eman2_b200.particles import particle_meta
+    jobs = _grouped_jobs()
+    nsym = {"c1": 1, "d2": 4}
+    keys = {(p["size"][0], p["mode"], nsym[p["sym"]]) for p, _, _, _ in jobs}
+    try:
+        for k in keys:
+            set_tile(k[0], k[1], k[2], -2)
+        b = BatchReconstructor([p for p, _, _, _ in jobs])
+        g = b.capture([ps.images.shape[-1] for _, ps, _, _ in jobs], [1] * len(jobs),
+                      [c for _, _, _, c in jobs])
+        for i in range(3):
+            imgs = [torch.as_tensor(ps.images[i:i + 1], device="cuda") for _, ps, _, _ in jobs]
+            metas = [particle_meta(ps.rots[i:i + 1], ps.shifts[i:i + 1], ps.weights[i:i + 1],
+                                   defocus=ps.defocus[i:i + 1]) for _, ps, _, _ in jobs]
+            g.launch(imgs, metas)
+        torch.cuda.synchronize()
+        got = [b.get_accumulators(j) for j in range(len(jobs))]
+        g.close()
+    finally:
+        for k in keys:
+            set_tile(k[0], k[1], k[2], -1)
+    for j, (params, ps, meta, _) in enumerate(jobs):
+        d0, n0 = _alone(params, ps.images[:3], particle_meta(
+            ps.rots[:3], ps.shifts[:3], ps.weights[:3], defocus=ps.defocus[:3]))
+        assert oracle.rel_l2(got[j][0], d0) < RTOL and oracle.rel_l2(got[j][1], n0) < RTOL
+
+
 def test_graph_rejects_ctf_mismatch(gpu):
     from eman2_b200.batch import BatchReconstructor
     from eman2_b200.exceptions import InvalidParameterException
