@@ -643,7 +643,7 @@ def run_gpu(args, wl, ws, rank, local):
 
     # e2e: the same steps through the public API from pinned host memory
     h_imgs = d_imgs.cpu().pin_memory()
-    for _ in range(max(1, args.warmup // 2)):
+    for _ in range(max(2, args.warmup)):      # both staging buffers allocated
         step(h_imgs)
     torch.cuda.synchronize()
     barrier(ws)
