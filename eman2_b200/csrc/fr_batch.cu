@@ -541,6 +541,7 @@ struct fr_graph {
   fr::RoundPlan plan;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
+  cudaGraphNode_t meta_node = nullptr;   // the metadata upload, the graph's first node
   std::mutex mu;
 };
 
@@ -566,9 +567,11 @@ static void graph_free(fr_graph *g) {
   delete g;
 }
 
-// The graph's device work: the groups' prologues (parallel branches when
-// there are several), then the round's insertion launches on st.
+// The graph's device work: the metadata upload (its source, one of the two
+// pinned staging blocks, is set per replay), the groups' prologues (parallel
+// branches when there are several), then the round's insertion launches.
 static int graph_device_work(fr_graph *g, cudaStream_t st) {
+  CU(cudaMemcpyAsync(g->d_meta.p, g->pinned[0], g->meta_bytes, cudaMemcpyHostToDevice, st));
   const int ng = (int)g->groups.size();
   const int nside = std::min(ng, (int)fr_graph::kSide);
   if (ng > 1) {
@@ -586,6 +589,26 @@ static int graph_device_work(fr_graph *g, cudaStream_t st) {
       CU(cudaStreamWaitEvent(st, g->join[k], 0));
     }
   return plan_launch(g->plan, g->bs, st);
+}
+
+// The captured metadata upload: the memcpy node that writes d_meta.
+static int find_meta_node(fr_graph *g) {
+  size_t nn = 0;
+  CU(cudaGraphGetNodes(g->graph, nullptr, &nn));
+  std::vector<cudaGraphNode_t> nodes(nn);
+  CU(cudaGraphGetNodes(g->graph, nodes.data(), &nn));
+  for (cudaGraphNode_t n : nodes) {
+    cudaGraphNodeType t;
+    CU(cudaGraphNodeGetType(n, &t));
+    if (t != cudaGraphNodeTypeMemcpy) continue;
+    cudaMemcpy3DParms p;
+    CU(cudaGraphMemcpyNodeGetParams(n, &p));
+    if (p.dstPtr.ptr == g->d_meta.p) {
+      g->meta_node = n;
+      return FR_OK;
+    }
+  }
+  return fail(FR_ECUDA, "captured graph has no metadata upload node");
 }
 
 static int graph_create(const std::vector<fr_recon *> &jobs, cudaStream_t st, int tile_pref,
@@ -685,6 +708,7 @@ static int graph_create(const std::vector<fr_recon *> &jobs, cudaStream_t st, in
       g->kernels = launches_noted() - noted;
     }
   }
+  if (rc == FR_OK) rc = find_meta_node(g);
   if (rc == FR_OK && cudaGraphInstantiate(&g->exec, g->graph, 0) != cudaSuccess)
     rc = fail(FR_ECUDA, "cudaGraphInstantiate failed: %s", cudaGetErrorString(cudaGetLastError()));
   stream_leave_all(jobs, st);
@@ -752,7 +776,7 @@ int fr_graph_launch(fr_graph *g, const float *const *imgs, const fr_particle *co
     host_src |= imgs && !in_place;
   }
   const int k = g->next;
-  // this staging block was last read by the copy two replays ago
+  // this staging block was last read by the replay before the previous one
   if (g->staged_used[k]) CU(cudaEventSynchronize(g->staged[k]));
   for (const ProGroup &q : g->groups) {
     const bool any = group_meta(q, meta, src.data(), g->pinned[k] + q.meta_off);
@@ -763,16 +787,18 @@ int fr_graph_launch(fr_graph *g, const float *const *imgs, const fr_particle *co
   }
   g->next ^= 1;
   for (fr_recon *r : g->jobs) TRY(stream_enter(r, st));
-  CU(cudaMemcpyAsync(g->d_meta.p, g->pinned[k], g->meta_bytes, cudaMemcpyHostToDevice, st));
-  CU(cudaEventRecord(g->staged[k], st));
-  g->staged_used[k] = true;
   for (int j = 0; host_src && j < nj; j++) {
     const int n = g->counts[j];
     if (n == 0 || is_device_ptr(imgs[j])) continue;
     const size_t bytes = sizeof(float) * (size_t)n * g->boxes[j] * g->boxes[j];
     CU(cudaMemcpyAsync(g->slots[j].p, imgs[j], bytes, cudaMemcpyHostToDevice, st));
   }
+  // the graph's first node uploads this replay's block
+  CU(cudaGraphExecMemcpyNodeSetParams1D(g->exec, g->meta_node, g->d_meta.p, g->pinned[k],
+                                        g->meta_bytes, cudaMemcpyHostToDevice));
   CU(cudaGraphLaunch(g->exec, st));
+  CU(cudaEventRecord(g->staged[k], st));
+  g->staged_used[k] = true;
   note_launch((int)g->kernels);
   TRY(stream_leave_all(g->jobs, st));
   if (host_src) CU(cudaStreamSynchronize(st));   // host images may be pinned: read them first

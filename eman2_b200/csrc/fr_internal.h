@@ -163,7 +163,7 @@ cudaError_t launch_shift_corner(const float *d_img_off, const float *d_img_on, c
                                 int N, float scale_out, float *d_out, cudaStream_t st);
 // Edge mean and shift in one launch (each block forms its particle's edge
 // mean); chosen by mean_shift_fused(n, N) for launches small enough that the
-// repeated border reads cost less than a kernel.
+// repeated reductions cost less than a kernel.
 bool mean_shift_fused(int n, int N);
 cudaError_t launch_mean_shift_corner(const float *d_img_off, const float *d_img_on,
                                      const void *d_ctf, const float *d_txy, int txy_stride, int n,

@@ -286,8 +286,13 @@ cudaError_t launch_shift_corner(const float *d_img_off, const float *d_img_on, c
 }
 
 bool mean_shift_fused(int n, int N) {
-  // border floats re-read by all blocks: at most ~16 MB
-  return (double)n * ((N * N + 255) / 256) * 4.0 * N <= 4.0e6;
+  // Each block's own edge-mean reduction lengthens its life by a few
+  // microseconds: worth one kernel fewer only while the launch is a single
+  // wave of at most two blocks per SM (one particle at N <= ~270).
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  return (long)n * ((N * N + 255) / 256) <= 2L * sms;
 }
 
 cudaError_t launch_mean_shift_corner(const float *d_img_off, const float *d_img_on,

@@ -10,6 +10,7 @@ are used in place).
 from __future__ import annotations
 
 import ctypes
+import threading
 
 import numpy as np
 
@@ -70,6 +71,25 @@ def library_stream(handle) -> int:
     return out.value or 0
 
 
+_joins = threading.local()
+
+
+def _join_parts(ptr: int, dev):
+    """This thread's wrapper of library stream `ptr` and its two events,
+    reused across calls (a wait takes the event as last recorded, so
+    re-recording it later does not move earlier waits)."""
+    import torch
+    cache = getattr(_joins, "cache", None)
+    if cache is None or len(cache) > 256:
+        cache = _joins.cache = {}
+    key = (ptr, dev.index)
+    parts = cache.get(key)
+    if parts is None:
+        parts = (torch.cuda.ExternalStream(ptr, device=dev), torch.cuda.Event(), torch.cuda.Event())
+        cache[key] = parts
+    return parts
+
+
 class join_streams:
     """Around an insertion call given CUDA tensors (the call returns before
     its kernels finish): the library stream first waits for torch's current
@@ -78,21 +98,23 @@ class join_streams:
     is not rewritten before the kernels have read it."""
 
     def __init__(self, stream_ptr: int, *arrays):
-        self.ts = [a for a in arrays if getattr(a, "is_cuda", False)]
+        self.ts = next((a for a in arrays if getattr(a, "is_cuda", False)), None)
         self.ptr = stream_ptr
 
     def __enter__(self):
-        if self.ts:
+        if self.ts is not None:
             import torch
-            dev = self.ts[0].device
+            dev = self.ts.device
             self.cur = torch.cuda.current_stream(dev)
-            self.ext = torch.cuda.ExternalStream(self.ptr, device=dev)
-            self.ext.wait_stream(self.cur)
+            self.ext, ev_in, self.ev_out = _join_parts(self.ptr, dev)
+            ev_in.record(self.cur)
+            self.ext.wait_event(ev_in)
         return self
 
     def __exit__(self, *exc):
-        if self.ts:
-            self.cur.wait_stream(self.ext)
+        if self.ts is not None:
+            self.ev_out.record(self.ext)
+            self.cur.wait_event(self.ev_out)
         return False
 
 

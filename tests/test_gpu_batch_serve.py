@@ -10,7 +10,10 @@ from oracle import oracle
 
 pytestmark = pytest.mark.gpu
 
-RTOL = 2e-6
+# Two GPU runs of the same job differ only in the order of their FP32 atomic
+# adds; for gauss_5 with symmetry copies (216 taps per pixel, several slices
+# per particle) that order alone moves the volumes by up to ~2e-6 relative L2.
+RTOL = 5e-6
 
 
 def _jobs():
