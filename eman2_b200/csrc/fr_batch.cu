@@ -284,38 +284,43 @@ static void plan_groups(const std::vector<fr_recon *> &jobs, RoundPlan &P) {
 // vectors: the copies have taken them when cudaMemcpyAsync returns).
 static int plan_upload(const RoundPlan &P, BatchScratch &bs, cudaStream_t st) {
   TRY(bs.d_jobs.ensure(sizeof(InsertJob) * std::max<size_t>(1, P.hj.size())));
-  TRY(bs.d_counter.ensure(sizeof(int)));
+  TRY(bs.d_counter.ensure(sizeof(int) * std::max<size_t>(1, P.groups.size())));
   TRY(bs.d_work.ensure(std::max<size_t>(16, P.work.size())));
   TRY(bs.ring.upload(bs.d_jobs.p, P.hj.data(), sizeof(InsertJob) * P.hj.size(), st));
   if (!P.work.empty()) TRY(bs.ring.upload(bs.d_work.p, P.work.data(), P.work.size(), st));
   return FR_OK;
 }
 
-// Device work of the round: per schedule group one persistent launch (or the
-// scatter), then the face taps.  Kernels and memsets only.
-static int plan_launch(const RoundPlan &P, BatchScratch &bs, cudaStream_t st) {
+// Device work of schedule group gi: one persistent launch (or the scatter
+// over all its jobs), then the face taps.  Kernels only; each group has its
+// own work counter, so groups (which insert into different jobs) may run
+// concurrently.
+static int plan_launch_group(const RoundPlan &P, BatchScratch &bs, size_t gi, cudaStream_t st) {
   const InsertJob *d_jobs = bs.d_jobs.as<InsertJob>();
-  for (const RoundGroup &g : P.groups) {
-    const int2 *units = (const int2 *)((const unsigned char *)bs.d_work.p + g.units_off);
-    if (g.tile == kTunedScatter) {
-      CU(launch_scatter_multi(d_jobs, units, (int)g.nunits, g.max_px, false, st));
-      continue;
-    }
-    const void *w = (const unsigned char *)bs.d_work.p + g.off;
-    if (g.tile == kPixelTile)
-      CU(launch_pixel(d_jobs, (const int4 *)w, (int)g.nwork, kColumnBlock, bs.d_counter.as<int>(),
-                      g.maxN, st));
-    else if (g.tile == kColumn3Tile)
-      CU(launch_column3(d_jobs, (const int4 *)w, (int)g.nwork, kColumnBlock, bs.d_counter.as<int>(),
-                        g.maxN, st));
-    else if (g.tile == kColumnTile)
-      CU(launch_column(d_jobs, (const int4 *)w, (int)g.nwork, kColumnBlock, bs.d_counter.as<int>(),
-                       g.max_mode, st));
-    else
-      CU(launch_gather(d_jobs, P.hj.data(), (int)P.hj.size(), (const int2 *)w, (int)g.nwork,
-                       g.tile, bs.d_counter.as<int>(), g.max_mode, st));
-    CU(launch_scatter_multi(d_jobs, units, (int)g.nunits, g.max_px, true, st));
+  const RoundGroup &g = P.groups[gi];
+  int *counter = bs.d_counter.as<int>() + gi;
+  const int2 *units = (const int2 *)((const unsigned char *)bs.d_work.p + g.units_off);
+  if (g.tile == kTunedScatter) {
+    CU(launch_scatter_multi(d_jobs, units, (int)g.nunits, g.max_px, false, st));
+    return FR_OK;
   }
+  const void *w = (const unsigned char *)bs.d_work.p + g.off;
+  if (g.tile == kPixelTile)
+    CU(launch_pixel(d_jobs, (const int4 *)w, (int)g.nwork, kColumnBlock, counter, g.maxN, st));
+  else if (g.tile == kColumn3Tile)
+    CU(launch_column3(d_jobs, (const int4 *)w, (int)g.nwork, kColumnBlock, counter, g.maxN, st));
+  else if (g.tile == kColumnTile)
+    CU(launch_column(d_jobs, (const int4 *)w, (int)g.nwork, kColumnBlock, counter, g.max_mode, st));
+  else
+    CU(launch_gather(d_jobs, P.hj.data(), (int)P.hj.size(), (const int2 *)w, (int)g.nwork, g.tile,
+                     counter, g.max_mode, st));
+  CU(launch_scatter_multi(d_jobs, units, (int)g.nunits, g.max_px, true, st));
+  return FR_OK;
+}
+
+// The round's schedule groups one after another on st.
+static int plan_launch(const RoundPlan &P, BatchScratch &bs, cudaStream_t st) {
+  for (size_t gi = 0; gi < P.groups.size(); gi++) TRY(plan_launch_group(P, bs, gi, st));
   return FR_OK;
 }
 
@@ -569,7 +574,8 @@ static void graph_free(fr_graph *g) {
 
 // The graph's device work: the metadata upload (its source, one of the two
 // pinned staging blocks, is set per replay), the groups' prologues (parallel
-// branches when there are several), then the round's insertion launches.
+// branches when there are several), then the round's insertion launches (one
+// branch per schedule group).
 static int graph_device_work(fr_graph *g, cudaStream_t st) {
   CU(cudaMemcpyAsync(g->d_meta.p, g->pinned[0], g->meta_bytes, cudaMemcpyHostToDevice, st));
   const int ng = (int)g->groups.size();
@@ -588,7 +594,19 @@ static int graph_device_work(fr_graph *g, cudaStream_t st) {
       CU(cudaEventRecord(g->join[k], g->side[k]));
       CU(cudaStreamWaitEvent(st, g->join[k], 0));
     }
-  return plan_launch(g->plan, g->bs, st);
+  // the schedule groups (disjoint jobs) as parallel branches too
+  const int nsched = (int)g->plan.groups.size();
+  if (nsched <= 1) return plan_launch(g->plan, g->bs, st);
+  const int nside2 = std::min(nsched, (int)fr_graph::kSide);
+  CU(cudaEventRecord(g->fork, st));
+  for (int k = 0; k < nside2; k++) CU(cudaStreamWaitEvent(g->side[k], g->fork, 0));
+  for (int gi = 0; gi < nsched; gi++)
+    TRY(plan_launch_group(g->plan, g->bs, gi, g->side[gi % fr_graph::kSide]));
+  for (int k = 0; k < nside2; k++) {
+    CU(cudaEventRecord(g->join[k], g->side[k]));
+    CU(cudaStreamWaitEvent(st, g->join[k], 0));
+  }
+  return FR_OK;
 }
 
 // The captured metadata upload: the memcpy node that writes d_meta.
