@@ -752,8 +752,10 @@ def main():
     V = (N // 2 + 1) * N * N
     alg_bytes = args.batch * (8 * (N // 2 + 1) * N + 64) + 24 * V
     if st["gather_launches"] > 0:
-        tile = args.tile if args.tile != -1 else 5          # the library's default: k_column3
-        kname = {5: "k_column3", 4: "k_column"}.get(tile, "k_gather") + " (gather schedule)"
+        # the library's default: k_column3 for gauss_5, k_pixel for the narrow windows
+        tile = args.tile if args.tile != -1 else (5 if wl["mode"] == "gauss_5" else 6)
+        kname = {6: "k_pixel", 5: "k_column3", 4: "k_column"}.get(tile, "k_gather") + \
+            " (gather schedule)"
         gms = st["gather_ms"] / st["gather_launches"]
     else:
         kname, gms = "k_scatter", st["insert_ms"] / max(1, st["insert_launches"])
