@@ -223,6 +223,7 @@ __device__ __forceinline__ float pixel_weight(const InsertJob &J, int p, int x, 
 __global__ void k_zero_int(int *p) { *p = 0; }
 
 cudaError_t zero_counter(int *d_counter, cudaStream_t st) {
+  note_launch();
   k_zero_int<<<1, 1, 0, st>>>(d_counter);
   return cudaGetLastError();
 }
