@@ -676,7 +676,8 @@ __device__ void tile_item3(const InsertJob &J, int tile, int s0, int s1, const S
 constexpr int PROWS = 32;   // rows per row batch of a pass
 
 struct Smem4 {
-  float *are, *aim, *awt, *aflag;   // accumulators, one array per component [NV]
+  float *are, *aim, *awt;     // accumulators, one array per component [NV]
+  int *origin;                // the volume's origin cell got a direct tap (its imag is 0)
   float4 *steps;
   float *rtab;
   int *xmax;
@@ -716,7 +717,7 @@ __device__ __forceinline__ void tile_tap(const Smem4 &S, int sg, int i, int j, i
   const int c = cell_slot(ti - base[0], tj - base[1], tk - base[2]);
   if (sg > 0) {
     atomicAdd(&S.are[c], vre);
-    if (origin) S.aflag[c] = 1.0f;
+    if (origin) *S.origin = 1;
     else atomicAdd(&S.aim[c], vim);
     atomicAdd(&S.awt[c], vw);
   } else {
@@ -886,9 +887,11 @@ __device__ void tile_item4(const InsertJob &J, int tile, int s0, int s1, const S
     S.are[i] = 0.f;
     S.aim[i] = 0.f;
     S.awt[i] = 0.f;
-    S.aflag[i] = 0.f;
   }
-  if (threadIdx.x == 0) *S.next = 0;
+  if (threadIdx.x == 0) {
+    *S.next = 0;
+    *S.origin = 0;
+  }
   __syncthreads();
   if (threadIdx.x == 0) {
     if (MODE == MODE_GAUSS2) S.state[0] = (unsigned long long)MODE;
@@ -916,9 +919,10 @@ __device__ void tile_item4(const InsertJob &J, int tile, int s0, int s1, const S
   for (int i = threadIdx.x; i < NV; i += NT) {
     const int lz = i >> 8, ly = (i >> 4) & 15, lx = i & 15;
     const int c = cell_slot(lx, ly, lz);
-    const float4 v = make_float4(S.are[c], S.aim[c], S.awt[c], S.aflag[c]);
-    if (v.x == 0.f && v.y == 0.f && v.z == 0.f && v.w == 0.f) continue;
     const int vx = base[0] + lx, vy = base[1] + ly, vz = base[2] + lz;
+    const bool org = vx == 0 && vy == 0 && vz == 0 && *S.origin;
+    const float4 v = make_float4(S.are[c], S.aim[c], S.awt[c], org ? 1.0f : 0.0f);
+    if (v.x == 0.f && v.y == 0.f && v.z == 0.f && v.w == 0.f) continue;
     if (vx > ext[0] || vy > ext[1] || vz > ext[2]) continue;
     const size_t row = (size_t)(vy < 0 ? N + vy : vy);
     const size_t slab = (size_t)(vz < 0 ? N + vz : vz);
@@ -1042,20 +1046,20 @@ cudaError_t launch_column3(const InsertJob *d_jobs, const int4 *d_work, int nwor
   return cudaGetLastError();
 }
 
-__global__ void __launch_bounds__(col::NT, 2)
+__global__ void __launch_bounds__(col::NT, 3)
     k_pixel(const InsertJob *__restrict__ jobs, const int4 *__restrict__ work, int nwork,
             int block, int *counter, float h2, ExpSteps st2, int maxN, int *err) {
   extern __shared__ float4 s_dyn[];
   __shared__ int s_work;
   __shared__ int s_wcount[col::NT / 32];
   __shared__ unsigned long long s_state[2];
-  __shared__ int s_next;
+  __shared__ int s_next, s_origin;
   col::Smem4 S;
   S.are = reinterpret_cast<float *>(s_dyn);
   S.aim = S.are + col::NV;
   S.awt = S.aim + col::NV;
-  S.aflag = S.awt + col::NV;
-  S.steps = s_dyn + col::NV;
+  S.origin = &s_origin;
+  S.steps = reinterpret_cast<float4 *>(S.awt + col::NV);
   S.rtab = reinterpret_cast<float *>(S.steps + col::STEP2CAP);
   S.xmax = reinterpret_cast<int *>(S.rtab + maxN + 2);
   S.hits = S.xmax + maxN;
@@ -1088,8 +1092,8 @@ cudaError_t launch_pixel(const InsertJob *d_jobs, const int4 *d_work, int nwork,
                          int *d_counter, int maxN, cudaStream_t st) {
   if (nwork == 0) return cudaSuccess;
   const Consts &c = consts();
-  const size_t smem = sizeof(float4) * (col::NV + col::STEP2CAP) + sizeof(float) * (maxN + 2) +
-                      sizeof(int) * maxN + sizeof(int) * block +
+  const size_t smem = sizeof(float) * 3 * col::NV + sizeof(float4) * col::STEP2CAP +
+                      sizeof(float) * (maxN + 2) + sizeof(int) * maxN + sizeof(int) * block +
                       sizeof(int) * (col::NT / 32) * (2 * col::PROWS + 1);
   static size_t configured = 0;
   if (configured < smem) {
