@@ -89,8 +89,9 @@ def _split(ps, meta_fn, a, b):
 
 
 def test_graph_replays_equal_batched_rounds(gpu):
-    """Two replays of a captured round (new particles each time, then the
-    slots as filled) give each job what two batched calls give it."""
+    """Replays of a captured round (device images, host images, the slots as
+    filled, then a mix of device and host images) give each job what the same
+    batched calls give it."""
     import torch
 
     from eman2_b200.batch import BatchReconstructor
@@ -102,13 +103,15 @@ def test_graph_replays_equal_batched_rounds(gpu):
     ctf = [bool(np.any(np.abs(ps.defocus) > 1e-4)) for _, ps, _ in jobs]
     boxes = [ps.images.shape[-1] for _, ps, _ in jobs]
     b1 = BatchReconstructor([p for p, _, _ in jobs])
-    for part in (first, second, second):
+    for part in (first, second, second, first):
         b1.insert_particles([im for im, _ in part], [m for _, m in part])
     b2 = BatchReconstructor([p for p, _, _ in jobs])
     g = b2.capture(boxes, half, ctf)
     g.launch([torch.as_tensor(im, device="cuda") for im, _ in first], [m for _, m in first])
     g.launch([im for im, _ in second], [m for _, m in second])      # host images
     g.launch(None, [m for _, m in second])                           # the slots as filled
+    mixed = [torch.as_tensor(im, device="cuda") if j % 2 else im for j, (im, _) in enumerate(first)]
+    g.launch(mixed, [m for _, m in first])          # device images in place, host ones copied
     torch.cuda.synchronize()
     for j in range(len(jobs)):
         d1, n1 = b1.get_accumulators(j)
