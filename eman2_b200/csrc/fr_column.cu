@@ -678,7 +678,7 @@ constexpr int PROWS = 32;   // rows per row batch of a pass
 struct Smem4 {
   float *are, *aim, *awt;     // accumulators, one array per component [NV]
   int *origin;                // the volume's origin cell got a direct tap (its imag is 0)
-  float4 *steps;
+  float *rexp;                // gauss_2's fast_exp entries, kRexpCopies interleaved copies
   float *rtab;
   int *xmax;
   int *hits;
@@ -687,8 +687,30 @@ struct Smem4 {
   int *rowoff;                 // [NT/32][PROWS + 1]
   int *wcount;
   int *next;                   // next (slice, pass) unit of the work item
-  unsigned long long *state;   // [0] step table loaded (mode), [1] xmax table loaded (address)
+  unsigned long long *state;   // [0] exp copies loaded (mode), [1] xmax table loaded (address)
 };
+
+// gauss_2 taps have r <= 3, so fast_exp(-r*h) only reads entries 0..370 of
+// the 1000-entry table.  Eight interleaved copies, entry g of copy c at
+// 8g + c, with lane l reading copy l & 7: the four lanes that share a copy
+// meet in one bank only when their entries differ by a multiple of 4, so a
+// warp's lookup takes ~2 shared wavefronts instead of the ~4.5 a 16-byte
+// step-table entry took.
+constexpr int kRexpEntries = 376;
+constexpr int kRexpCopies = 8;
+
+// Util::fast_exp(f) for f in [-19.98, 0] read from the interleaved copies
+// (the index arithmetic is fast_exp's, fr_device.cuh).
+__device__ __forceinline__ float rexp_lookup(float f, const float *rexp) {
+  const float y = -f;
+  const float p = __fmul_rn(y, 50.0f);
+  const float e = __fmaf_rn(y, 50.0f, -p);
+  const float q = floorf(p);
+  const float fr = __fsub_rn(p, q);
+  int g = __float_as_int(__fadd_rn(q, 8388608.0f)) - 0x4B000000;
+  g += (fr > 0.5f || (fr == 0.5f && e >= 0.0f)) ? 1 : 0;
+  return rexp[g * kRexpCopies + (threadIdx.x & (kRexpCopies - 1))];
+}
 
 // Slot of local cell (lx, ly, lz) in the component arrays.  Each pair of rows
 // (ly >> 1, lz) fills 32 consecutive words, one per bank; within it the
@@ -731,8 +753,7 @@ __device__ __forceinline__ void tile_tap(const Smem4 &S, int sg, int i, int j, i
 template <int MODE>
 __device__ __forceinline__ void pixel_pass(const InsertJob &J, const Smem4 &S, const float *M,
                                            int sg, const int *base, const int *ext,
-                                           const float2 *__restrict__ sl, float w, float h,
-                                           const ExpSteps &steps) {
+                                           const float2 *__restrict__ sl, float w, float h) {
   constexpr float RLO = Win<MODE>::lo, RHI = Win<MODE>::hi;
   const int N = J.N, n2 = N >> 1;
   const float Nf = (float)N;
@@ -817,7 +838,7 @@ __device__ __forceinline__ void pixel_pass(const InsertJob &J, const Smem4 &S, c
               float vre, vim, vw;
               if (MODE == MODE_GAUSS2) {
                 const float r = __fadd_rn(__fadd_rn(dxx[a], dyy[b]), dzz[c]);
-                const float gg = __fmul_rn(step_exp(r, h, steps, S.steps), w);
+                const float gg = __fmul_rn(rexp_lookup(__fmul_rn(-r, h), S.rexp), w);
                 vre = __fmul_rn(val.x, gg);
                 vim = __fmul_rn(val.y, gg);
                 vw = gg;
@@ -835,7 +856,7 @@ __device__ __forceinline__ void pixel_pass(const InsertJob &J, const Smem4 &S, c
 
 template <int MODE>
 __device__ void tile_item4(const InsertJob &J, int tile, int s0, int s1, const Smem4 &S, float h,
-                           const ExpSteps &steps, int *err) {
+                           const float *__restrict__ exp_g) {
   constexpr float RLO = Win<MODE>::lo, RHI = Win<MODE>::hi;
   const int N = J.N, n2 = N >> 1;
   const int tix = tile % J.tiles_x, tiy = (tile / J.tiles_x) % J.tiles_y,
@@ -878,11 +899,9 @@ __device__ void tile_item4(const InsertJob &J, int tile, int s0, int s1, const S
     for (int i = threadIdx.x; i < N + 2; i += NT) S.rtab[i] = __ldg(&J.rtab[i]);
     for (int i = threadIdx.x; i < N; i += NT) S.xmax[i] = __ldg(&J.xmax[i]);
   }
-  if (MODE == MODE_GAUSS2 && S.state[0] != (unsigned long long)MODE) {
-    const int nb = min(steps.nbins, STEP2CAP);
-    for (int i = threadIdx.x; i < nb; i += NT) S.steps[i] = __ldg(&steps.d_bins[i]);
-    if (threadIdx.x == 0 && steps.nbins > STEP2CAP) atomicOr(err, 8);
-  }
+  if (MODE == MODE_GAUSS2 && S.state[0] != (unsigned long long)MODE)
+    for (int i = threadIdx.x; i < kRexpEntries * kRexpCopies; i += NT)
+      S.rexp[i] = __ldg(&exp_g[i / kRexpCopies]);
   for (int i = threadIdx.x; i < NV; i += NT) {
     S.are[i] = 0.f;
     S.aim[i] = 0.f;
@@ -911,7 +930,7 @@ __device__ void tile_item4(const InsertJob &J, int tile, int s0, int s1, const S
     for (int i = 0; i < 9; i++) M[i] = __ldg(&J.t3d[9 * s + i]);
     const float w = __ldg(&J.pw[p]);
     const float2 *sl = J.slices + (size_t)p * N * w2;
-    pixel_pass<MODE>(J, S, M, (u & 1) ? -1 : 1, base, ext, sl, w, h, steps);
+    pixel_pass<MODE>(J, S, M, (u & 1) ? -1 : 1, base, ext, sl, w, h);
   }
   __syncthreads();
   // ---- flush (as tile_item3)
@@ -1048,7 +1067,8 @@ cudaError_t launch_column3(const InsertJob *d_jobs, const int4 *d_work, int nwor
 
 __global__ void __launch_bounds__(col::NT, 3)
     k_pixel(const InsertJob *__restrict__ jobs, const int4 *__restrict__ work, int nwork,
-            int block, int *counter, float h2, ExpSteps st2, int maxN, int *err) {
+            int block, int *counter, float h2, const float *__restrict__ exp_g, int maxN,
+            int *err) {
   extern __shared__ float4 s_dyn[];
   __shared__ int s_work;
   __shared__ int s_wcount[col::NT / 32];
@@ -1059,8 +1079,8 @@ __global__ void __launch_bounds__(col::NT, 3)
   S.aim = S.are + col::NV;
   S.awt = S.aim + col::NV;
   S.origin = &s_origin;
-  S.steps = reinterpret_cast<float4 *>(S.awt + col::NV);
-  S.rtab = reinterpret_cast<float *>(S.steps + col::STEP2CAP);
+  S.rexp = S.awt + col::NV;
+  S.rtab = S.rexp + col::kRexpEntries * col::kRexpCopies;
   S.xmax = reinterpret_cast<int *>(S.rtab + maxN + 2);
   S.hits = S.xmax + maxN;
   S.rowc0 = S.hits + block;
@@ -1079,9 +1099,9 @@ __global__ void __launch_bounds__(col::NT, 3)
     const InsertJob J = jobs[wk.x];
     const int s0 = wk.z, s1 = min(min(wk.w, wk.z + block), J.np * J.nsym);
     switch (J.mode) {
-      case MODE_GAUSS2: col::tile_item4<MODE_GAUSS2>(J, wk.y, s0, s1, S, h2, st2, err); break;
-      case MODE_NEAREST: col::tile_item4<MODE_NEAREST>(J, wk.y, s0, s1, S, h2, st2, err); break;
-      case MODE_TRILINEAR: col::tile_item4<MODE_TRILINEAR>(J, wk.y, s0, s1, S, h2, st2, err); break;
+      case MODE_GAUSS2: col::tile_item4<MODE_GAUSS2>(J, wk.y, s0, s1, S, h2, exp_g); break;
+      case MODE_NEAREST: col::tile_item4<MODE_NEAREST>(J, wk.y, s0, s1, S, h2, exp_g); break;
+      case MODE_TRILINEAR: col::tile_item4<MODE_TRILINEAR>(J, wk.y, s0, s1, S, h2, exp_g); break;
       default:
         if (threadIdx.x == 0) atomicOr(err, 4);   // gauss_5 takes the column kernel
     }
@@ -1092,7 +1112,8 @@ cudaError_t launch_pixel(const InsertJob *d_jobs, const int4 *d_work, int nwork,
                          int *d_counter, int maxN, cudaStream_t st) {
   if (nwork == 0) return cudaSuccess;
   const Consts &c = consts();
-  const size_t smem = sizeof(float) * 3 * col::NV + sizeof(float4) * col::STEP2CAP +
+  const size_t smem = sizeof(float) * 3 * col::NV +
+                      sizeof(float) * col::kRexpEntries * col::kRexpCopies +
                       sizeof(float) * (maxN + 2) + sizeof(int) * maxN + sizeof(int) * block +
                       sizeof(int) * (col::NT / 32) * (2 * col::PROWS + 1);
   static size_t configured = 0;
@@ -1109,7 +1130,7 @@ cudaError_t launch_pixel(const InsertJob *d_jobs, const int4 *d_work, int nwork,
   if (per_sm < 1) per_sm = 1;
   const int grid = std::max(1, std::min(nwork, sms * per_sm));
   note_launch();
-  k_pixel<<<grid, col::NT, smem, st>>>(d_jobs, d_work, nwork, block, d_counter, c.h2, c.steps2,
+  k_pixel<<<grid, col::NT, smem, st>>>(d_jobs, d_work, nwork, block, d_counter, c.h2, c.d_exp,
                                        maxN, c.d_err);
   return cudaGetLastError();
 }
