@@ -683,8 +683,6 @@ struct Smem4 {
   int *xmax;
   int *hits;
   int *tmp;
-  int *rowc0;                  // [NT/32][PROWS]
-  int *rowoff;                 // [NT/32][PROWS + 1]
   int *wcount;
   int *next;                   // next (slice, pass) unit of the work item
   unsigned long long *state;   // [0] exp copies loaded (mode), [1] xmax table loaded (address)
@@ -757,9 +755,7 @@ __device__ __forceinline__ void pixel_pass(const InsertJob &J, const Smem4 &S, c
   constexpr float RLO = Win<MODE>::lo, RHI = Win<MODE>::hi;
   const int N = J.N, n2 = N >> 1;
   const float Nf = (float)N;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  int *c0s = S.rowc0 + warp * PROWS;
-  int *offs = S.rowoff + warp * (PROWS + 1);
+  const int lane = threadIdx.x & 31;
   float lo[3], hi[3];
 #pragma unroll
   for (int a = 0; a < 3; a++) {
@@ -791,25 +787,48 @@ __device__ __forceinline__ void pixel_pass(const InsertJob &J, const Smem4 &S, c
       const int c1 = min(S.xmax[y + n2], (int)floorf(xhi));
       cnt = max(0, c1 - c0 + 1);
     }
-    int incl = cnt;
+    // ---- the batch's nonempty rows, compacted: lane j holds the j-th one
+    // (its row in the batch, first pixel column, pixel count, first pixel)
+    const unsigned full = 0xffffffffu;
+    const unsigned ne = __ballot_sync(full, cnt > 0);
+    const int nrows = __popc(ne);
+    int src;
+    {
+      int lo = 0, hi = 31;   // position of the (lane+1)-th set bit of ne
+      while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (__popc(ne & ((2u << mid) - 1u)) >= lane + 1) hi = mid;
+        else lo = mid + 1;
+      }
+      src = lo;
+    }
+    const int rc0 = __shfl_sync(full, c0, src);
+    int rcnt = __shfl_sync(full, cnt, src);
+    if (lane >= nrows) rcnt = 0;
+    int incl = rcnt;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-      const int t = __shfl_up_sync(0xffffffffu, incl, o);
+      const int t = __shfl_up_sync(full, incl, o);
       if (lane >= o) incl += t;
     }
-    const int total = __shfl_sync(0xffffffffu, incl, 31);
-    c0s[lane] = c0;
-    offs[lane] = incl - cnt;
-    if (lane == 31) offs[PROWS] = total;
-    __syncwarp();
-    // ---- the pixels of the batch, one per lane
-    for (int idx = lane; idx < total; idx += 32) {
-      int row = 0;
-#pragma unroll
-      for (int step = 16; step > 0; step >>= 1)
-        if (offs[row + step] <= idx) row += step;
-      const int x = c0s[row] + (idx - offs[row]);
-      const int py = rb + row;
+    const int total = __shfl_sync(full, incl, 31);
+    const int rstart = incl - rcnt;
+    // ---- the pixels of the batch, one per lane.  The row of pixel wb+lane:
+    // the row holding pixel wb, plus the rows starting in (wb, wb+lane], read
+    // from a mask of the row starts inside the window (registers only).
+    for (int wb = 0; wb < total; wb += 32) {
+      const bool real = lane < nrows;
+      const unsigned le = __ballot_sync(full, real && rstart <= wb);
+      const int kb = 31 - __clz(le);
+      const unsigned bit = (real && rstart > wb && rstart < wb + 32) ? (1u << (rstart - wb)) : 0u;
+      const unsigned starts = __reduce_or_sync(full, bit);
+      const int kr = kb + __popc(starts & ((2u << lane) - 1u));
+      const int kx0 = __shfl_sync(full, rc0, kr), ks = __shfl_sync(full, rstart, kr),
+                krow = __shfl_sync(full, src, kr);
+      const int idx = wb + lane;
+      if (idx >= total) continue;
+      const int x = kx0 + (idx - ks);
+      const int py = rb + krow;
       float xx, yy, zz;
       pixel_coords(S.rtab[x + n2], S.rtab[py + n2], M, Nf, xx, yy, zz);
       const float2 val = slice_value(sl, N, x, py);
@@ -1083,8 +1102,6 @@ __global__ void __launch_bounds__(col::NT, 3)
   S.rtab = S.rexp + col::kRexpEntries * col::kRexpCopies;
   S.xmax = reinterpret_cast<int *>(S.rtab + maxN + 2);
   S.hits = S.xmax + maxN;
-  S.rowc0 = S.hits + block;
-  S.rowoff = S.rowc0 + (col::NT / 32) * col::PROWS;
   S.wcount = s_wcount;
   S.next = &s_next;
   S.state = s_state;
@@ -1114,8 +1131,7 @@ cudaError_t launch_pixel(const InsertJob *d_jobs, const int4 *d_work, int nwork,
   const Consts &c = consts();
   const size_t smem = sizeof(float) * 3 * col::NV +
                       sizeof(float) * col::kRexpEntries * col::kRexpCopies +
-                      sizeof(float) * (maxN + 2) + sizeof(int) * maxN + sizeof(int) * block +
-                      sizeof(int) * (col::NT / 32) * (2 * col::PROWS + 1);
+                      sizeof(float) * (maxN + 2) + sizeof(int) * maxN + sizeof(int) * block;
   static size_t configured = 0;
   if (configured < smem) {
     cudaFuncSetAttribute(k_pixel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
