@@ -60,7 +60,7 @@ def test_batch_equals_each_job_alone(gpu):
 
 
 def test_autotune_and_mixed_schedules_in_one_batch(gpu):
-    """The autotuner times all seven schedules; with each job pinned to a
+    """The autotuner times every schedule; with each job pinned to a
     different one, the batch still gives every job its alone result."""
     from eman2_b200.batch import BatchReconstructor, autotune, set_tile
     tile, ms = autotune(48, "gauss_2", 1, nparticles=64)
