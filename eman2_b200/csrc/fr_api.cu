@@ -319,9 +319,12 @@ int stream_leave(fr_recon *r, cudaStream_t st) {
   return FR_OK;
 }
 
-int stream_leave_all(const std::vector<fr_recon *> &rs, cudaStream_t st) {
+int stream_leave_all(const std::vector<fr_recon *> &rs, cudaStream_t st,
+                     std::shared_ptr<SharedEvent> *reuse) {
   std::shared_ptr<SharedEvent> e;
-  TRY(new_event(e));
+  if (reuse && *reuse) e = *reuse;
+  else TRY(new_event(e));
+  if (reuse) *reuse = e;
   CU(cudaEventRecord(e->ev, st));
   for (fr_recon *r : rs) {
     r->done = e;

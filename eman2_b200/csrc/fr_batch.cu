@@ -547,6 +547,7 @@ struct fr_graph {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   cudaGraphNode_t meta_node = nullptr;   // the metadata upload, the graph's first node
+  std::shared_ptr<fr::SharedEvent> after; // recorded after each replay, held by the handles
   std::mutex mu;
 };
 
@@ -818,7 +819,7 @@ int fr_graph_launch(fr_graph *g, const float *const *imgs, const fr_particle *co
   CU(cudaEventRecord(g->staged[k], st));
   g->staged_used[k] = true;
   note_launch((int)g->kernels);
-  TRY(stream_leave_all(g->jobs, st));
+  TRY(stream_leave_all(g->jobs, st, &g->after));
   if (host_src) CU(cudaStreamSynchronize(st));   // host images may be pinned: read them first
   return FR_OK;
 }

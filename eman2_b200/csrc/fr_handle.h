@@ -289,7 +289,11 @@ int stream_enter(fr_recon *r, cudaStream_t st);
 // Marks the end of the handle's work enqueued so far on st.
 int stream_leave(fr_recon *r, cudaStream_t st);
 // The same for many handles whose work went to st: one event for all.
-int stream_leave_all(const std::vector<fr_recon *> &rs, cudaStream_t st);
+// reuse: a caller that always leaves on the same stream may keep the event
+// and have it recorded again (handles that still hold it from an earlier call
+// then wait for a later point of that stream, which includes their work).
+int stream_leave_all(const std::vector<fr_recon *> &rs, cudaStream_t st,
+                     std::shared_ptr<SharedEvent> *reuse = nullptr);
 InsertJob make_job(fr_recon *r, const float2 *slices, const float *t3d, const float *pw, int np);
 int run_scatter(const InsertJob &j0, bool edge_only, cudaStream_t st);
 int insert_device(fr_recon *r, const float2 *d_slices, const float *d_t3d, const float *d_pw, int np,
