@@ -1065,11 +1065,8 @@ cudaError_t launch_column3(const InsertJob *d_jobs, const int4 *d_work, int nwor
   const Consts &c = consts();
   const size_t smem = sizeof(float4) * (col::NV + col::STEP2CAP) + sizeof(float) * 1000 +
                       sizeof(float) * (maxN + 2) + sizeof(int) * maxN + 2 * sizeof(int) * block;
-  static size_t configured = 0;
-  if (configured < smem) {
-    cudaFuncSetAttribute(k_column3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    configured = smem;
-  }
+  cudaError_t ea = set_max_smem((const void *)k_column3, smem);
+  if (ea != cudaSuccess) return ea;
   cudaError_t e = zero_counter(d_counter, st);
   if (e != cudaSuccess) return e;
   int dev = 0, sms = 148, per_sm = 1;
@@ -1132,11 +1129,8 @@ cudaError_t launch_pixel(const InsertJob *d_jobs, const int4 *d_work, int nwork,
   const size_t smem = sizeof(float) * 3 * col::NV +
                       sizeof(float) * col::kRexpEntries * col::kRexpCopies +
                       sizeof(float) * (maxN + 2) + sizeof(int) * maxN + sizeof(int) * block;
-  static size_t configured = 0;
-  if (configured < smem) {
-    cudaFuncSetAttribute(k_pixel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    configured = smem;
-  }
+  cudaError_t ea = set_max_smem((const void *)k_pixel, smem);
+  if (ea != cudaSuccess) return ea;
   cudaError_t e = zero_counter(d_counter, st);
   if (e != cudaSuccess) return e;
   int dev = 0, sms = 148, per_sm = 1;
@@ -1170,11 +1164,8 @@ cudaError_t launch_column(const InsertJob *d_jobs, const int4 *d_work, int nwork
   const Consts &c = consts();
   const int side = column_side(max_mode);
   const size_t smem = column_smem(side, block);
-  static size_t configured = 0;
-  if (configured < smem) {
-    cudaFuncSetAttribute(k_column, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    configured = smem;
-  }
+  cudaError_t ea = set_max_smem((const void *)k_column, smem);
+  if (ea != cudaSuccess) return ea;
   cudaError_t e = zero_counter(d_counter, st);
   if (e != cudaSuccess) return e;
   int dev = 0, sms = 148, per_sm = 1;

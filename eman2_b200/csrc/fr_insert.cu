@@ -19,6 +19,8 @@
 //                  pixels, with atomics.  Those taps write only face cells,
 //                  which the gather kernel never touches, and vice versa.
 #include <algorithm>
+#include <map>
+#include <mutex>
 #include <cmath>
 #include <cstdio>
 
@@ -221,6 +223,20 @@ __device__ __forceinline__ float pixel_weight(const InsertJob &J, int p, int x, 
 // Resets a persistent launch's work counter.  A kernel rather than a memset:
 // on the copy engine a memset would queue behind uploads of other streams.
 __global__ void k_zero_int(int *p) { *p = 0; }
+
+cudaError_t set_max_smem(const void *func, size_t smem) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  static std::mutex mu;
+  static std::map<std::pair<const void *, int>, size_t> done;
+  std::lock_guard<std::mutex> lk(mu);
+  size_t &have = done[std::make_pair(func, dev)];
+  if (have >= smem) return cudaSuccess;
+  e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess) have = smem;
+  return e;
+}
 
 cudaError_t zero_counter(int *d_counter, cudaStream_t st) {
   note_launch();
@@ -764,11 +780,8 @@ static cudaError_t launch_gather_t(const InsertJob *d_jobs, int nwork, const int
                                    int *d_counter, int side, int max_mode, cudaStream_t st) {
   const Consts &c = consts();
   const size_t smem = (size_t)side * side * (sizeof(float4) + sizeof(float2));
-  static int configured = 0;
-  if (configured < (int)smem) {
-    cudaFuncSetAttribute(k_gather<TX, TY, TZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    configured = (int)smem;
-  }
+  cudaError_t ea = set_max_smem((const void *)k_gather<TX, TY, TZ>, smem);
+  if (ea != cudaSuccess) return ea;
   int dev = 0, sms = 148, per_sm = 1;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);

@@ -58,6 +58,9 @@ struct InsertJob {
 // Launch accounting (fr_api.cu).
 void note_launch(int n = 1);
 cudaError_t zero_counter(int *d_counter, cudaStream_t st);
+// Raises kernel func's dynamic shared-memory limit on the current device to
+// at least smem bytes (the attribute is per device; set once per size).
+cudaError_t set_max_smem(const void *func, size_t smem);
 long long launches_noted();
 
 // fast_exp(-r*h) as a function of r: the table index is monotone in r, so
