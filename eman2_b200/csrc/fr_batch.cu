@@ -510,7 +510,12 @@ int fr_insert_particles_multi(fr_recon *const *handles, int nh, const float *con
     if (!r) return fail(FR_ENULL, "null reconstructor handle");
   std::vector<std::unique_lock<std::mutex>> locks;
   TRY(lock_handles(jobs, locks));
-  static thread_local BatchScratch bs;
+  // this thread's scratch on the current device (its buffers and events
+  // belong to one device)
+  int dev = 0;
+  CU(cudaGetDevice(&dev));
+  static thread_local std::map<int, BatchScratch> scratch;
+  BatchScratch &bs = scratch[dev];
   cudaStream_t st = stream ? (cudaStream_t)stream : jobs[0]->stream;
   return batch_insert(jobs, bs, -1, st, imgs, boxes, counts, meta);
 }
