@@ -183,3 +183,26 @@ def test_scheduler_joins_late_arrivals_at_next_tick():
     assert len(sched.tick_work()) == 1
     sched.admit(0.6, exe)                  # arrived while job 0 was on the GPU
     assert len(sched.tick_work()) == 2     # both in the same tick now
+
+
+def test_batched_call_argument_marshalling():
+    """The batched calls hand the library contiguous float32 particles and the
+    addresses of fr_particle arrays: float32 contiguous tensors pass through
+    untouched, other arrays are converted, None stays None."""
+    import torch
+
+    from eman2_b200.batch import _meta_address, _particles
+    from eman2_b200.particles import particle_meta
+    t32 = torch.zeros(2, 4, 4)
+    a64 = np.arange(32, dtype=np.float64).reshape(2, 4, 4)
+    strided = torch.zeros(2, 4, 8)[:, :, ::2]
+    keep, ptrs = _particles([t32, a64, None, strided])
+    assert keep[0] is t32 and ptrs[0] == t32.data_ptr()
+    assert keep[1].dtype == np.float32 and keep[1].flags["C_CONTIGUOUS"]
+    assert np.array_equal(keep[1], a64.astype(np.float32)) and ptrs[1] == keep[1].ctypes.data
+    assert keep[2] is None and ptrs[2] is None
+    assert keep[3].is_contiguous() and ptrs[3] == keep[3].data_ptr()
+    meta = particle_meta(np.eye(3, dtype=np.float32)[None], np.zeros((1, 2), np.float32),
+                         np.ones(1, np.float32))
+    assert _meta_address(meta) == ctypes.cast(meta, ctypes.c_void_p).value
+    assert _meta_address(None) is None
