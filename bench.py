@@ -426,8 +426,8 @@ def run_io(dev, wl: dict, n: int = 16384, chunk: int = 4096):
 
 # ------------------------------------------------------------------ batched
 def run_batched(dev, seed: int = 33, pairs: int = 32, reps: int = 5, plain_sample: int = 16):
-    """The batched form on a round of SURVEY config 3's shape: 32 even/odd
-    half-map pairs (64 reconstructions), boxes {64, 96, 128, 160} padded x1.5,
+    """The batched form on a round of 64 reconstructions: 32 even/odd
+    half-map pairs, boxes {64, 96, 128, 160} padded x1.5,
     sym c1/d7, gauss_2/gauss_5 (each 50/50), CTF; per round every job inserts
     a chunk of log-uniform [64, 512] particles.  Schedules come from the
     autotuner; the round is captured once as a CUDA graph and replayed.
