@@ -598,7 +598,6 @@ int prologue_run(PlanCache &plans, const ProScratch &b, const unsigned char *d_m
   const MetaView mv = meta_view(d_meta, n);
   TRY(b.img->ensure(sizeof(float) * img * n));
   TRY(b.slices->ensure(sizeof(float) * slice_floats(N) * n));
-  TRY(b.mean->ensure(sizeof(float) * n));
   TRY(b.spec->ensure(std::max(sizeof(cufftComplex) * spec, sizeof(float) * img) * n));
   TRY(b.t3d->ensure(sizeof(float) * 9 * (size_t)n * nsym));
   if (any_ctf) TRY(b.img2->ensure(sizeof(float) * img * n));
@@ -611,25 +610,19 @@ int prologue_run(PlanCache &plans, const ProScratch &b, const unsigned char *d_m
     TRY(plans.exec2d(false, N, n, b.spec->p, b.img2->p, st, exact_fft));
     img_on = b.img2->as<float>();
   }
-  // edge mean; preprocess_slice: shift, phase origin to corner,
-  // x sqrt((N+2)/N), r2c.  spec is the real staging for the r2c input.
+  // edge mean (in the shift kernel); preprocess_slice: shift, phase origin
+  // to corner, x sqrt((N+2)/N), r2c.  spec is the real staging for the r2c
+  // input.
   volatile float inv = 1.0f / (float)N;
   const float scale = sqrtf(inv * (float)(N + 2));
-  if (mean_shift_fused(n, N)) {
-    CU(launch_mean_shift_corner(b.img->as<float>(), img_on, any_ctf ? mv.ctf : nullptr, mv.txy, 2,
-                                n, N, scale, b.spec->as<float>(), st));
-  } else {
-    CU(launch_edge_mean(b.img->as<float>(), img_on, any_ctf ? mv.ctf : nullptr, n, N,
-                        b.mean->as<float>(), st));
-    CU(launch_shift_corner(b.img->as<float>(), img_on, any_ctf ? mv.ctf : nullptr,
-                           b.mean->as<float>(), mv.txy, 2, n, N, scale, b.spec->as<float>(), st));
-  }
+  CU(launch_shift_corner(b.img->as<float>(), img_on, any_ctf ? mv.ctf : nullptr, nullptr, mv.txy,
+                         2, n, N, scale, b.spec->as<float>(), st, true));
   TRY(plans.exec2d(true, N, n, b.spec->p, b.slices->p, st, exact_fft));
   return FR_OK;
 }
 
 int prologue_device(fr_recon *r, const float *d_raw, int n, int box, bool any_ctf) {
-  const ProScratch b{&r->s_img, &r->s_slices, &r->s_mean, &r->s_spec, &r->s_t3d, &r->s_img2};
+  const ProScratch b{&r->s_img, &r->s_slices, &r->s_spec, &r->s_t3d, &r->s_img2};
   return prologue_run(r->plans, b, r->d_meta, d_raw, nullptr, n, box, r->N, r->d_sym.as<float>(),
                       r->nsym, any_ctf, r->stream);
 }
@@ -750,7 +743,7 @@ int fr_destroy(fr_recon *r) {
     DevBuf *bufs[] = {&r->vol_data, &r->vol_norm, &r->d_sym, &r->s_in, &r->s_slices, &r->s_rot,
                       &r->s_meta, &r->ref,
                       &r->s_w, &r->s_t3d, &r->s_img, &r->s_img2, &r->s_spec, &r->s_ctf,
-                      &r->s_mean, &r->s_txy, &r->s_out, &r->s_ssnr, &r->s_jobs, &r->s_work,
+                      &r->s_txy, &r->s_out, &r->s_ssnr, &r->s_jobs, &r->s_work,
                       &r->s_counter};
     for (DevBuf *b : bufs) b->release();
     for (int k = 0; k < 2; k++) {

@@ -49,10 +49,10 @@ int default_tile(int mode, int N, int nsym, int np) {
 namespace fr {
 // Scratch of one prologue group (see ProGroup).
 struct ProBufs {
-  DevBuf img, slices, mean, spec, t3d, img2;
-  ProScratch view() { return {&img, &slices, &mean, &spec, &t3d, &img2}; }
+  DevBuf img, slices, spec, t3d, img2;
+  ProScratch view() { return {&img, &slices, &spec, &t3d, &img2}; }
   void release() {
-    for (DevBuf *b : {&img, &slices, &mean, &spec, &t3d, &img2}) b->release();
+    for (DevBuf *b : {&img, &slices, &spec, &t3d, &img2}) b->release();
   }
 };
 

@@ -248,7 +248,7 @@ struct fr_recon {
   float wfilt = 0.0f;         // 1: Wiener normalisation, data / (weight + 1)
   fr::DevBuf vol_data, vol_norm, d_sym;
   // scratch
-  fr::DevBuf s_in, s_slices, s_rot, s_w, s_t3d, s_img, s_img2, s_spec, s_ctf, s_mean, s_txy, s_out,
+  fr::DevBuf s_in, s_slices, s_rot, s_w, s_t3d, s_img, s_img2, s_spec, s_ctf, s_txy, s_out,
       s_ssnr, s_jobs, s_work, s_counter;
   fr::PlanCache plans;
   int tile = -1;              // gather tile shape (-1: tuned default)
@@ -316,10 +316,10 @@ struct MetaView {
   const float *txy, *w, *rot;
 };
 MetaView meta_view(const unsigned char *d_meta, int n);
-// Scratch of one prologue run: padded images, spectra (and the r2c input),
-// the CTF round trip's images, edge means, slices, composed rotations.
+// Scratch of one prologue run: padded images, slices, spectra (and the r2c
+// input), composed rotations, the CTF round trip's images.
 struct ProScratch {
-  DevBuf *img, *slices, *mean, *spec, *t3d, *img2;
+  DevBuf *img, *slices, *spec, *t3d, *img2;
 };
 // The device half of a prologue over n particles of size box into slices of
 // size N: metadata block (prologue_meta layout) at d_meta, raw images at

@@ -159,18 +159,13 @@ void ctf_constants(float defocus, float dfdiff, float dfang, float voltage, floa
 size_t ctf_dev_size();
 cudaError_t launch_ctf_flip_dev(cufftComplex *d_spec, const void *d_ctf, int n, int N,
                                 cudaStream_t st);
-cudaError_t launch_edge_mean(const float *d_img_off, const float *d_img_on, const void *d_ctf,
-                             int n, int N, float *d_mean, cudaStream_t st);
+// Shift, phase origin to corner and scale of n images of size N.  fuse_mean:
+// each block forms its particle's edge mean from the selected image (the
+// same value in every block) instead of reading d_mean.
 cudaError_t launch_shift_corner(const float *d_img_off, const float *d_img_on, const void *d_ctf,
                                 const float *d_mean, const float *d_txy, int txy_stride, int n,
-                                int N, float scale_out, float *d_out, cudaStream_t st);
-// Edge mean and shift in one launch (each block forms its particle's edge
-// mean); chosen by mean_shift_fused(n, N) for launches small enough that the
-// repeated reductions cost less than a kernel.
-bool mean_shift_fused(int n, int N);
-cudaError_t launch_mean_shift_corner(const float *d_img_off, const float *d_img_on,
-                                     const void *d_ctf, const float *d_txy, int txy_stride, int n,
-                                     int N, float scale_out, float *d_out, cudaStream_t st);
+                                int N, float scale_out, float *d_out, cudaStream_t st,
+                                bool fuse_mean = false);
 
 // Finish / agreement (fr_finish.cu).
 cudaError_t launch_normalize(float *d_data, float *d_norm, int N, int sqrtnorm, cudaStream_t st,

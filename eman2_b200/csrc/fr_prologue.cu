@@ -121,13 +121,21 @@ __device__ __forceinline__ float hypot_int(int x, int y) {
 // correctly rounded float cosine returns.
 struct CtfDev { float g1, g2, acac, ds, defocus, dfdiff, dfang, on; };
 
-__global__ void k_ctf_flip(cufftComplex *__restrict__ spec, const CtfDev *__restrict__ c, int N) {
+// Blocks of 256 threads per particle for a launch over n particles of npx
+// elements each: about `waves` blocks per SM in all, at most one element
+// per thread.  Few particles get many blocks each; many get one.
+static int blocks_per_particle(int n, int npx, int waves) {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const long want = ((long)waves * sms + n - 1) / n;
+  return (int)std::max(1L, std::min<long>(want, (npx + 255) / 256));
+}
+
+// One spectrum element i of a particle: x CTF_SIGN at its frequency.
+__device__ __forceinline__ void flip_one(cufftComplex *__restrict__ spec, const CtfDev &k, int N,
+                                         int i) {
   const int w = N / 2 + 1;
-  const int p = blockIdx.y;
-  const CtfDev k = c[p];
-  if (k.on == 0.0f) return;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= N * w) return;
   const int r = i / w, x = i % w;
   const int y = r < N / 2 ? r : r - N;
   const float s = __fmul_rn(hypot_int(x, y), k.ds);
@@ -143,17 +151,28 @@ __global__ void k_ctf_flip(cufftComplex *__restrict__ spec, const CtfDev *__rest
   }
   const double v = cos((double)__fsub_rn(gam, k.acac));
   const float sg = v < 0.0 ? -1.0f : 1.0f;
-  cufftComplex z = spec[(size_t)p * N * w + i];
+  cufftComplex z = spec[i];
   z.x = __fmul_rn(z.x, sg);
   z.y = __fmul_rn(z.y, sg);
-  spec[(size_t)p * N * w + i] = z;
+  spec[i] = z;
+}
+
+// grid.y = particle; the grid.x blocks of a particle stride over its
+// N*(N/2+1) spectrum.
+__global__ void k_ctf_flip(cufftComplex *__restrict__ spec, const CtfDev *__restrict__ c, int N) {
+  const int w = N / 2 + 1;
+  const int p = blockIdx.y;
+  const CtfDev k = c[p];
+  if (k.on == 0.0f) return;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N * w; i += gridDim.x * blockDim.x)
+    flip_one(spec + (size_t)p * N * w, k, N, i);
 }
 
 cudaError_t launch_ctf_flip_dev(cufftComplex *d_spec, const void *d_ctf, int n, int N,
                                 cudaStream_t st) {
   if (n == 0) return cudaSuccess;
   const int w = N / 2 + 1;
-  dim3 grid((N * w + 255) / 256, n);
+  dim3 grid(blocks_per_particle(n, N * w, 8), n);
   note_launch();
   k_ctf_flip<<<grid, 256, 0, st>>>(d_spec, reinterpret_cast<const CtfDev *>(d_ctf), N);
   return cudaGetLastError();
@@ -196,23 +215,6 @@ struct SrcSel {
   }
 };
 
-// Per-particle edge mean of the selected image (after its scaling).
-__global__ void __launch_bounds__(256) k_edge_mean(SrcSel sel, int N, float *__restrict__ mean) {
-  __shared__ double s_red[8];
-  const int p = blockIdx.x;
-  const float m = edge_mean_dev(sel.img(p, (size_t)N * N), N, N, sel.scale(p), s_red);
-  if (threadIdx.x == 0) mean[p] = m;
-}
-
-cudaError_t launch_edge_mean(const float *d_img_off, const float *d_img_on, const void *d_ctf,
-                             int n, int N, float *d_mean, cudaStream_t st) {
-  if (n == 0) return cudaSuccess;
-  SrcSel sel{d_img_off, d_img_on, reinterpret_cast<const CtfDev *>(d_ctf),
-             1.0f / ((float)N * (float)N)};
-  note_launch();
-  k_edge_mean<<<n, 256, 0, st>>>(sel, N, d_mean);
-  return cudaGetLastError();
-}
 
 // src(k) = (v_k * scale_in) - mean: the image after do_ift's scaling and the
 // second edge-mean subtraction.
@@ -224,86 +226,70 @@ __device__ __forceinline__ float src_at(const float *img, size_t k, float scale_
 // inverse translation (tx, ty), then phase origin to corner, then x scale_out
 // (the sqrt((N+2)/N) factor, applied before the r2c instead of after it).
 // txy == nullptr or |t| < 1e-6 (Transform::is_identity) copies.
-// fuse_mean: each block forms its particle's edge mean itself (as
-// k_edge_mean does, same partition and order, so the same value): for small
-// launches, where one kernel fewer matters more than the repeated border reads.
+// fuse_mean: each block forms its particle's edge mean itself (the same
+// partition and summation order in every block, so the same value) instead
+// of reading mean[p].  grid.y = particle; the grid.x blocks of a particle
+// stride over its N*N pixels, so the edge-mean reduction is paid once per
+// block, not once per 256 pixels.
 __global__ void __launch_bounds__(256) k_shift_corner(SrcSel sel, const float *__restrict__ mean,
                                                       const float *__restrict__ txy,
                                                       int txy_stride, int N, float scale_out,
                                                       float *__restrict__ out, int fuse_mean) {
   __shared__ double s_red[8];
   const int p = blockIdx.y;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const float *src = sel.img(p, (size_t)N * N);
   const float scale_in = sel.scale(p);
   const float m = fuse_mean ? edge_mean_dev(src, N, N, scale_in, s_red) : (mean ? mean[p] : 0.0f);
-  if (i >= N * N) return;
-  const int yo = i / N, xo = i % N;
-  const int h = N / 2;
-  // phase origin to corner (even N): out[y][x] = in[(y+N/2)%N][(x+N/2)%N]
-  const int j = (yo + h) % N, ii = (xo + h) % N;
   float tx = 0.f, ty = 0.f;
   if (txy) { tx = txy[(size_t)p * txy_stride]; ty = txy[(size_t)p * txy_stride + 1]; }
-  float v;
-  if (fabsf(tx) < 1e-6f && fabsf(ty) < 1e-6f) {
-    v = src_at(src, (size_t)j * N + ii, scale_in, m);
-  } else {
-    const float cx = (float)(ii - h), cy = (float)(j - h);
-    const float sx = __fadd_rn(__fadd_rn(__fmul_rn(1.0f, cx), __fmul_rn(0.0f, cy)), tx);
-    const float sy = __fadd_rn(__fadd_rn(__fmul_rn(0.0f, cx), __fmul_rn(1.0f, cy)), ty);
-    const float x2 = __fadd_rn(sx, (float)h), y2 = __fadd_rn(sy, (float)h);
-    if (x2 < 0 || x2 >= N || y2 < 0 || y2 >= N) {
-      v = 0.0f;
+  const bool copy = fabsf(tx) < 1e-6f && fabsf(ty) < 1e-6f;
+  const int h = N / 2;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N * N; i += gridDim.x * blockDim.x) {
+    const int yo = i / N, xo = i % N;
+    // phase origin to corner (even N): out[y][x] = in[(y+N/2)%N][(x+N/2)%N]
+    const int j = (yo + h) % N, ii = (xo + h) % N;
+    float v;
+    if (copy) {
+      v = src_at(src, (size_t)j * N + ii, scale_in, m);
     } else {
-      const int ix = (int)x2, jy = (int)y2;
-      int k0 = ix + jy * N, k1 = k0 + 1, k2 = k0 + N, k3 = k0 + N + 1;
-      if (ix == N - 1) { k1--; k3--; }
-      if (jy == N - 1) { k2 -= N; k3 -= N; }
-      const float t = __fsub_rn(x2, (float)ix), u = __fsub_rn(y2, (float)jy);
-      const float p1 = src_at(src, k0, scale_in, m), p2 = src_at(src, k1, scale_in, m);
-      const float p3 = src_at(src, k2, scale_in, m), p4 = src_at(src, k3, scale_in, m);
-      const float omt = __fsub_rn(1.0f, t), omu = __fsub_rn(1.0f, u);
-      float a = __fmul_rn(__fmul_rn(omt, omu), p1);
-      a = __fadd_rn(a, __fmul_rn(__fmul_rn(t, omu), p2));
-      a = __fadd_rn(a, __fmul_rn(__fmul_rn(omt, u), p3));
-      a = __fadd_rn(a, __fmul_rn(__fmul_rn(t, u), p4));
-      v = a;
+      const float cx = (float)(ii - h), cy = (float)(j - h);
+      const float sx = __fadd_rn(__fadd_rn(__fmul_rn(1.0f, cx), __fmul_rn(0.0f, cy)), tx);
+      const float sy = __fadd_rn(__fadd_rn(__fmul_rn(0.0f, cx), __fmul_rn(1.0f, cy)), ty);
+      const float x2 = __fadd_rn(sx, (float)h), y2 = __fadd_rn(sy, (float)h);
+      if (x2 < 0 || x2 >= N || y2 < 0 || y2 >= N) {
+        v = 0.0f;
+      } else {
+        const int ix = (int)x2, jy = (int)y2;
+        int k0 = ix + jy * N, k1 = k0 + 1, k2 = k0 + N, k3 = k0 + N + 1;
+        if (ix == N - 1) { k1--; k3--; }
+        if (jy == N - 1) { k2 -= N; k3 -= N; }
+        const float t = __fsub_rn(x2, (float)ix), u = __fsub_rn(y2, (float)jy);
+        const float p1 = src_at(src, k0, scale_in, m), p2 = src_at(src, k1, scale_in, m);
+        const float p3 = src_at(src, k2, scale_in, m), p4 = src_at(src, k3, scale_in, m);
+        const float omt = __fsub_rn(1.0f, t), omu = __fsub_rn(1.0f, u);
+        float a = __fmul_rn(__fmul_rn(omt, omu), p1);
+        a = __fadd_rn(a, __fmul_rn(__fmul_rn(t, omu), p2));
+        a = __fadd_rn(a, __fmul_rn(__fmul_rn(omt, u), p3));
+        a = __fadd_rn(a, __fmul_rn(__fmul_rn(t, u), p4));
+        v = a;
+      }
     }
+    out[(size_t)p * N * N + i] = __fmul_rn(v, scale_out);
   }
-  out[(size_t)p * N * N + i] = __fmul_rn(v, scale_out);
 }
 
 cudaError_t launch_shift_corner(const float *d_img_off, const float *d_img_on, const void *d_ctf,
                                 const float *d_mean, const float *d_txy, int txy_stride, int n,
-                                int N, float scale_out, float *d_out, cudaStream_t st) {
+                                int N, float scale_out, float *d_out, cudaStream_t st,
+                                bool fuse_mean) {
   if (n == 0) return cudaSuccess;
   SrcSel sel{d_img_off, d_img_on, reinterpret_cast<const CtfDev *>(d_ctf),
              1.0f / ((float)N * (float)N)};
-  dim3 grid((N * N + 255) / 256, n);
+  // with the edge mean formed per block, about two blocks per SM in all
+  dim3 grid(blocks_per_particle(n, N * N, fuse_mean ? 2 : 8), n);
   note_launch();
-  k_shift_corner<<<grid, 256, 0, st>>>(sel, d_mean, d_txy, txy_stride, N, scale_out, d_out, 0);
-  return cudaGetLastError();
-}
-
-bool mean_shift_fused(int n, int N) {
-  // Each block's own edge-mean reduction lengthens its life by a few
-  // microseconds: worth one kernel fewer only while the launch is a single
-  // wave of at most two blocks per SM (one particle at N <= ~270).
-  int dev = 0, sms = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  return (long)n * ((N * N + 255) / 256) <= 2L * sms;
-}
-
-cudaError_t launch_mean_shift_corner(const float *d_img_off, const float *d_img_on,
-                                     const void *d_ctf, const float *d_txy, int txy_stride, int n,
-                                     int N, float scale_out, float *d_out, cudaStream_t st) {
-  if (n == 0) return cudaSuccess;
-  SrcSel sel{d_img_off, d_img_on, reinterpret_cast<const CtfDev *>(d_ctf),
-             1.0f / ((float)N * (float)N)};
-  dim3 grid((N * N + 255) / 256, n);
-  note_launch();
-  k_shift_corner<<<grid, 256, 0, st>>>(sel, nullptr, d_txy, txy_stride, N, scale_out, d_out, 1);
+  k_shift_corner<<<grid, 256, 0, st>>>(sel, d_mean, d_txy, txy_stride, N, scale_out, d_out,
+                                       fuse_mean ? 1 : 0);
   return cudaGetLastError();
 }
 
