@@ -593,16 +593,17 @@ int prologue_upload(fr_recon *r, int n, const unsigned char *blk, cudaStream_t s
 
 int prologue_run(PlanCache &plans, const ProScratch &b, const unsigned char *d_meta,
                  const float *d_raw, const float *const *d_src, int n, int box, int N,
-                 const float *d_sym, int nsym, bool any_ctf, cudaStream_t st, bool exact_fft) {
+                 const float *d_sym, int nsym, bool any_ctf, cudaStream_t st, bool exact_fft,
+                 const PartSym *d_psym, long nslices) {
   const size_t img = (size_t)N * N, spec = (size_t)N * (N / 2 + 1);
   const MetaView mv = meta_view(d_meta, n);
   TRY(b.img->ensure(sizeof(float) * img * n));
   TRY(b.slices->ensure(sizeof(float) * slice_floats(N) * n));
   TRY(b.spec->ensure(std::max(sizeof(cufftComplex) * spec, sizeof(float) * img) * n));
-  TRY(b.t3d->ensure(sizeof(float) * 9 * (size_t)n * nsym));
+  TRY(b.t3d->ensure(sizeof(float) * 9 * (size_t)(nslices >= 0 ? nslices : (long)n * nsym)));
   if (any_ctf) TRY(b.img2->ensure(sizeof(float) * img * n));
   CU(launch_pad_compose(d_raw, d_src, n, box, N, b.img->as<float>(), mv.rot, d_sym, nsym,
-                        b.t3d->as<float>(), st));
+                        b.t3d->as<float>(), st, d_psym));
   const float *img_on = nullptr;
   if (any_ctf) {
     TRY(plans.exec2d(true, N, n, b.img->p, b.spec->p, st, exact_fft));

@@ -3,7 +3,7 @@
 //
 // A batch holds independent FourierReconstructor states (uneven N, modes and
 // symmetries: even/odd half maps, heterogeneity classes).  Each insert call
-// runs one prologue per group of jobs of equal (N, box, symmetry) on the batch
+// runs one prologue per group of jobs of equal (N, box) on the batch
 // stream, then per schedule ONE persistent insertion launch whose work list
 // interleaves all its jobs' (tile, slice block) items, heaviest first, and one
 // launch of their face taps (or one scatter launch over all its jobs' slices).
@@ -325,23 +325,27 @@ static int plan_launch(const RoundPlan &P, BatchScratch &bs, cudaStream_t st) {
 }
 
 // ------------------------------------------------------------ prologue groups
-// Jobs of a round that share (N, box, symmetry operators) run ONE prologue
-// over their concatenated particles, so each prologue stage is one launch
-// (or one batched FFT) per group rather than per job.  A group's metadata
-// block is the prologue_meta layout for all its particles, then a table of
-// their raw image addresses, so the jobs' images need not be contiguous.
+// Jobs of a round that share (N, box) run ONE prologue over their
+// concatenated particles, so each prologue stage is one launch (or one
+// batched FFT) per group rather than per job.  A group's metadata block is
+// the prologue_meta layout for all its particles, then a table of their raw
+// image addresses (the jobs' images need not be contiguous), then each
+// particle's symmetry operators and first slice (jobs of one group may have
+// different symmetries).
 struct ProGroup {
-  int N = 0, box = 0, nsym = 1, n = 0;
+  int N = 0, box = 0, n = 0;
+  long nslices = 0;                     // symmetry copies of all its particles
   bool ctf = false;                     // the group runs the CTF round trip
-  fr_recon *lead = nullptr;             // its FFT plans and symmetry operators serve the group
+  fr_recon *lead = nullptr;             // its FFT plans serve the group
   std::vector<int> jobs, first, count;  // job indices, first particle and count of each
+  std::vector<long> slice0;             // each job's first slice in the group
   size_t meta_off = 0;                  // the group's block in the round's block
 };
 
 static size_t align16(size_t b) { return (b + 15) & ~(size_t)15; }
-static size_t group_meta_bytes(int n) {
-  return align16(prologue_meta_bytes(n)) + sizeof(float *) * (size_t)n;
-}
+static size_t group_tab_off(int n) { return align16(prologue_meta_bytes(n)); }
+static size_t group_psym_off(int n) { return group_tab_off(n) + sizeof(float *) * (size_t)n; }
+static size_t group_meta_bytes(int n) { return group_psym_off(n) + sizeof(PartSym) * (size_t)n; }
 
 // Groups the jobs with counts[j] > 0 (in job order); returns the bytes of
 // the round's metadata block.
@@ -353,7 +357,7 @@ static size_t make_groups(const std::vector<fr_recon *> &jobs, const int *counts
     fr_recon *r = jobs[j];
     ProGroup *g = nullptr;
     for (ProGroup &q : G)
-      if (q.N == r->N && q.box == boxes[j] && q.nsym == r->nsym && q.lead->syms == r->syms) {
+      if (q.N == r->N && q.box == boxes[j]) {
         g = &q;
         break;
       }
@@ -362,13 +366,14 @@ static size_t make_groups(const std::vector<fr_recon *> &jobs, const int *counts
       g = &G.back();
       g->N = r->N;
       g->box = boxes[j];
-      g->nsym = r->nsym;
       g->lead = r;
     }
     g->jobs.push_back(j);
     g->first.push_back(g->n);
     g->count.push_back(counts[j]);
+    g->slice0.push_back(g->nslices);
     g->n += counts[j];
+    g->nslices += (long)counts[j] * r->nsym;
   }
   size_t off = 0;
   for (ProGroup &g : G) {
@@ -378,18 +383,28 @@ static size_t make_groups(const std::vector<fr_recon *> &jobs, const int *counts
   return off;
 }
 
-// Writes group g's block at blk: each job's particle metadata meta[j], then
-// particle i of job j's raw image address src[j] + i * box^2.  Returns
-// whether any particle carries a CTF.
-static bool group_meta(const ProGroup &g, const fr_particle *const *meta,
-                       const float *const *src, unsigned char *blk) {
+// Writes group g's block at blk: each job's particle metadata meta[j],
+// particle i of job j's raw image address src[j] + i * box^2, and its
+// symmetry operators (the job's) and first slice.  Returns whether any
+// particle carries a CTF.
+static bool group_meta(const std::vector<fr_recon *> &jobs, const ProGroup &g,
+                       const fr_particle *const *meta, const float *const *src,
+                       unsigned char *blk) {
   bool any = false;
-  const float **tab = reinterpret_cast<const float **>(blk + align16(prologue_meta_bytes(g.n)));
+  const float **tab = reinterpret_cast<const float **>(blk + group_tab_off(g.n));
+  PartSym *ps = reinterpret_cast<PartSym *>(blk + group_psym_off(g.n));
   const size_t img = (size_t)g.box * g.box;
   for (size_t k = 0; k < g.jobs.size(); k++) {
     const int j = g.jobs[k];
+    const fr_recon *r = jobs[j];
     any |= prologue_meta_range(g.N, g.n, g.first[k], g.count[k], meta[j], blk);
-    for (int i = 0; i < g.count[k]; i++) tab[g.first[k] + i] = src[j] + (size_t)i * img;
+    for (int i = 0; i < g.count[k]; i++) {
+      tab[g.first[k] + i] = src[j] + (size_t)i * img;
+      PartSym &q = ps[g.first[k] + i];
+      q.sym = r->d_sym.as<float>();
+      q.nsym = r->nsym;
+      q.slice0 = (int)(g.slice0[k] + (long)i * r->nsym);
+    }
   }
   return any;
 }
@@ -400,23 +415,23 @@ static bool group_meta(const ProGroup &g, const fr_particle *const *meta,
 static int group_run(const std::vector<fr_recon *> &jobs, const ProGroup &g, ProBufs &b,
                      const unsigned char *d_blk, RoundPlan *P, int tile_pref, cudaStream_t st,
                      bool exact_fft = false) {
-  const float *const *tab =
-      reinterpret_cast<const float *const *>(d_blk + align16(prologue_meta_bytes(g.n)));
+  const float *const *tab = reinterpret_cast<const float *const *>(d_blk + group_tab_off(g.n));
+  const PartSym *ps = reinterpret_cast<const PartSym *>(d_blk + group_psym_off(g.n));
   TRY(prologue_run(g.lead->plans, b.view(), d_blk, nullptr, tab, g.n, g.box, g.N,
-                   g.lead->d_sym.as<float>(), g.nsym, g.ctf, st, exact_fft));
+                   g.lead->d_sym.as<float>(), g.lead->nsym, g.ctf, st, exact_fft, ps, g.nslices));
   if (!P) return FR_OK;
   const MetaView mv = meta_view(d_blk, g.n);
   const size_t sl = (size_t)g.N * (g.N / 2 + 1);
   for (size_t k = 0; k < g.jobs.size(); k++) {
     const int j = g.jobs[k], f = g.first[k];
     plan_add(*P, jobs[j], j, g.count[k], tile_pref, b.slices.as<float2>() + (size_t)f * sl,
-             b.t3d.as<float>() + (size_t)f * g.nsym * 9, mv.w + f);
+             b.t3d.as<float>() + (size_t)g.slice0[k] * 9, mv.w + f);
   }
   return FR_OK;
 }
 
 // Inserts, for every job, counts[j] particles through the caller pipeline:
-// per round one prologue per group of jobs of equal (N, box, symmetry), and
+// per round one prologue per group of jobs of equal (N, box), and
 // all jobs' insertion work in one persistent launch per schedule.  Every
 // job runs on `st` for the duration of the call.
 static int batch_insert(std::vector<fr_recon *> &jobs, BatchScratch &bs, int tile_pref,
@@ -468,7 +483,7 @@ static int batch_insert(std::vector<fr_recon *> &jobs, BatchScratch &bs, int til
     int slot;
     unsigned char *blk;
     TRY(bs.ring.acquire(bytes, &slot, &blk));
-    for (ProGroup &g : G) g.ctf = group_meta(g, m.data(), src.data(), blk + g.meta_off);
+    for (ProGroup &g : G) g.ctf = group_meta(jobs, g, m.data(), src.data(), blk + g.meta_off);
     TRY(bs.d_meta.ensure(bytes));
     CU(cudaMemcpyAsync(bs.d_meta.p, blk, bytes, cudaMemcpyHostToDevice, st));
     TRY(bs.ring.done(slot, st));
@@ -702,7 +717,8 @@ static int graph_create(const std::vector<fr_recon *> &jobs, cudaStream_t st, in
   }
   if (rc == FR_OK) {
     std::vector<unsigned char> blk(std::max<size_t>(16, g->meta_bytes));
-    for (const ProGroup &q : g->groups) group_meta(q, zmeta.data(), src.data(), blk.data() + q.meta_off);
+    for (const ProGroup &q : g->groups)
+      group_meta(jobs, q, zmeta.data(), src.data(), blk.data() + q.meta_off);
     if (cudaMemcpyAsync(g->d_meta.p, blk.data(), g->meta_bytes, cudaMemcpyHostToDevice, st) !=
         cudaSuccess)
       rc = fail(FR_ECUDA, "metadata upload failed");
@@ -803,7 +819,7 @@ int fr_graph_launch(fr_graph *g, const float *const *imgs, const fr_particle *co
   // this staging block was last read by the replay before the previous one
   if (g->staged_used[k]) CU(cudaEventSynchronize(g->staged[k]));
   for (const ProGroup &q : g->groups) {
-    const bool any = group_meta(q, meta, src.data(), g->pinned[k] + q.meta_off);
+    const bool any = group_meta(g->jobs, q, meta, src.data(), g->pinned[k] + q.meta_off);
     if (any && !q.ctf)
       return fail(FR_EINVAL_PARAM,
                   "jobs of box %d (N %d) carry a CTF but were captured without the phase flip",

@@ -328,7 +328,7 @@ struct ProScratch {
 int prologue_run(PlanCache &plans, const ProScratch &b, const unsigned char *d_meta,
                  const float *d_raw, const float *const *d_src, int n, int box, int N,
                  const float *d_sym, int nsym, bool any_ctf, cudaStream_t st,
-                 bool exact_fft = false);
+                 bool exact_fft = false, const PartSym *d_psym = nullptr, long nslices = -1);
 int prologue_device(fr_recon *r, const float *d_raw, int n, int box, bool any_ctf);
 int particles_chunk(fr_recon *r, const float *d_raw, int n, int box, const fr_particle *meta,
                     int schedule);

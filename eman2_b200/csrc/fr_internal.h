@@ -148,12 +148,19 @@ void gather_tiles(int N, int mode, int tile, int corners, std::vector<int> &out,
                   int &tz);
 
 // Prologue (fr_prologue.cu).
+// Symmetry composition per particle, for a launch over the particles of
+// several jobs: the particle's job's operators, their count and the
+// particle's first slice in the launch's rotation blocks.
+struct PartSym {
+  const float *sym;
+  int nsym, slice0;
+};
 // Edge-mean subtraction and zero-pad clip of n raw images of size box to N
 // (from d_raw, or particle p from d_src[p] when a device pointer table is
 // given) and, in the same launch, the rotation composition launch_compose does.
 cudaError_t launch_pad_compose(const float *d_raw, const float *const *d_src, int n, int box, int N,
                                float *d_img, const float *d_rot, const float *d_sym, int nsym,
-                               float *d_t3d, cudaStream_t st);
+                               float *d_t3d, cudaStream_t st, const PartSym *d_psym = nullptr);
 void ctf_constants(float defocus, float dfdiff, float dfang, float voltage, float cs, float apix,
                    float ampcont, int N, void *out);
 size_t ctf_dev_size();

@@ -58,7 +58,8 @@ __device__ float edge_mean_dev(const float *img, int nx, int ny, float scale, do
 // per-particle table is given (the particles of several jobs in one launch).
 // grid.x = particle; the grid.y blocks of a particle share its pixels (each
 // forms the same edge mean).  With rot, block (p, 0) also composes the
-// particle's symmetry copies, t3d[p*nsym+q] = rot[p] * sym[q]
+// particle's symmetry copies, t3d[p*nsym+q] = rot[p] * sym[q] (with psym:
+// the particle's own operators, from its first slice on)
 // (libEM/transform.cpp:1384-1395), in float with the products and sums
 // rounded in that order.
 __global__ void __launch_bounds__(256) k_pad(const float *__restrict__ raw,
@@ -66,18 +67,28 @@ __global__ void __launch_bounds__(256) k_pad(const float *__restrict__ raw,
                                              int N, float *__restrict__ out,
                                              const float *__restrict__ rot,
                                              const float *__restrict__ sym, int nsym,
-                                             float *__restrict__ t3d) {
+                                             float *__restrict__ t3d,
+                                             const PartSym *__restrict__ psym) {
   __shared__ double s_red[8];
   const int p = blockIdx.x;
   if (rot && blockIdx.y == 0) {
-    for (int t = threadIdx.x; t < nsym * 9; t += blockDim.x) {
+    const float *sy = sym;
+    int ns = nsym;
+    size_t s0 = (size_t)p * nsym;
+    if (psym) {
+      const PartSym ps = psym[p];
+      sy = ps.sym;
+      ns = ps.nsym;
+      s0 = (size_t)ps.slice0;
+    }
+    for (int t = threadIdx.x; t < ns * 9; t += blockDim.x) {
       const int q = t / 9, e = t % 9, i = e / 3, j = e % 3;
       const float *a = rot + 9 * (size_t)p;
-      const float *b = sym + 9 * q;
+      const float *b = sy + 9 * q;
       float v = __fmul_rn(a[3 * i + 0], b[j]);
       v = __fadd_rn(v, __fmul_rn(a[3 * i + 1], b[3 + j]));
       v = __fadd_rn(v, __fmul_rn(a[3 * i + 2], b[6 + j]));
-      t3d[((size_t)p * nsym + q) * 9 + e] = v;
+      t3d[(s0 + q) * 9 + e] = v;
     }
   }
   const float *src = src_tab ? src_tab[p] : raw + (size_t)p * box * box;
@@ -96,7 +107,7 @@ __global__ void __launch_bounds__(256) k_pad(const float *__restrict__ raw,
 
 cudaError_t launch_pad_compose(const float *d_raw, const float *const *d_src, int n, int box, int N,
                                float *d_img, const float *d_rot, const float *d_sym, int nsym,
-                               float *d_t3d, cudaStream_t st) {
+                               float *d_t3d, cudaStream_t st, const PartSym *d_psym) {
   if (n == 0) return cudaSuccess;
   // few particles: several blocks each, so the launch still fills the device
   int dev = 0, sms = 148;
@@ -104,7 +115,8 @@ cudaError_t launch_pad_compose(const float *d_raw, const float *const *d_src, in
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const int parts = std::max(1, std::min(16, (16 * sms + n - 1) / n));
   note_launch();
-  k_pad<<<dim3(n, parts), 256, 0, st>>>(d_raw, d_src, box, N, d_img, d_rot, d_sym, nsym, d_t3d);
+  k_pad<<<dim3(n, parts), 256, 0, st>>>(d_raw, d_src, box, N, d_img, d_rot, d_sym, nsym, d_t3d,
+                                        d_psym);
   return cudaGetLastError();
 }
 

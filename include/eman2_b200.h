@@ -288,7 +288,7 @@ FR_API int fr_insert_particles_multi(fr_recon *const *handles, int nh, const flo
  * box boxes[j] for handle j; 0 leaves a job out), captured once as a CUDA
  * graph on `stream` (NULL: the first handle's): the prologue (pad, CTF flip
  * pair where ctf[j] is set, edge mean, shift, r2c, rotation composition), run
- * once per group of jobs of equal (N, box, symmetry) over their particles,
+ * once per group of jobs of equal (N, box) over their particles,
  * the groups as parallel branches; then the insertion launches (per schedule
  * one persistent launch or one scatter over all its jobs) and the face taps.
  * The graph owns the device image slots and the prologue scratch; the

@@ -121,14 +121,14 @@ def test_graph_replays_equal_batched_rounds(gpu):
 
 
 def _grouped_jobs():
-    """Jobs that share (N, box, symmetry) and so one prologue launch per
-    stage: with and without a CTF, different inserters (so different
-    schedules), beside a job of its own group."""
+    """Jobs that share (N, box) and so one prologue launch per stage: with
+    and without a CTF, different inserters (so different schedules),
+    different symmetries, beside a job of its own group."""
     from eman2_b200.particles import particle_meta
     from eman2_b200.synth import make_particles
     specs = [(32, 48, "gauss_2", "c1", 20, True), (32, 48, "gauss_2", "c1", 14, False),
              (32, 48, "gauss_5", "c1", 9, True), (32, 48, "nearest_neighbor", "c1", 17, False),
-             (40, 60, "gauss_2", "d2", 11, True)]
+             (32, 48, "gauss_2", "d3", 8, True), (40, 60, "gauss_2", "d2", 11, True)]
     jobs = []
     for k, (box, N, mode, sym, n, ctf) in enumerate(specs):
         ps = make_particles(box, n, seed=700 + k, snr=0.5, shift=2.0, weights=(0.5, 1.0), ctf=ctf)
@@ -138,8 +138,8 @@ def _grouped_jobs():
 
 
 def test_grouped_prologue_equals_each_job_alone(gpu):
-    """Jobs of equal (N, box, symmetry) run one prologue over their
-    concatenated particles (mixed CTF, mixed schedules): each job still gets
+    """Jobs of equal (N, box) run one prologue over their concatenated
+    particles (mixed CTF, schedules and symmetries): each job still gets
     its alone result, batched and through a graph reading device images in
     place."""
     import torch
@@ -174,7 +174,7 @@ def test_graph_of_one_particle_jobs_scatter(gpu):
     from eman2_b200.batch import BatchReconstructor, set_tile
     from eman2_b200.particles import particle_meta
     jobs = _grouped_jobs()
-    nsym = {"c1": 1, "d2": 4}
+    nsym = {"c1": 1, "d2": 4, "d3": 6}
     keys = {(p["size"][0], p["mode"], nsym[p["sym"]]) for p, _, _, _ in jobs}
     try:
         for k in keys:
