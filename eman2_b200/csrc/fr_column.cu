@@ -242,8 +242,13 @@ __device__ void tile_item(const InsertJob &J, int tile, int s0, int s1, const Sm
     bool hit = false;
     if (s < s1 && __ldg(&J.pw[s / J.nsym]) != 0.0f) {
       const float n[3] = {__ldg(&J.t3d[9 * s + 6]), __ldg(&J.t3d[9 * s + 7]), __ldg(&J.t3d[9 * s + 8])};
-      const float lo[3] = {base[0] - RLO - kDel, base[1] - RLO - kDel, base[2] - RLO - kDel};
-      const float hi[3] = {ext[0] + RHI + kDel, ext[1] + RHI + kDel, ext[2] + RHI + kDel};
+      // A pixel's direct taps reach the tile from [base - RLO, ext + RHI];
+      // its conjugate taps (mirrored) from [base - RHI, ext + RLO].  The
+      // plane passes through the origin, so one test against the union box
+      // covers both passes (gauss_5's window is asymmetric: 2.5 / 3.5).
+      constexpr float RC = (RLO > RHI ? RLO : RHI) + kDel;
+      const float lo[3] = {base[0] - RC, base[1] - RC, base[2] - RC};
+      const float hi[3] = {ext[0] + RC, ext[1] + RC, ext[2] + RC};
       float mn, mx;
       box_dot(n, lo, hi, mn, mx);
       hit = mn <= kPlaneTol && mx >= -kPlaneTol;
@@ -561,8 +566,13 @@ __device__ void tile_item3(const InsertJob &J, int tile, int s0, int s1, const S
     int grp = -1;
     if (s < s1 && __ldg(&J.pw[s / J.nsym]) != 0.0f) {
       const float n[3] = {__ldg(&J.t3d[9 * s + 6]), __ldg(&J.t3d[9 * s + 7]), __ldg(&J.t3d[9 * s + 8])};
-      const float lo[3] = {base[0] - RLO - kDel, base[1] - RLO - kDel, base[2] - RLO - kDel};
-      const float hi[3] = {ext[0] + RHI + kDel, ext[1] + RHI + kDel, ext[2] + RHI + kDel};
+      // A pixel's direct taps reach the tile from [base - RLO, ext + RHI];
+      // its conjugate taps (mirrored) from [base - RHI, ext + RLO].  The
+      // plane passes through the origin, so one test against the union box
+      // covers both passes (gauss_5's window is asymmetric: 2.5 / 3.5).
+      constexpr float RC = (RLO > RHI ? RLO : RHI) + kDel;
+      const float lo[3] = {base[0] - RC, base[1] - RC, base[2] - RC};
+      const float hi[3] = {ext[0] + RC, ext[1] + RC, ext[2] + RC};
       float mn, mx;
       box_dot(n, lo, hi, mn, mx);
       if (mn <= kPlaneTol && mx >= -kPlaneTol) {
@@ -892,8 +902,13 @@ __device__ void tile_item4(const InsertJob &J, int tile, int s0, int s1, const S
     bool hit = false;
     if (s < s1 && __ldg(&J.pw[s / J.nsym]) != 0.0f) {
       const float n[3] = {__ldg(&J.t3d[9 * s + 6]), __ldg(&J.t3d[9 * s + 7]), __ldg(&J.t3d[9 * s + 8])};
-      const float lo[3] = {base[0] - RLO - kDel, base[1] - RLO - kDel, base[2] - RLO - kDel};
-      const float hi[3] = {ext[0] + RHI + kDel, ext[1] + RHI + kDel, ext[2] + RHI + kDel};
+      // A pixel's direct taps reach the tile from [base - RLO, ext + RHI];
+      // its conjugate taps (mirrored) from [base - RHI, ext + RLO].  The
+      // plane passes through the origin, so one test against the union box
+      // covers both passes (gauss_5's window is asymmetric: 2.5 / 3.5).
+      constexpr float RC = (RLO > RHI ? RLO : RHI) + kDel;
+      const float lo[3] = {base[0] - RC, base[1] - RC, base[2] - RC};
+      const float hi[3] = {ext[0] + RC, ext[1] + RC, ext[2] + RC};
       float mn, mx;
       box_dot(n, lo, hi, mn, mx);
       hit = mn <= kPlaneTol && mx >= -kPlaneTol;

@@ -516,11 +516,14 @@ __device__ __forceinline__ void gather_tile(const InsertJob &J, int bx, int by, 
     if (s < total && __ldg(&J.pw[s / J.nsym]) != 0.0f) {
       const float n[3] = {__ldg(&J.t3d[9 * s + 6]), __ldg(&J.t3d[9 * s + 7]),
                           __ldg(&J.t3d[9 * s + 8])};
-      const float lo[3] = {bx - RLO - kDel, by - RLO - kDel, bz - RLO - kDel};
-      const float hi[3] = {ex + RHI + kDel, ey + RHI + kDel, ez + RHI + kDel};
+      // Direct taps reach the tile from [b - RLO, e + RHI], conjugate taps
+      // (mirrored) from [b - RHI, e + RLO]; the plane passes through the
+      // origin, so one test against the union box covers both passes.
+      const float RC = fmaxf(RLO, RHI) + kDel;
+      const float lo[3] = {bx - RC, by - RC, bz - RC};
+      const float hi[3] = {ex + RC, ey + RC, ez + RC};
       float mn, mx;
       box_dot(n, lo, hi, mn, mx);
-      // the mirrored box (-tile) gives (-mx, -mn): the same test
       hit = mn <= kPlaneTol && mx >= -kPlaneTol;
     }
     const unsigned b = __ballot_sync(0xffffffffu, hit);
