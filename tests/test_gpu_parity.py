@@ -83,6 +83,10 @@ def test_insert_schedules_match_oracle(gpu, sched, mode, N, sym):
     assert rel(d, o.data) < RTOL_ACC
     # same support: no tap went missing or appeared
     assert np.array_equal(nm != 0, o.norm != 0)
+    # every cell's weight (a sum of positive taps) to FP32 summation noise: a
+    # missing far tap (gauss_5's weights reach 1e-9) shows here, not in the L2
+    m = o.norm != 0
+    assert np.max(np.abs(nm[m] - o.norm[m]) / o.norm[m]) < 1e-4
     # Same taps summed in FP64: what is left is summation-order noise only.
     oa = oracle_insert(N, sl, rt, w, mode, sym, "fp32acc64")
     assert rel(d, oa.data) < RTOL_ACC and rel(nm, oa.norm) < RTOL_ACC
@@ -428,3 +432,54 @@ def test_column_kernel_many_blocks_matches_oracle(gpu):
         # dense centre cells is itself ~2e-5 from the exact sum
         assert rel(got, acc) <= rel(f32, acc) + 1e-7
         assert rel(got, f32) <= 1.5 * rel(f32, acc) + RTOL_ACC
+
+
+@pytest.mark.parametrize("sched", ["scatter", "gather"])
+@pytest.mark.parametrize("mode", ["gauss_2", "gauss_5", "nearest_neighbor"])
+@pytest.mark.parametrize("sym", ["tet", "oct", "icos"])
+def test_platonic_symmetry_matches_oracle(gpu, sched, mode, sym):
+    """The tetrahedral, octahedral and icosahedral groups (12, 24, 60 copies
+    of every slice) through both schedules."""
+    N, n = 24, 6
+    sl, rt = rand_slices(N, n, 111), rand_rots(n, 112)
+    w = np.random.default_rng(113).uniform(0.5, 1.0, n).astype(np.float32)
+    r = recon(N, mode, sym)
+    assert r.insert_slices(sl, rt, w, schedule=sched) == [0] * n
+    d, nm = r.get_accumulators()
+    o = oracle_insert(N, sl, rt, w, mode, sym)
+    assert np.array_equal(nm != 0, o.norm != 0)
+    # 60 copies of every slice into a 24^3 volume: the FP32 order noise of
+    # the oracle's own sums grows past RTOL_ACC, so the GPU is held to the
+    # same taps summed in FP64, within RTOL_ACC or the FP32 oracle's distance
+    oa = oracle_insert(N, sl, rt, w, mode, sym, "fp32acc64")
+    for got, want, own in ((nm, oa.norm, o.norm), (d, oa.data, o.data)):
+        assert rel(got, want) < max(RTOL_ACC, 2 * rel(own, want))
+    m = o.norm != 0
+    assert np.max(np.abs(nm[m] - o.norm[m]) / o.norm[m]) < 1e-4
+
+
+@pytest.mark.parametrize("sched", ["scatter", "gather_column3", "gather_column", "gather_v1"])
+def test_gauss5_far_taps_every_cell(gpu, sched):
+    """gauss_5 reaches 3.5 voxels on one side of a pixel and 2.5 on the other,
+    so a pixel's conjugate taps reach a voxel tile from the other side than
+    its direct taps: every cell's weight and normalised value at N = 96, d7,
+    against the oracle, including the periphery where only far taps (weights
+    down to 1e-9) land."""
+    N, n = 96, 24
+    sl, rt = rand_slices(N, n, 121), rand_rots(n, 122)
+    w = np.random.default_rng(123).uniform(0.5, 1.0, n).astype(np.float32)
+    r = recon(N, "gauss_5", "d7")
+    if sched != "scatter":
+        use_tile(N, "gauss_5", "d7", {"gather_v1": 0, "gather_column": 4, "gather_column3": 5}[sched])
+    try:
+        r.insert_slices(sl, rt, w, schedule="scatter" if sched == "scatter" else "gather")
+    finally:
+        use_tile(N, "gauss_5", "d7", -1)
+    d, nm = r.get_accumulators()
+    o = oracle_insert(N, sl, rt, w, "gauss_5", "d7")
+    assert np.array_equal(nm != 0, o.norm != 0)
+    m = o.norm != 0
+    assert np.max(np.abs(nm[m] - o.norm[m]) / o.norm[m]) < 1e-4
+    gd = r.finish(False).numpy()
+    want, _ = o.finish(False)
+    assert rel(gd, want) < 1e-5
