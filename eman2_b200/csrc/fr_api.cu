@@ -210,22 +210,79 @@ void eman_matrix(double az, double alt, double phi, float *m) {
   m[8] = (float)cos(altp);
 }
 
+// The platonic groups' operators as EMAN Euler triples (az, alt, phi), in the
+// reference's order: TetrahedralSym::get_sym (libEM/symmetry.cpp:2007-2027),
+// OctahedralSym::get_sym (:1950-1973), IcosahedralSym::get_sym (:1822-1868,
+// with its +90 / -90 azimuth alignment).  Each group is a few levels of
+// altitude, each with a ring of azimuths and a ring of in-plane angles.
+static int platonic_ops(const std::string &name, std::vector<float> &out) {
+  const double rad2deg = 180.0 / 3.141592653589793238462643383279502884197169399;
+  std::vector<float> e;   // (az, alt, phi) triples
+  if (name == "tet") {
+    const float l1 = (float)(rad2deg * acos((double)(-1.0f / 3.0f)));
+    for (int k = 0; k < 3; k++) e.insert(e.end(), {0.0f, 0.0f, 120.0f * k});
+    for (int a = 0; a < 3; a++)
+      for (int k = 0; k < 3; k++) e.insert(e.end(), {120.0f * a, l1, 60.0f + 120.0f * k});
+  } else if (name == "oct") {
+    for (int k = 0; k < 4; k++) e.insert(e.end(), {0.0f, 0.0f, 90.0f * k});
+    for (int a = 0; a < 4; a++)
+      for (int k = 0; k < 4; k++) e.insert(e.end(), {90.0f * a, 90.0f, 90.0f * k});
+    for (int k = 0; k < 4; k++) e.insert(e.end(), {0.0f, 180.0f, 90.0f * k});
+  } else if (name == "icos" || name == "icos5") {
+    const float l1 = (float)(rad2deg * atan((double)2.0f));
+    const float l2 = 180.0f - l1;
+    // in-plane ring of a pentagon centred on a level: 0, 288, 216, 144, 72
+    // (or those plus 36: 36, 324, 252, 180, 108)
+    auto ring = [](int k, float base) {
+      float v = base - 72.0f * k;
+      return v < 0 ? v + 360.0f : v;
+    };
+    for (int k = 0; k < 5; k++) e.insert(e.end(), {0.0f, 0.0f, ring(k, 0.0f)});
+    for (int a = 0; a < 5; a++)
+      for (int k = 0; k < 5; k++) e.insert(e.end(), {72.0f * a, l1, ring(k, 36.0f)});
+    for (int a = 0; a < 5; a++)
+      for (int k = 0; k < 5; k++) e.insert(e.end(), {36.0f + 72.0f * a, l2, ring(k, 0.0f)});
+    for (int k = 0; k < 5; k++) e.insert(e.end(), {0.0f, 180.0f, ring(k, 0.0f)});
+    for (size_t i = 0; i < e.size(); i += 3) {   // get_az_alignment_offset() == 234
+      e[i] = e[i] + 90.0f;
+      e[i + 2] = e[i + 2] - 90.0f;
+    }
+  } else {
+    return -1;
+  }
+  out.clear();
+  float m[9];
+  for (size_t i = 0; i < e.size(); i += 3) {
+    eman_matrix((double)e[i], (double)e[i + 1], (double)e[i + 2], m);
+    out.insert(out.end(), m, m + 9);
+  }
+  return (int)(e.size() / 3);
+}
+
 // Symmetry3D::get_symmetries (libEM/symmetry.cpp:1240-1246) for the cyclic
-// (CSym::get_sym, :1407-1417) and dihedral (DSym::get_sym, :1452-1470) groups;
-// the name parse follows Factory<Symmetry3D>::get (:76-100): "c" -> c1.
+// (CSym::get_sym, :1407-1417), dihedral (DSym::get_sym, :1452-1470) and
+// platonic groups (tet, oct, icos / icos5); the name parse follows
+// Factory<Symmetry3D>::get (:76-130): "c" -> c1.  Orders are parsed with a
+// range check: at most kMaxSymOps operators (c1000, d500), so a malformed
+// or huge order is refused before any operator is built.
 int sym_ops(const std::string &sym_in, std::vector<float> &out) {
   std::string sym;
   for (char ch : sym_in) sym.push_back((char)tolower((unsigned char)ch));
   if (sym.empty()) return -1;
+  if (sym == "tet" || sym == "oct" || sym == "icos" || sym == "icos5")
+    return platonic_ops(sym, out);
   const char kind = sym[0];
   if (kind != 'c' && kind != 'd') return -1;
-  int nsym = 1;
+  long nsym = 1;
   if (sym.size() > 1) {
+    if (sym.size() > 8) return -1;
     for (size_t i = 1; i < sym.size(); i++)
       if (sym[i] < '0' || sym[i] > '9') return -1;
-    nsym = atoi(sym.c_str() + 1);
+    char *end = nullptr;
+    nsym = strtol(sym.c_str() + 1, &end, 10);
+    if (!end || *end) return -1;
   }
-  if (nsym <= 0) return -1;
+  if (nsym <= 0 || (kind == 'c' ? nsym : 2 * nsym) > kMaxSymOps) return -1;
   out.clear();
   float m[9];
   if (kind == 'c') {
@@ -712,7 +769,7 @@ int fr_create(const fr_params *p, fr_recon **out) {
     return fail(FR_EUNSUPPORTED, "inserter mode %d is not built", p->mode);
   std::vector<float> ops;
   const int ns = sym_ops(p->sym, ops);
-  if (ns < 0) return fail(FR_EUNSUPPORTED, "symmetry '%s' is not supported (c<n>, d<n>)", p->sym);
+  if (ns < 0) return fail(FR_EUNSUPPORTED, "symmetry '%s' is not supported (c<n>, d<n> up to 1000 operators, tet, oct, icos)", p->sym);
   fr_recon *r = new fr_recon();
   r->p = *p;
   r->N = p->nx;

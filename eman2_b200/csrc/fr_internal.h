@@ -193,7 +193,10 @@ cudaError_t launch_projection_rt(const float *d_data, const float *d_norm, int N
                                  const float *d_rot, const float *d_rtab, float *d_out,
                                  cudaStream_t st);
 
-// Host-side symmetry (Symmetry3D::get_symmetries for c<n>/d<n>).
+// Host-side symmetry (Symmetry3D::get_symmetries for c<n>, d<n>, tet, oct,
+// icos): the operator count, or -1 for an unknown name or an order beyond
+// kMaxSymOps operators.
+constexpr int kMaxSymOps = 1000;
 int sym_ops(const std::string &sym, std::vector<float> &out);
 void eman_matrix(double az, double alt, double phi, float *m);
 

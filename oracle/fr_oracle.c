@@ -142,6 +142,41 @@ OR_EXPORT int or_sym_ops(char kind, int nsym, float *out, int cap) {
     }
     return ns;
   }
+  /* Platonic groups, row by row of the reference's Euler tables:
+   * 't' TetrahedralSym::get_sym (libEM/symmetry.cpp:2007-2027),
+   * 'o' OctahedralSym::get_sym (:1950-1973),
+   * 'i' IcosahedralSym::get_sym (:1822-1868; az + 90, phi - 90). */
+  if (kind == 't' || kind == 'o' || kind == 'i') {
+    const int count = kind == 't' ? 12 : kind == 'o' ? 24 : 60;
+    if (cap < count) return -1;
+    const float tlvl1 = (float)((180.0 / M_PI) * acos((double)(-1.0f / 3.0f)));
+    const float ilvl1 = (float)((180.0 / M_PI) * atan((double)2.0f));
+    for (int idx = 0; idx < count; idx++) {
+      float az, alt, phi;
+      if (kind == 't') {
+        if (idx < 3) { az = 0.0f; alt = 0.0f; phi = 120.0f * idx; }
+        else { az = 120.0f * ((idx - 3) / 3); alt = tlvl1; phi = 60.0f + 120.0f * ((idx - 3) % 3); }
+      } else if (kind == 'o') {
+        const int row = idx / 4, col = idx % 4;
+        phi = 90.0f * col;
+        if (row == 0) { az = 0.0f; alt = 0.0f; }
+        else if (row == 5) { az = 0.0f; alt = 180.0f; }
+        else { az = 90.0f * (row - 1); alt = 90.0f; }
+      } else {
+        const int row = idx / 5, col = idx % 5;
+        const int p0 = (360 - 72 * col) % 360;           /* 0, 288, 216, 144, 72 */
+        const int p36 = (36 - 72 * col + 360) % 360;     /* 36, 324, 252, 180, 108 */
+        if (row == 0) { az = 0.0f; alt = 0.0f; phi = (float)p0; }
+        else if (row <= 5) { az = 72.0f * (row - 1); alt = ilvl1; phi = (float)p36; }
+        else if (row <= 10) { az = 36.0f + 72.0f * (row - 6); alt = 180.0f - ilvl1; phi = (float)p0; }
+        else { az = 0.0f; alt = 180.0f; phi = (float)p0; }
+        az = az + 90.0f;
+        phi = phi - 90.0f;
+      }
+      or_eman_matrix((double)az, (double)alt, (double)phi, out + 9 * idx);
+    }
+    return count;
+  }
   return -1;
 }
 

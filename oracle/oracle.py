@@ -118,9 +118,14 @@ def quaternion_matrix(q) -> np.ndarray:
 
 
 def sym_ops(sym: str) -> np.ndarray:
-    """Symmetry operators of ``c<n>`` / ``d<n>`` as (nsym, 3, 3) float32."""
+    """Symmetry operators of ``c<n>`` / ``d<n>`` / ``tet`` / ``oct`` / ``icos``
+    (``icos5``) as (nsym, 3, 3) float32."""
     sym = sym.lower()
-    kind, n = sym[0], int(sym[1:] or 1)
+    platonic = {"tet": ("t", 12), "oct": ("o", 24), "icos": ("i", 60), "icos5": ("i", 60)}
+    if sym in platonic:
+        kind, n = platonic[sym]
+    else:
+        kind, n = sym[0], int(sym[1:] or 1)
     out = np.zeros(9 * 2 * n, np.float32)
     k = _lib().or_sym_ops(kind.encode(), n, _fp(out), 2 * n)
     if k < 0:

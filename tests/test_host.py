@@ -52,18 +52,40 @@ def test_abi_errors_without_touching_the_device(lib):
     p.mode = 3
     assert lib.fr_create(ctypes.byref(p), ctypes.byref(h)) == 7   # gauss_3 not built
     p.mode = 2
-    p.sym = b"icos"
+    p.sym = b"h3"                                                   # helical: not built
+    assert lib.fr_create(ctypes.byref(p), ctypes.byref(h)) == 7
+    p.sym = b"c2000000000"                                          # beyond the operator limit
     assert lib.fr_create(ctypes.byref(p), ctypes.byref(h)) == 7
     assert lib.fr_version().startswith(b"eman2_b200")
 
 
-@pytest.mark.parametrize("sym", ["c1", "c4", "c7", "d1", "d2", "d7", "D3", "C2"])
+@pytest.mark.parametrize("sym", ["c1", "c4", "c7", "d1", "d2", "d7", "D3", "C2", "tet", "oct",
+                                 "icos", "ICOS5", "c1000", "d500"])
 def test_library_symmetry_matches_oracle(lib, sym):
-    out = np.zeros(9 * 64, np.float32)
-    n = lib.fr_sym_ops(sym.encode(), out.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), 64)
+    out = np.zeros(9 * 1000, np.float32)
+    n = lib.fr_sym_ops(sym.encode(), out.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), 1000)
     want = oracle.sym_ops(sym)
     assert n == len(want)
     assert np.array_equal(out[: 9 * n].reshape(n, 3, 3), want)
+
+
+def test_platonic_groups_are_groups():
+    """tet, oct and icos: 12, 24 and 60 distinct rotations closed under products."""
+    for sym, count in (("tet", 12), ("oct", 24), ("icos", 60)):
+        ops = oracle.sym_ops(sym).astype(np.float64)
+        assert len(ops) == count
+        np.testing.assert_allclose(np.linalg.det(ops), 1.0, atol=1e-6)
+        for a in ops:
+            prod = np.einsum("ij,njk->nik", a, ops)
+            d = np.abs(prod[:, None] - ops[None]).max(axis=(2, 3)).min(axis=1)
+            assert d.max() < 1e-5
+
+
+def test_symmetry_order_limits(lib):
+    out = np.zeros(9, np.float32)
+    P = ctypes.POINTER(ctypes.c_float)
+    for bad in (b"c1001", b"d501", b"c2000000000", b"c99999999999", b"c-3", b"c0", b"x2", b"h4"):
+        assert lib.fr_sym_ops(bad, out.ctypes.data_as(P), 1) == -1, bad
 
 
 def test_params_and_exceptions():
