@@ -8,6 +8,7 @@
 // interleaves all its jobs' (tile, slice block) items, heaviest first, and one
 // launch of their face taps (or one scatter launch over all its jobs' slices).
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -348,7 +349,9 @@ static size_t group_psym_off(int n) { return group_tab_off(n) + sizeof(float *) 
 static size_t group_meta_bytes(int n) { return group_psym_off(n) + sizeof(PartSym) * (size_t)n; }
 
 // Groups the jobs with counts[j] > 0 (in job order); returns the bytes of
-// the round's metadata block.
+// the round's metadata block, or kGroupsTooLarge when a group would hold more
+// than INT_MAX particles or slices (its slice indices are ints on the device).
+constexpr size_t kGroupsTooLarge = ~(size_t)0;
 static size_t make_groups(const std::vector<fr_recon *> &jobs, const int *counts,
                           const int *boxes, std::vector<ProGroup> &G) {
   G.clear();
@@ -374,6 +377,7 @@ static size_t make_groups(const std::vector<fr_recon *> &jobs, const int *counts
     g->slice0.push_back(g->nslices);
     g->n += counts[j];
     g->nslices += (long)counts[j] * r->nsym;
+    if (g->nslices > INT_MAX || g->n > INT_MAX - kBatchChunk) return kGroupsTooLarge;
   }
   size_t off = 0;
   for (ProGroup &g : G) {
@@ -479,6 +483,9 @@ static int batch_insert(std::vector<fr_recon *> &jobs, BatchScratch &bs, int til
     }
     std::vector<ProGroup> G;
     const size_t bytes = make_groups(jobs, c.data(), boxes, G);
+    if (bytes == kGroupsTooLarge)
+      return fail(FR_EINVAL_PARAM, "a round's jobs of one (N, box) exceed INT_MAX slices; "
+                  "split the call");
     if (G.empty()) continue;
     int slot;
     unsigned char *blk;
@@ -659,16 +666,23 @@ static int graph_create(const std::vector<fr_recon *> &jobs, cudaStream_t st, in
     if (counts[j] < 0 || counts[j] > kBatchChunk || (counts[j] > 0 && boxes[j] <= 0))
       return fail(FR_EINVAL_PARAM, "job %d: count must be in [0, %d] with a positive box", j,
                   kBatchChunk);
+    if (total > INT_MAX - counts[j])
+      return fail(FR_EINVAL_PARAM, "a graph holds at most INT_MAX particles");
     total += counts[j];
   }
   if (total == 0) return fail(FR_EINVAL_PARAM, "a graph needs at least one particle");
+  std::vector<ProGroup> groups;
+  const size_t meta_bytes = make_groups(jobs, counts, boxes, groups);
+  if (meta_bytes == kGroupsTooLarge)
+    return fail(FR_EINVAL_PARAM, "the graph's jobs of one (N, box) exceed INT_MAX slices");
   fr_graph *g = new fr_graph();
   g->jobs = jobs;
   g->st = st;
   g->boxes.assign(boxes, boxes + nj);
   g->counts.assign(counts, counts + nj);
   g->slots.resize(nj);
-  g->meta_bytes = make_groups(jobs, counts, boxes, g->groups);
+  g->meta_bytes = meta_bytes;
+  g->groups = std::move(groups);
   g->gbufs.resize(g->groups.size());
   // a group runs the CTF round trip when any of its jobs was captured with one
   for (ProGroup &q : g->groups)

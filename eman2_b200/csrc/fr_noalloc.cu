@@ -42,14 +42,33 @@ static __device__ __align__(256) float g_scratch[kFloats];
 static std::mutex g_mu;
 static std::vector<float *> g_ptr;    // device address of g_scratch, per device
 
+// Whether p is device memory of device dev, or managed memory (which every
+// device reaches).  The kernels and the scratch are on the current device; a
+// buffer of another device would be read and written across devices.
+static bool on_device(const void *p, int dev) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  if (a.type == cudaMemoryTypeManaged) return true;
+  return a.type == cudaMemoryTypeDevice && a.device == dev;
+}
+
 // Set-up once per device (the device is current): the symbol's address and
-// the exp table, which never changes.
-static int scratch_for_current_device(cudaStream_t st, float **out) {
-  int dev = 0;
-  CU(cudaGetDevice(&dev));
+// the exp table, which never changes.  The upload waits for the stream, so
+// this first call on a device must not be captured into a graph: it is
+// refused with FR_EINVAL_PARAM on a capturing stream instead of breaking the
+// caller's capture.
+static int scratch_for_current_device(cudaStream_t st, int dev, float **out) {
   std::lock_guard<std::mutex> lk(g_mu);
   if ((int)g_ptr.size() <= dev) g_ptr.resize(dev + 1, nullptr);
   if (!g_ptr[dev]) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    CU(cudaStreamIsCapturing(st, &cs));
+    if (cs != cudaStreamCaptureStatusNone)
+      return fail(FR_EINVAL_PARAM, "the first allocation-free call on device %d sets up its "
+                  "scratch and cannot be captured; make one call before capturing", dev);
     float *p = nullptr;
     cudaError_t e = cudaGetSymbolAddress((void **)&p, g_scratch);
     if (e != cudaSuccess || !p)
@@ -87,19 +106,23 @@ extern "C" int fr_insert_slices_noalloc(const float *d_slices, int n, int N, int
     return fail(FR_EUNSUPPORTED, "inserter mode %d is not built", mode);
   std::vector<float> ops;
   const int nsym = sym_ops(sym, ops);
-  if (nsym < 0) return fail(FR_EUNSUPPORTED, "symmetry '%s' is not supported (c<n>, d<n>)", sym);
+  if (nsym < 0) return fail(FR_EUNSUPPORTED, "symmetry '%s' is not supported (c<n>, d<n> up to 1000 operators, tet, oct, icos)", sym);
   if (nsym > kMaxOps)
     return fail(FR_EINVAL_PARAM, "symmetry '%s' has %d operators; the allocation-free insertion "
                 "takes at most %d", sym, nsym, kMaxOps);
   if ((long)n * nsym > kMaxSlices)
     return fail(FR_EINVAL_PARAM, "%d slices x %d symmetry copies = %ld exceeds the allocation-free "
                 "limit of %d per call; split the batch", n, nsym, (long)n * nsym, kMaxSlices);
+  int dev = 0;
+  CU(cudaGetDevice(&dev));
   const void *ptrs[] = {d_slices, d_rot, d_weights, d_data, d_norm};
   for (const void *q : ptrs)
-    if (!is_device_ptr(q)) return fail(FR_EINVAL_PARAM, "all buffers must be device memory");
+    if (!on_device(q, dev))
+      return fail(FR_EINVAL_PARAM, "all buffers must be device memory of the current device (%d)",
+                  dev);
   cudaStream_t st = (cudaStream_t)stream;
   float *scr = nullptr;
-  TRY(scratch_for_current_device(st, &scr));
+  TRY(scratch_for_current_device(st, dev, &scr));
   if (n == 0) return FR_OK;
   // Per-size tables, formed on the host exactly as get_geom() forms them.
   const int n2 = N / 2;

@@ -219,9 +219,12 @@ FR_API int fr_stats_reset(void);
  * __device__ array of 596 KiB (152,696 floats) inside the library, held by
  * every GPU that loads it until exit.  Limits: even N <= 1024, at most 240 symmetry operators and
  * n * nsym <= 16384 per call; larger requests fail with FR_EINVAL_PARAM.
+ * Every buffer must be device memory of the current device (or managed
+ * memory); others fail with FR_EINVAL_PARAM.
  * The first call on a device looks up the array's address (with that device
  * current) and uploads the exp table: make that first call before any stream
- * capture.  All calls share the array: calls that overlap on the GPU race. */
+ * capture (a first call on a capturing stream fails with FR_EINVAL_PARAM).
+ * All calls share the array: calls that overlap on the GPU race. */
 FR_API int fr_insert_slices_noalloc(const float *d_slices, int n, int N, int mode,
                                     const char *sym, const float *d_rot,
                                     const float *d_weights, float *d_data, float *d_norm,

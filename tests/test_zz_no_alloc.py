@@ -25,7 +25,9 @@ def _rel(a, b):
     return float(np.linalg.norm(a - b) / np.linalg.norm(b))
 
 
-@pytest.mark.parametrize("mode,sym", [("gauss_2", "c1"), ("gauss_5", "d2")])
+@pytest.mark.parametrize("mode,sym", [("gauss_2", "c1"), ("gauss_5", "d2"),
+                                      ("nearest_neighbor", "c3"), ("trilinear", "c1"),
+                                      ("gauss_2", "tet")])
 def test_noalloc_matches_regular_insert_twice(gpu, mode, sym):
     import torch
 
@@ -81,3 +83,11 @@ def test_noalloc_rejects_oversized_requests(gpu):
     # too many slices x symmetry copies for one call
     assert lib.fr_insert_slices_noalloc(p, 2000, 32, 2, b"d7", p, p, p, p, None) == 1
     assert b"16384" in lib.fr_last_error()
+    # a symmetry order beyond the operator limit is refused before any operator is built
+    assert lib.fr_insert_slices_noalloc(p, 1, 32, 2, b"c2000000000", p, p, p, p, None) != 0
+    assert lib.fr_insert_slices_noalloc(p, 1, 32, 2, b"c99999999999", p, p, p, p, None) != 0
+    # a host buffer is refused (the kernels would read it from the device)
+    host = (ctypes.c_float * 16)()
+    hp = ctypes.cast(host, ctypes.c_void_p)
+    assert lib.fr_insert_slices_noalloc(hp, 1, 32, 2, b"c1", p, p, p, p, None) == 1
+    assert b"current device" in lib.fr_last_error()
