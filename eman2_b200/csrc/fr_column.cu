@@ -381,6 +381,36 @@ struct Smem3 {
 };
 constexpr int STEP2CAP = 800;   // gauss_2 step table entries (K = 256 over r <= 3.01: 772)
 
+// Tile-local coordinates (x, y, z) of cell i in layout L: L = A holds the
+// tile A-major, (a, b, c) at a*T*T + c*T + b with b < c the other two axes;
+// layout 2 is the volume's own [z][y][x] order.
+__device__ __forceinline__ void tile_cell(int L, int i, int *l) {
+  const int a = i >> 8, c = (i >> 4) & 15, b = i & 15;
+  if (L == 0) { l[0] = a; l[1] = b; l[2] = c; }
+  else if (L == 1) { l[0] = b; l[1] = a; l[2] = c; }
+  else { l[0] = b; l[1] = c; l[2] = a; }
+}
+__device__ __forceinline__ int tile_index(int L, const int *l) {
+  if (L == 0) return (l[0] << 8) | (l[2] << 4) | l[1];
+  if (L == 1) return (l[1] << 8) | (l[2] << 4) | l[0];
+  return (l[2] << 8) | (l[1] << 4) | l[0];
+}
+// Moves the tile's accumulators from layout `from` to layout `to` (all
+// threads; barriers inside).
+__device__ __noinline__ void relayout(float4 *acc, int from, int to) {
+  float4 v[NV / NT];
+#pragma unroll
+  for (int j = 0; j < NV / NT; j++) v[j] = acc[threadIdx.x + j * NT];
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < NV / NT; j++) {
+    int l[3];
+    tile_cell(from, threadIdx.x + j * NT, l);
+    acc[tile_index(to, l)] = v[j];
+  }
+  __syncthreads();
+}
+
 template <int MODE, int A>
 __device__ __forceinline__ void column_work(const Smem3 &S, const float *M, int sg, const int *base,
                                             const int *ext, int N, const float2 *__restrict__ sl,
@@ -429,8 +459,10 @@ __device__ __forceinline__ void column_work(const Smem3 &S, const float *M, int 
   float inv0[3];
 #pragma unroll
   for (int a = 0; a < 3; a++) inv0[a] = fabsf(m0[a]) > 1e-4f ? 1.0f / m0[a] : 0.0f;
-  const int str[3] = {1, T, T * T};
-  const int col_addr = lb * str[B] + lc * str[C];
+  // The tile is held A-major while group A runs: cell (a, b, c) of the tile
+  // at a*T*T + c*T + b, so a thread's column is threadIdx.x + a*T*T and the
+  // lanes of a warp always fall in distinct banks, whatever taps they add.
+  const int col_addr = threadIdx.x;
   const bool xzero_col = (A != 0) && (vb == 0);
   for (int y = r0; y <= r1; y++) {
     const int xm = S.xmax[y + n2];
@@ -473,10 +505,10 @@ __device__ __forceinline__ void column_work(const Smem3 &S, const float *M, int 
       // the window's taps along A inside the tile (the rest belong to the
       // neighbouring tile's work item): a predicated straight line for the
       // 2-tap windows, a loop for gauss_5's 6 (its unrolled form is slower)
-      auto tap = [&](int k) {
+      auto tap = [&](int k, float kf) {
         float vre, vim, vw;
         if (MODE == MODE_GAUSS2 || MODE == MODE_GAUSS5) {
-          const float d = __fsub_rn((float)k, pa);
+          const float d = __fsub_rn(kf, pa);
           const float d2 = __fmul_rn(d, d);
           float r;
           if (A == 0) r = __fadd_rn(__fadd_rn(d2, f0), f1);
@@ -488,7 +520,14 @@ __device__ __forceinline__ void column_work(const Smem3 &S, const float *M, int 
             vim = __fmul_rn(v.y, gg);
             vw = gg;
           } else {
-            const float gg = fast_exp(__fmul_rn(-r, h), S.exp);
+            // Util::fast_exp(f): the table index (int)(-f*50.0+0.5) is formed
+            // in double as the reference forms it; -f*50 + 0.5 is exact in
+            // double (a float times 50 plus 0.5 needs at most 31 bits), so
+            // one DFMA and a truncating conversion give the reference's index.
+            const float f = __fmul_rn(-r, h);
+            float gg;
+            if (f > 0.0f || f < -19.98f) gg = expf(f);
+            else gg = S.exp[__double2int_rz(__fma_rn((double)(-f), 50.0, 0.5))];
             vre = __fmul_rn(__fmul_rn(v.x, gg), w);
             vim = __fmul_rn(__fmul_rn(v.y, gg), w);
             vw = __fmul_rn(gg, w);
@@ -499,7 +538,7 @@ __device__ __forceinline__ void column_work(const Smem3 &S, const float *M, int 
           tap_value<MODE>(t[0], t[1], t[2], xx, yy, zz, v.x, v.y, w, h, nullptr, vre, vim, vw);
         }
         const int la = sg * k - base[A];
-        float4 *cell = &S.acc[col_addr + la * str[A]];
+        float4 *cell = &S.acc[col_addr + la * (T * T)];
         float4 u = *cell;
         const bool origin = (k == 0 && tb == 0 && tc == 0);
         if (sg > 0) {
@@ -520,10 +559,11 @@ __device__ __forceinline__ void column_work(const Smem3 &S, const float *M, int 
 #pragma unroll
         for (int j = 0; j < K; j++) {
           const int k = a0 + j;
-          if (k >= k0 && k <= k1) tap(k);
+          if (k >= k0 && k <= k1) tap(k, (float)k);
         }
       } else {
-        for (int k = k0; k <= k1; k++) tap(k);
+        float kf = (float)k0;   // exact: |k| < 2^24
+        for (int k = k0; k <= k1; k++, kf += 1.0f) tap(k, kf);
       }
     }
   }
@@ -642,12 +682,25 @@ __device__ void tile_item3(const InsertJob &J, int tile, int s0, int s1, const S
     if (MODE == MODE_GAUSS2) *S.state = MODE;
     *(S.state + 1) = J.N;
   }
-  // ---- the three axis groups; ownership of a voxel changes only between them
-  if (gstart[1] > gstart[0]) group_work<MODE, 0>(J, S, gstart[0], gstart[1], base, ext, h, steps);
+  // ---- the three axis groups; ownership of a voxel changes only between
+  // them, and so does the tile's layout (A-major for group A)
+  int layout = -1;   // -1: nothing added yet, any layout holds the zeros
+  if (gstart[1] > gstart[0]) {
+    group_work<MODE, 0>(J, S, gstart[0], gstart[1], base, ext, h, steps);
+    layout = 0;
+  }
   __syncthreads();
-  if (gstart[2] > gstart[1]) group_work<MODE, 1>(J, S, gstart[1], gstart[2], base, ext, h, steps);
+  if (gstart[2] > gstart[1]) {
+    if (layout == 0) relayout(S.acc, 0, 1);
+    group_work<MODE, 1>(J, S, gstart[1], gstart[2], base, ext, h, steps);
+    layout = 1;
+  }
   __syncthreads();
-  if (gstart[3] > gstart[2]) group_work<MODE, 2>(J, S, gstart[2], gstart[3], base, ext, h, steps);
+  if (gstart[3] > gstart[2]) {
+    if (layout == 0 || layout == 1) relayout(S.acc, layout, 2);
+    group_work<MODE, 2>(J, S, gstart[2], gstart[3], base, ext, h, steps);
+    layout = 2;
+  }
   __syncthreads();
   // ---- flush
   const size_t nxf = (size_t)N + 2;
@@ -655,7 +708,9 @@ __device__ void tile_item3(const InsertJob &J, int tile, int s0, int s1, const S
   for (int i = threadIdx.x; i < NV; i += NT) {
     const float4 v = S.acc[i];
     if (v.x == 0.f && v.y == 0.f && v.z == 0.f && v.w == 0.f) continue;
-    const int vx = base[0] + (i & 15), vy = base[1] + ((i >> 4) & 15), vz = base[2] + (i >> 8);
+    int l3[3];
+    tile_cell(layout, i, l3);
+    const int vx = base[0] + l3[0], vy = base[1] + l3[1], vz = base[2] + l3[2];
     if (vx > ext[0] || vy > ext[1] || vz > ext[2]) continue;
     const size_t row = (size_t)(vy < 0 ? N + vy : vy);
     const size_t slab = (size_t)(vz < 0 ? N + vz : vz);
