@@ -61,7 +61,9 @@ SIGNATURES = {
     "fr_determine_slice_agreement": ([_P, _P, ctypes.c_int, _P, _P, ctypes.c_float, ctypes.c_int,
                                       _P], ctypes.c_int),
     "fr_projection": ([_P, _P, _P], ctypes.c_int),
+    "fr_projection_xf": ([_P, _P, ctypes.c_int, _P], ctypes.c_int),
     "fr_finish": ([_P, ctypes.c_int, _P, _P], ctypes.c_int),
+    "fr_finish_async": ([_P, ctypes.c_int, _P, _P, _P], ctypes.c_int),
     "fr_get_accumulators": ([_P, _P, _P], ctypes.c_int),
     "fr_get_size": ([_P, _I], ctypes.c_int),
     "fr_footprint_bytes": ([ctypes.c_int], ctypes.c_size_t),

@@ -1176,22 +1176,48 @@ int fr_determine_slice_agreement(fr_recon *r, const float *slices, int n, const 
   return FR_OK;
 }
 
-int fr_projection(fr_recon *r, const float *rot, float *out_slice) {
+int fr_projection_xf(fr_recon *r, const float *xf, int ret_fourier, float *out) {
   TRY(check_state(r));
-  if (!rot || !out_slice) return fail(FR_ENULL, "null argument");
+  if (!xf || !out) return fail(FR_ENULL, "null argument");
   std::lock_guard<std::mutex> lk(r->mu);
   TRY(stream_enter(r, r->stream));
   const int N = r->N;
   cudaStream_t st = r->stream;
-  TRY(r->s_rot.ensure(sizeof(float) * 9));
-  const cudaMemcpyKind k = is_device_ptr(rot) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
-  CU(cudaMemcpyAsync(r->s_rot.p, rot, sizeof(float) * 9, k, st));
-  TRY(r->s_out.ensure(sizeof(float) * slice_floats(N)));
-  CU(cudaMemsetAsync(r->s_out.p, 0, sizeof(float) * slice_floats(N), st));
+  // the rotation block (the reference drops scale, mirror and translation
+  // for the slice itself) and the translation the result is shifted by
+  float h[12];
+  if (is_device_ptr(xf)) CU(cudaMemcpy(h, xf, sizeof h, cudaMemcpyDeviceToHost));
+  else memcpy(h, xf, sizeof h);
+  const float rot[9] = {h[0], h[1], h[2], h[4], h[5], h[6], h[8], h[9], h[10]};
+  TRY(r->s_rot.ensure(sizeof rot));
+  CU(cudaMemcpyAsync(r->s_rot.p, rot, sizeof rot, cudaMemcpyHostToDevice, st));
+  TRY(r->s_out.ensure(sizeof(float) * (slice_floats(N) + (size_t)N * N)));
+  float *spec = r->s_out.as<float>();
+  CU(cudaMemsetAsync(spec, 0, sizeof(float) * slice_floats(N), st));
   CU(launch_projection_rt(r->vol_data.as<float>(), r->vol_norm.as<float>(), N, r->s_rot.as<float>(),
-                          r->geom->d_rtab, r->s_out.as<float>(), st));
-  TRY(from_device(out_slice, r->s_out.p, sizeof(float) * slice_floats(N), st));
+                          r->geom->d_rtab, spec, st));
+  CU(launch_proj_shift(spec, N, h[3], h[7], ret_fourier ? 0 : 1, ret_fourier ? 0 : 1, st));
+  if (ret_fourier) {
+    TRY(from_device(out, spec, sizeof(float) * slice_floats(N), st));
+    return FR_OK;
+  }
+  // do_ift (libEM/emdata_transform.cpp:330-375): inverse real FFT, then each
+  // value times 1.0f / (N*N)
+  float *real = spec + slice_floats(N);
+  TRY(r->plans.exec2d(false, N, 1, spec, real, st));
+  const float scale = 1.0f / (float)(N * N);
+  CU(launch_scale(real, (size_t)N * N, scale, real, st));
+  TRY(from_device(out, real, sizeof(float) * (size_t)N * N, st));
   return FR_OK;
+}
+
+int fr_projection(fr_recon *r, const float *rot, float *out_slice) {
+  if (!rot || !out_slice) return fail(FR_ENULL, "null argument");
+  float h[9];
+  if (is_device_ptr(rot)) CU(cudaMemcpy(h, rot, sizeof h, cudaMemcpyDeviceToHost));
+  else memcpy(h, rot, sizeof h);
+  const float xf[12] = {h[0], h[1], h[2], 0.f, h[3], h[4], h[5], 0.f, h[6], h[7], h[8], 0.f};
+  return fr_projection_xf(r, xf, 1, out_slice);
 }
 
 int fr_get_accumulators(fr_recon *r, float *data, float *norm) {
@@ -1234,6 +1260,55 @@ int fr_finish(fr_recon *r, int doift, float *out, float *normout) {
     TRY(from_device(out, r->vol_data.p, vol_floats(N) * sizeof(float), st));
   }
   CU(cudaStreamSynchronize(st));
+  r->state = 2;
+  return FR_OK;
+}
+
+// Page-locked host memory (cudaHostAlloc / cudaHostRegister): the copy
+// engine reads and writes it without a staging copy, so copies into it are
+// asynchronous.
+static bool is_pinned_host(const void *p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
+int fr_finish_async(fr_recon *r, int doift, float *out, float *normout, void *stream) {
+  TRY(check_state(r));
+  for (const void *b : {(const void *)out, (const void *)normout})
+    if (b && !is_device_ptr(b) && !is_pinned_host(b))
+      return fail(FR_EINVAL_PARAM, "fr_finish_async writes device or page-locked host memory only");
+  std::lock_guard<std::mutex> lk(r->mu);
+  cudaStream_t st = stream ? (cudaStream_t)stream : r->stream;
+  TRY(stream_enter(r, st));
+  const int N = r->N;
+  CU(launch_normalize(r->vol_data.as<float>(), r->vol_norm.as<float>(), N, r->p.sqrtnorm, st,
+                      r->wfilt));
+  if (normout)
+    CU(cudaMemcpyAsync(normout, r->vol_norm.p, norm_floats(N) * sizeof(float), cudaMemcpyDefault,
+                       st));
+  if (doift) {
+    cufftHandle plan;
+    TRY(r->plans.get3d(N, st, &plan));
+    CUFFT(cufftExecC2R(plan, r->vol_data.as<cufftComplex>(), r->vol_data.as<cufftReal>()));
+    const float scale = 1.0f / (float)((size_t)N * N * N);
+    if (out) {
+      if (is_device_ptr(out)) {
+        CU(launch_depad_center(r->vol_data.as<float>(), N, scale, out, st));
+      } else {
+        TRY(r->s_out.ensure(sizeof(float) * (size_t)N * N * N));
+        CU(launch_depad_center(r->vol_data.as<float>(), N, scale, r->s_out.as<float>(), st));
+        CU(cudaMemcpyAsync(out, r->s_out.p, sizeof(float) * (size_t)N * N * N,
+                           cudaMemcpyDeviceToHost, st));
+      }
+    }
+  } else if (out) {
+    CU(cudaMemcpyAsync(out, r->vol_data.p, vol_floats(N) * sizeof(float), cudaMemcpyDefault, st));
+  }
+  TRY(stream_leave(r, st));
   r->state = 2;
   return FR_OK;
 }

@@ -328,21 +328,23 @@ cudaError_t launch_agree_rt(const float *d_data, const float *d_norm, int N, con
 // Fourier-space part: nearest-voxel value/weight for each slice pixel.
 // pixel_at divides by the weight; cells with weight < 0.005 stay 0; x=0 and
 // x=N/2 columns are halved except at y=0 and y=-N/2.
-__global__ void k_projection(const float *__restrict__ rdata, const float *__restrict__ norm, int N,
-                             const float *__restrict__ rot, const float *__restrict__ rtab,
-                             float *__restrict__ out) {
+// Value of pixel (x, y) of FourierReconstructor::projection
+// (libEM/reconstructor.cpp:1407-1431): the slice coordinate rotated
+// (transpose multiply), the nearest voxel's value over its weight
+// (pixel_at, :1448-1462); false where the reference skips the pixel.
+__device__ __forceinline__ bool proj_pixel(const float *__restrict__ rdata,
+                                           const float *__restrict__ norm, int N,
+                                           const float *__restrict__ rot,
+                                           const float *__restrict__ rtab, int x, int y,
+                                           float &d0, float &d1) {
   const int n2 = N / 2, nxf = N + 2;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int xw = n2 + 2;
-  if (i >= xw * N) return;
-  const int x = i % xw, y = i / xw - n2;
   const long nxy = (long)nxf * N;
   const float rx = __fdiv_rn((float)x, (float)(nxf - 2));
   const float ry = __ldg(&rtab[y + n2]);
   float xx = __fadd_rn(__fmul_rn(rx, rot[0]), __fmul_rn(ry, rot[3]));
   float yy = __fadd_rn(__fmul_rn(rx, rot[1]), __fmul_rn(ry, rot[4]));
   float zz = __fadd_rn(__fmul_rn(rx, rot[2]), __fmul_rn(ry, rot[5]));
-  if (fabsf(xx) > 0.5f || fabsf(yy) >= 0.5f || fabsf(zz) >= 0.5f) return;
+  if (fabsf(xx) > 0.5f || fabsf(yy) >= 0.5f || fabsf(zz) >= 0.5f) return false;
   xx = __fmul_rn(xx, (float)N);
   yy = __fmul_rn(yy, (float)N);
   zz = __fmul_rn(zz, (float)N);
@@ -356,21 +358,112 @@ __global__ void k_projection(const float *__restrict__ rdata, const float *__res
     vim = x0 < 0 ? -rdata[cidx + 1] : rdata[cidx + 1];
   }
   const float nv = norm[cidx / 2];
-  float d0 = __fdiv_rn(vre, nv), d1 = __fdiv_rn(vim, nv);
-  if (nv < 0.005f) return;
-  if ((x == 0 || x == nxf / 2) && (y != 0 && y != -N / 2)) { d0 = d0 / 2; d1 = d1 / 2; }
-  // set_complex_at(x, y) of the 2-D result (libEM/emdata_core.cpp set_complex_at)
-  if (x > n2) return;
-  const long o = (long)(y < 0 ? N + y : y) * nxf + 2 * x;
-  out[o] = d0;
-  out[o + 1] = d1;
+  if (nv < 0.005f) return false;
+  d0 = __fdiv_rn(vre, nv);
+  d1 = __fdiv_rn(vim, nv);
+  // the x == nx/2 branch of the reference's halving is the column past
+  // Nyquist, which set_complex_at drops
+  if (x == 0 && y != 0 && y != -n2) { d0 = d0 / 2; d1 = d1 / 2; }
+  return true;
+}
+
+// The projection's complex slice, written as the 2-D EMData::set_complex_at
+// writes it (libEM/emdata_core.cpp:171-206): columns x = 0 and x = N/2 are
+// kept Hermitian, a pixel at y > 0 setting rows y and N-y (its conjugate),
+// the one at -y only when the pixel at y was skipped (it comes first in the
+// reference's loop); rows 0 and N/2 of those columns keep the real part.
+// out[N][N+2] zeroed beforehand.  Grid: (N/2+1) x N pixels.
+__global__ void k_projection(const float *__restrict__ rdata, const float *__restrict__ norm, int N,
+                             const float *__restrict__ rot, const float *__restrict__ rtab,
+                             float *__restrict__ out) {
+  const int n2 = N / 2, nxf = N + 2, xw = n2 + 1;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= xw * N) return;
+  const int x = i % xw, y = i / xw - n2;
+  float d0, d1;
+  if (x == 0 || x == n2) {
+    if (y == 0 || y == -n2) {
+      if (proj_pixel(rdata, norm, N, rot, rtab, x, y, d0, d1)) {
+        const long o = (long)(y == 0 ? 0 : n2) * nxf + 2 * x;
+        out[o] = d0;
+        out[o + 1] = 0.0f;
+      }
+      return;
+    }
+    if (y < 0) return;
+    const long op = (long)y * nxf + 2 * x, om = (long)(N - y) * nxf + 2 * x;
+    if (proj_pixel(rdata, norm, N, rot, rtab, x, y, d0, d1)) {
+      out[op] = d0; out[op + 1] = d1;
+      out[om] = d0; out[om + 1] = -d1;
+    } else if (proj_pixel(rdata, norm, N, rot, rtab, x, -y, d0, d1)) {
+      out[om] = d0; out[om + 1] = d1;
+      out[op] = d0; out[op + 1] = -d1;
+    }
+    return;
+  }
+  if (proj_pixel(rdata, norm, N, rot, rtab, x, y, d0, d1)) {
+    const long o = (long)(y < 0 ? N + y : y) * nxf + 2 * x;
+    out[o] = d0;
+    out[o + 1] = d1;
+  }
+}
+
+// The projection's translation (libEM/reconstructor.cpp:1435-1437): the
+// xform processor's 2-D complex branch for a rotation-free transform
+// (libEM/processor.cpp:11082-11178) copies each value and rotates it by the
+// phase -2*pi*(ky*ty + kx*tx)/N (ky of row r: r - N for r > N/2).  The
+// reference forms the phase in long double and rounds it to float, and
+// takes cos/sin and the products in double; here the phase is formed in
+// double.  checker: the phase origin to the centre (center_origin_fft,
+// libEM/sparx/emdata_sparx.cpp:8420-8462: -1 where x + row is odd);
+// c2r_prep: the imaginary parts of the four self-conjugate values set to 0
+// (the part of them an inverse real FFT ignores).
+__global__ void k_proj_shift(float *__restrict__ out, int N, float tx, float ty, int checker,
+                             int c2r_prep) {
+  const int n2 = N / 2, nxf = N + 2, xw = n2 + 1;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= xw * N) return;
+  const int x = i % xw, row = i / xw;
+  const int ky = row >= n2 + 1 ? row - N : row;
+  const double pi = 3.141592653589793238462643383279502884197169399;
+  const float phase_y = (float)((((-2.0 * pi) * ky) * (double)ty) / N);
+  const float phase = (float)((double)phase_y - (((2.0 * pi) * x) * (double)tx) / N);
+  const double c = cos((double)phase), s = sin((double)phase);
+  const long o = (long)row * nxf + 2 * x;
+  const double re = out[o], im = out[o + 1];
+  float a = (float)(re * c - im * s), b = (float)(re * s + im * c);
+  if (checker && ((x + row) & 1)) { a = -a; b = -b; }
+  if (c2r_prep && (x == 0 || x == n2) && (row == 0 || row == n2)) b = 0.0f;
+  out[o] = a;
+  out[o + 1] = b;
+}
+
+__global__ void k_scale(const float *__restrict__ in, size_t n, float scale, float *__restrict__ out) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    out[i] = in[i] * scale;
 }
 
 cudaError_t launch_projection_rt(const float *d_data, const float *d_norm, int N, const float *d_rot,
                                  const float *d_rtab, float *d_out, cudaStream_t st) {
-  const int n = (N / 2 + 2) * N;
+  const int n = (N / 2 + 1) * N;
   note_launch();
   k_projection<<<(n + 255) / 256, 256, 0, st>>>(d_data, d_norm, N, d_rot, d_rtab, d_out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_proj_shift(float *d_out, int N, float tx, float ty, int checker, int c2r_prep,
+                              cudaStream_t st) {
+  const int n = (N / 2 + 1) * N;
+  note_launch();
+  k_proj_shift<<<(n + 255) / 256, 256, 0, st>>>(d_out, N, tx, ty, checker, c2r_prep);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_scale(const float *d_in, size_t n, float scale, float *d_out, cudaStream_t st) {
+  note_launch();
+  const int grid = (int)std::min<size_t>((n + 255) / 256, 4096);
+  k_scale<<<grid, 256, 0, st>>>(d_in, n, scale, d_out);
   return cudaGetLastError();
 }
 

@@ -192,6 +192,9 @@ cudaError_t launch_agree_rt(const float *d_data, const float *d_norm, int N, con
 cudaError_t launch_projection_rt(const float *d_data, const float *d_norm, int N,
                                  const float *d_rot, const float *d_rtab, float *d_out,
                                  cudaStream_t st);
+cudaError_t launch_proj_shift(float *d_out, int N, float tx, float ty, int checker, int c2r_prep,
+                              cudaStream_t st);
+cudaError_t launch_scale(const float *d_in, size_t n, float scale, float *d_out, cudaStream_t st);
 
 // Host-side symmetry (Symmetry3D::get_symmetries for c<n>, d<n>, tet, oct,
 // icos): the operator count, or -1 for an unknown name or an order beyond

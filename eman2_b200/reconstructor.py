@@ -417,15 +417,21 @@ class FourierReconstructor:
         return out
 
     def projection(self, xform, ret_fourier: int = 1) -> EMData:
-        """FourierReconstructor::projection (libEM/reconstructor.cpp:1383-1445),
-        Fourier-space part (ret_fourier=1, no translation)."""
+        """FourierReconstructor::projection (libEM/reconstructor.cpp:1383-1445)
+        of the current accumulators: the slice through the volume at the
+        transform's rotation, shifted by its translation; ret_fourier=1 the
+        complex slice (N, N+2), 0 the real (N, N) image (phase origin to the
+        centre, inverse FFT)."""
+        if self._state != 1:
+            self._require_setup()
         N = self.N
-        out = np.zeros((N, N + 2), np.float32)
-        rot = _rot_of(xform)
-        _lib.check(_lib.load().fr_projection(self._h, _lib.ptr(rot), _lib.ptr(out)))
-        if not ret_fourier:
-            raise UnsupportedParameterException("real-space projections are not built")
-        return EMData(out, is_complex=True)
+        xf = np.zeros((3, 4), np.float32)
+        xf[:, :3] = _rot_of(xform)
+        xf[0, 3], xf[1, 3] = _trans_of(xform)
+        out = np.zeros((N, N + 2) if ret_fourier else (N, N), np.float32)
+        _lib.check(_lib.load().fr_projection_xf(self._h, _lib.ptr(xf), int(bool(ret_fourier)),
+                                                _lib.ptr(out)))
+        return EMData(out, is_complex=bool(ret_fourier))
 
     # --------------------------------------------------------- results
     def get_accumulators(self):
@@ -453,6 +459,29 @@ class FourierReconstructor:
         if self.params.get("savenorm"):
             np.save(str(self.params["savenorm"]), norm)
         return EMData(out, is_complex=not doift)
+
+    def finish_async(self, doift: bool = True, stream=None) -> "PendingFinish":
+        """finish() enqueued without waiting (fr_finish_async): the map and
+        the weights are written into page-locked host buffers on ``stream``
+        (a torch CUDA stream; default the library stream).  Returns a
+        PendingFinish: ready() polls, result() waits and returns the EMData
+        (and fills the ``normout`` EMData, as finish() does)."""
+        import torch
+        if self._state != 1:
+            self._require_setup()
+        N = self.N
+        out = torch.empty((N, N, N) if doift else (N, N, N + 2), dtype=torch.float32,
+                          pin_memory=True)
+        norm = torch.empty((N, N, N // 2 + 1), dtype=torch.float32, pin_memory=True)
+        if stream is None:
+            dev = torch.device("cuda", torch.cuda.current_device())
+            stream = _join_parts(library_stream(self._h), dev)[0]
+        _lib.check(_lib.load().fr_finish_async(self._h, int(bool(doift)), out.data_ptr(),
+                                               norm.data_ptr(), ctypes.c_void_p(stream.cuda_stream)))
+        ev = torch.cuda.Event()
+        ev.record(stream)
+        self._state = 2
+        return PendingFinish(self, out, norm, ev, not doift)
 
     # e2make3dpar's Gaussian widths per mode (programs/e2make3dpar.py:422)
     KERNEL_FIX_WIDTH = {"gauss_2": 4.0, "gauss_3": 6.4, "gauss_4": 8.8, "gauss_5": 10.4,
@@ -488,6 +517,29 @@ class FourierReconstructor:
     def _require_setup(self):
         raise StateException("setup() has not been called" if self._state == 0 else
                              "finish() was called; call setup() again")
+
+
+class PendingFinish:
+    """A finish enqueued by FourierReconstructor.finish_async."""
+
+    def __init__(self, owner, out, norm, event, is_complex):
+        self.owner = owner
+        self._out, self._norm, self._event = out, norm, event
+        self._complex = is_complex
+        self._result = None
+
+    def ready(self) -> bool:
+        return self._result is not None or self._event.query()
+
+    def result(self) -> EMData:
+        if self._result is None:
+            self._event.synchronize()
+            r = self.owner
+            if "normout" in r.params and isinstance(r.params["normout"], EMData):
+                r.params["normout"].set_data(self._norm.numpy().copy())
+            self._result = EMData(self._out.numpy().copy(), is_complex=self._complex)
+            self._out = self._norm = None
+        return self._result
 
 
 class WienerFourierReconstructor(FourierReconstructor):

@@ -152,8 +152,16 @@ FR_API int fr_determine_slice_agreement(fr_recon *r, const float *slices, int n,
                                         const float *rot, const float *weights, float apix,
                                         int sub, float *out);
 
-/* FourierReconstructor::projection (libEM/reconstructor.cpp:1383-1445),
- * ret_fourier=1 form without the final translation: writes float[N][N+2]. */
+/* FourierReconstructor::projection (libEM/reconstructor.cpp:1383-1445) of
+ * the current accumulators.  xf: the Transform as its 3x4 matrix (float[12],
+ * row-major: rotation block and the translation column xf[3], xf[7],
+ * xf[11]); the slice uses the rotation only and is then shifted by the
+ * translation (the xform processor, :1435-1437).  ret_fourier=1: out =
+ * float[N][N+2] complex slice; ret_fourier=0: phase origin to the centre and
+ * the inverse FFT, out = float[N][N] real image. */
+FR_API int fr_projection_xf(fr_recon *r, const float *xf, int ret_fourier, float *out);
+/* The same for a rotation block rot[9] with no translation, ret_fourier=1:
+ * out = float[N][N+2]. */
 FR_API int fr_projection(fr_recon *r, const float *rot, float *out_slice);
 
 /* FourierReconstructor::finish (libEM/reconstructor.cpp:1552-1641).
@@ -162,6 +170,17 @@ FR_API int fr_projection(fr_recon *r, const float *rot, float *out_slice);
  * normout (optional) = float[N][N][N/2+1] weights (the "normout" param).
  * The handle needs fr_setup() again afterwards (ownership passes out). */
 FR_API int fr_finish(fr_recon *r, int doift, float *out, float *normout);
+
+/* fr_finish without waiting (no counterpart in the reference, whose finish
+ * returns the map): the same work is enqueued on `stream` (NULL: the
+ * handle's stream) after the handle's earlier work, with out and normout
+ * device memory or page-locked host memory (FR_EINVAL_PARAM otherwise), and
+ * the call returns once it is enqueued.  The results are complete when the
+ * stream reaches this point (an event recorded after the call).  A server
+ * retiring a job this way keeps inserting other jobs meanwhile.  Device-side
+ * inconsistency codes of earlier insertions are reported by the handle's
+ * next synchronous call instead. */
+FR_API int fr_finish_async(fr_recon *r, int doift, float *out, float *normout, void *stream);
 
 /* finish(True) followed by what e2make3dpar does with the map
  * (programs/e2make3dpar.py:421-431): the radial kernel correction

@@ -5,11 +5,13 @@
 # oracle/_ref/libfr_ref.so.  Test infrastructure only.  -I- stops the compiler from
 # resolving "emdata.h" next to the reference source, so the stand-in is used.
 # Strict IEEE flags (no contraction) so results compare bitwise with fr_oracle.c.
+# The reference tree's location is the first argument or $EMAN2_REFERENCE;
+# without either (or without the tree) nothing is built.
 set -e
-REF=${EMAN2_REFERENCE:-/root/reference}
+REF=${1:-$EMAN2_REFERENCE}
 HERE=$(cd "$(dirname "$0")" && pwd)
-if [ ! -f "$REF/libEM/reconstructor_tools.cpp" ]; then
-  echo "reference tree not found at $REF; oracle/_ref not built" >&2
+if [ -z "$REF" ] || [ ! -f "$REF/libEM/reconstructor_tools.cpp" ]; then
+  echo "reference tree not given or not found ('$REF'); oracle/_ref not built" >&2
   exit 0
 fi
 mkdir -p "$HERE/_ref"

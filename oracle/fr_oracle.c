@@ -630,6 +630,74 @@ static inline void or_pixel_at(const acc_t *rdata, const acc_t *norm, int N, rea
   dt[2] = nv;
 }
 
+/* FourierReconstructor::projection (libEM/reconstructor.cpp:1383-1445),
+ * Fourier-space part, into out[N][N+2] (zeroed here): each pixel x in
+ * [0, N/2+1], y in [-N/2, N/2) rotated (transpose multiply, float), the
+ * nearest voxel's value over its weight, skipped where the weight is below
+ * 0.005, the x = 0 column halved off rows 0 and -N/2, written with the 2-D
+ * EMData::set_complex_at (libEM/emdata_core.cpp:171-206); then the
+ * translation (tx, ty) applied by the xform processor's 2-D complex branch
+ * (libEM/processor.cpp:11082-11178, a rotation-free transform: each value
+ * copied and rotated by its phase, the phase formed in long double --
+ * the processor's pi, libEM/sparx/emconstants.h:38 -- and rounded to
+ * float, cos/sin and the products in double). */
+static void or_set_complex_2d(float *d, int nx, int ny, int x, int y, float re, float im) {
+  if (abs(x) >= nx / 2 || abs(y) > ny / 2) return;
+  if (x == 0 || x == nx / 2 - 1) {
+    const int c = x == 0 ? 0 : nx - 2;
+    if (y == 0) { d[c] = re; d[c + 1] = 0; }
+    else if (y == ny / 2 || y == -ny / 2) { d[ny / 2 * nx + c] = re; d[ny / 2 * nx + c + 1] = 0; }
+    else if (y > 0) {
+      d[y * nx + c] = d[(ny - y) * nx + c] = re;
+      d[y * nx + c + 1] = im;
+      d[(ny - y) * nx + c + 1] = -im;
+    } else {
+      d[(ny + y) * nx + c] = d[-y * nx + c] = re;
+      d[(ny + y) * nx + c + 1] = im;
+      d[-y * nx + c + 1] = -im;
+    }
+    return;
+  }
+  if (y >= 0) { d[x * 2 + y * nx] = re; d[x * 2 + y * nx + 1] = im; }
+  else { d[x * 2 + (ny + y) * nx] = re; d[x * 2 + (ny + y) * nx + 1] = im; }
+}
+
+OR_EXPORT void or_projection(const acc_t *rdata, const acc_t *norm, int N, const float *rot,
+                             float tx, float ty, float *out) {
+  const int nx = N + 2, ny = N, nz = N;
+  memset(out, 0, sizeof(float) * (size_t)nx * ny);
+  for (int y = -ny / 2; y < ny / 2; y++) {
+    for (int x = 0; x <= nx / 2; x++) {
+      const float rx = (float)x / (nx - 2);
+      const float ry = (float)y / ny;
+      float xx = rx * rot[0] + ry * rot[3];
+      float yy = rx * rot[1] + ry * rot[4];
+      float zz = rx * rot[2] + ry * rot[5];
+      if (fabsf(xx) > 0.5f || fabsf(yy) >= 0.5f || fabsf(zz) >= 0.5f) continue;
+      xx = xx * (nx - 2);
+      yy = yy * ny;
+      zz = zz * nz;
+      real dt[3];
+      or_pixel_at(rdata, norm, N, xx, yy, zz, dt);
+      if (dt[2] < 0.005) continue;
+      float d0 = (float)dt[0], d1 = (float)dt[1];
+      if ((x == 0 || x == nx / 2) && (y != 0 && y != -ny / 2)) { d0 /= 2; d1 /= 2; }
+      or_set_complex_2d(out, nx, ny, x, y, d0, d1);
+    }
+  }
+  const long double pi = 3.141592653589793238462643383279502884197L;
+  for (int kyN = 0; kyN < ny; kyN++) {
+    const int kyNew = kyN >= nx / 2 ? kyN - ny : kyN;
+    const float phaseY = (float)(-2 * pi * kyNew * ty / ny);
+    for (int kx = 0; kx < nx / 2; kx++) {
+      const float phase = (float)(phaseY - 2 * pi * kx * tx / ny);
+      const float r = out[2 * kx + nx * kyN], i = out[2 * kx + 1 + nx * kyN];
+      out[2 * kx + nx * kyN] = (float)((double)r * cos((double)phase) - (double)i * sin((double)phase));
+      out[2 * kx + 1 + nx * kyN] = (float)((double)r * sin((double)phase) + (double)i * cos((double)phase));
+    }
+  }
+}
+
 /* FourierReconstructor::do_compare_slice_work (libEM/reconstructor.cpp:1259-1381),
  * CPU branch.  out[0..4] = reconstruct_norm, reconstruct_absqual,
  * reconstruct_absqual_lowres, reconstruct_qual, reconstruct_weight.

@@ -40,11 +40,13 @@ _D = ctypes.POINTER(ctypes.c_double)
 _libs: dict = {}
 
 
-def build(ref: bool = True) -> None:
-    """Compile the oracle libraries (and the reference pin, when its tree is present)."""
+def build(ref: bool = True, reference: str | None = None) -> None:
+    """Compile the oracle libraries and, when ``ref`` and a reference tree is
+    given (``reference`` or $EMAN2_REFERENCE), the reference pin."""
     subprocess.run(["make", "-s", "-C", HERE], check=True)
-    if ref:
-        subprocess.run(["sh", os.path.join(HERE, "build_ref.sh")], check=True,
+    tree = reference or os.environ.get("EMAN2_REFERENCE")
+    if ref and tree:
+        subprocess.run(["sh", os.path.join(HERE, "build_ref.sh"), tree], check=True,
                        stdout=subprocess.DEVNULL)
 
 
@@ -72,6 +74,7 @@ def _lib(kind: str = "fp32"):
     lib.or_compare_slice.argtypes = [R, R, ctypes.c_int, _F, _F, ctypes.c_int, ctypes.c_float,
                                      ctypes.c_float, _F]
     lib.or_sym_ops.argtypes = [ctypes.c_char, ctypes.c_int, _F, ctypes.c_int]
+    lib.or_projection.argtypes = [R, R, ctypes.c_int, _F, ctypes.c_float, ctypes.c_float, _F]
     lib.or_eman_matrix.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_double, _F]
     lib.or_quaternion_matrix.argtypes = [ctypes.c_double] * 4 + [_F]
     lib.or_compose.argtypes = [_F, _F, _F]
@@ -235,6 +238,27 @@ class OracleVolume:
                                   _fp(np.ascontiguousarray(t3d)), t3d.shape[0], float(weight),
                                   float(apix), _fp(out))
         return out
+
+    def projection(self, rot, tx: float = 0.0, ty: float = 0.0, ret_fourier: bool = True):
+        """FourierReconstructor::projection (libEM/reconstructor.cpp:1383-1445)
+        of the current accumulators for rotation block rot (3, 3) and
+        translation (tx, ty): the complex slice (N, N+2), or with
+        ret_fourier False the phase origin moved to the centre
+        (center_origin_fft, libEM/sparx/emdata_sparx.cpp:8420-8462) and the
+        inverse FFT x 1/N^2 (do_ift, libEM/emdata_transform.cpp:330-375):
+        a real (N, N) image."""
+        N = self.N
+        out = np.zeros((N, N + 2), np.float32)
+        r = np.ascontiguousarray(rot, np.float32).reshape(9)
+        self.lib.or_projection(_rp(self.data), _rp(self.norm), N, _fp(r), float(tx), float(ty),
+                               _fp(out))
+        if ret_fourier:
+            return out
+        c = out[:, 0::2] + 1j * out[:, 1::2].astype(np.float64)
+        kx = np.arange(N // 2 + 1)[None, :]
+        row = np.arange(N)[:, None]
+        c = np.where((kx + row) % 2 == 1, -c, c)
+        return _ift_f32(c.astype(np.complex64), N)
 
     def copy(self):
         o = OracleVolume.__new__(OracleVolume)

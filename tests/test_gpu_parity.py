@@ -483,3 +483,73 @@ def test_gauss5_far_taps_every_cell(gpu, sched):
     gd = r.finish(False).numpy()
     want, _ = o.finish(False)
     assert rel(gd, want) < 1e-5
+
+
+def test_clear_zeroes_and_insertion_continues(gpu):
+    """FourierReconstructor::clear (libEM/reconstructor.cpp:999-1020): both
+    accumulators zeroed; the handle stays set up and later inserts match a
+    fresh reconstruction of only those slices."""
+    N, n = 24, 10
+    sl, rt = rand_slices(N, n, 131), rand_rots(n, 132)
+    w = np.ones(n, np.float32)
+    r = recon(N, "gauss_5", "c2")
+    r.insert_slices(sl[:5], rt[:5], w[:5])
+    d, nm = r.get_accumulators()
+    assert np.any(d != 0) and np.any(nm != 0)
+    r.clear()
+    d, nm = r.get_accumulators()
+    assert not np.any(d) and not np.any(nm)
+    r.insert_slices(sl[5:], rt[5:], w[5:])
+    d, nm = r.get_accumulators()
+    o = oracle_insert(N, sl[5:], rt[5:], w[5:], "gauss_5", "c2")
+    assert rel(d, o.data) < RTOL_ACC and rel(nm, o.norm) < RTOL_ACC
+
+
+@pytest.mark.parametrize("doift", [False, True])
+def test_sqrtnorm_finish_matches_oracle(gpu, doift):
+    """normalize_threed with sqrtnorm (libEM/reconstructor.cpp:377): every
+    complex value divided by the square root of its summed weight."""
+    N, n = 32, 30
+    sl, rt = rand_slices(N, n, 141), rand_rots(n, 142)
+    w = np.random.default_rng(143).uniform(0.5, 1.0, n).astype(np.float32)
+    r = recon(N, "gauss_2", "d1", sqrtnorm=True)
+    r.insert_slices(sl, rt, w)
+    out = r.finish(doift).numpy()
+    o = oracle_insert(N, sl, rt, w, "gauss_2", "d1")
+    want, _ = o.finish(doift, sqrtnorm=True)
+    assert rel(out, want) < (RTOL_FFT if doift else RTOL_ACC)
+    # and it differs from the plain normalisation
+    o2 = oracle_insert(N, sl, rt, w, "gauss_2", "d1")
+    plain, _ = o2.finish(doift)
+    assert rel(out, plain) > 1e-2
+
+
+@pytest.mark.parametrize("ret_fourier", [1, 0])
+@pytest.mark.parametrize("shift", [(0.0, 0.0), (2.5, -1.25)])
+def test_projection_matches_oracle(gpu, ret_fourier, shift):
+    """FourierReconstructor::projection (libEM/reconstructor.cpp:1383-1445):
+    nearest-voxel slice of the current accumulators at the transform's
+    rotation (x=0 and Nyquist columns written Hermitian as the 2-D
+    set_complex_at writes them), shifted by its translation, and for
+    ret_fourier=0 moved to the centre and inverse transformed."""
+    from eman2_b200 import Transform
+    N, n = 32, 40
+    sl, rt = rand_slices(N, n, 151), rand_rots(n, 152)
+    w = np.ones(n, np.float32)
+    r = recon(N, "gauss_2", "c1")
+    r.insert_slices(sl, rt, w)
+    o = oracle_insert(N, sl, rt, w, "gauss_2", "c1")
+    for k in range(3):
+        rot = rand_rots(1, 160 + k)[0]
+        m = np.zeros((3, 4), np.float32)
+        m[:, :3] = rot
+        m[0, 3], m[1, 3] = shift
+        got = r.projection(Transform(m), ret_fourier).numpy()
+        want = o.projection(rot, shift[0], shift[1], bool(ret_fourier))
+        assert got.shape == ((N, N + 2) if ret_fourier else (N, N))
+        assert rel(got, want) < 2e-6 if ret_fourier else rel(got, want) < RTOL_FFT
+    # the x=0 column is Hermitian as the reference writes it
+    if ret_fourier:
+        c = got[:, 0] + 1j * got[:, 1]
+        for y in range(1, N // 2):
+            assert c[y] == np.conj(c[N - y])
