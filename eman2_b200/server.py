@@ -5,8 +5,14 @@ persistent insertion launch per tick (continuous batching: a request that
 arrives while others are on the GPU joins at the next tick once a slot and
 its memory are free).
 
+A job whose chunks are all inserted leaves the active set at once: with an
+executor that finishes asynchronously (``finish_async``), its normalise,
+inverse FFT and copy-out run on a stream of their own while the tick loop
+keeps inserting the other jobs, and the job completes (its memory is
+released) when that work has landed.
+
 The scheduler is plain Python (testable without a GPU through any executor
-with the same three methods); ``GpuExecutor`` runs it on the device.
+with the same methods); ``GpuExecutor`` runs it on the device.
 """
 from __future__ import annotations
 
@@ -40,6 +46,7 @@ class Job:
     done: float = 0.0
     footprint: int = 0
     result: object = None
+    pending: object = None         # an asynchronous finish in flight
 
     @property
     def finished_inserting(self) -> bool:
@@ -66,6 +73,7 @@ class Scheduler:
         self.chunks_per_tick = chunks_per_tick
         self.waiting: list[Request] = []
         self.active: list[Job] = []
+        self.finishing: list[Job] = []    # finish enqueued, memory still held
         self.done: list[Job] = []
         self.used = 0
         self.rejected: list[Request] = []
@@ -108,19 +116,42 @@ class Scheduler:
         return work
 
     def retire(self, now: float, executor) -> list[Job]:
+        """Jobs with every chunk inserted leave the active set (freeing their
+        slot).  An asynchronous executor's finish is only started here; the
+        job completes in collect().  Returns the jobs completed now."""
         out = []
         for job in list(self.active):
             if job.finished_inserting:
-                job.result = executor.finish(job.handle)
-                job.done = now
                 self.active.remove(job)
-                self.used -= job.footprint
-                self.done.append(job)
+                if hasattr(executor, "finish_async"):
+                    job.pending = executor.finish_async(job.handle)
+                    self.finishing.append(job)
+                else:
+                    job.result = executor.finish(job.handle)
+                    self._complete(job, now)
+                    out.append(job)
+        return out + self.collect(now, executor)
+
+    def collect(self, now: float, executor, wait: bool = False) -> list[Job]:
+        """Completes the jobs whose asynchronous finish has landed (all of
+        them, waiting, when ``wait``)."""
+        out = []
+        for job in list(self.finishing):
+            if wait or executor.finish_ready(job.pending):
+                job.result = executor.finish_result(job.pending)
+                job.pending = None
+                self.finishing.remove(job)
+                self._complete(job, now)
                 out.append(job)
         return out
 
+    def _complete(self, job: Job, now: float):
+        job.done = now
+        self.used -= job.footprint
+        self.done.append(job)
+
     def idle(self) -> bool:
-        return not self.waiting and not self.active
+        return not self.waiting and not self.active and not self.finishing
 
 
 def percentile(v, q):
@@ -137,6 +168,7 @@ class Server:
         self.sched = scheduler
         self.exe = executor
         self.clock = clock
+        self.trace: list[tuple] = []    # (time, "tick" | "finish_start" | "done", job ids)
 
     def run(self, requests: list[Request], timeout: float = 3600.0) -> dict:
         for r in sorted(requests, key=lambda r: r.arrival):
@@ -152,12 +184,22 @@ class Server:
             if work:
                 self.exe.insert([(job.handle, chunk) for job, chunk in work])
                 ticks += 1
-            self.sched.retire(self.clock() - t0, self.exe)
-            if not work and not self.sched.active and self.sched.waiting:
-                nxt = self.sched.waiting[0].arrival
-                wait = nxt - (self.clock() - t0)
-                if wait > 0:
-                    time.sleep(min(wait, 0.05))
+                self.trace.append((self.clock() - t0, "tick", [job.req.rid for job, _ in work]))
+            before = {id(j) for j in self.sched.finishing}
+            done = self.sched.retire(self.clock() - t0, self.exe)
+            started = [j.req.rid for j in self.sched.finishing if id(j) not in before]
+            if started:
+                self.trace.append((self.clock() - t0, "finish_start", started))
+            if done:
+                self.trace.append((self.clock() - t0, "done", [j.req.rid for j in done]))
+            if not work and not self.sched.active:
+                if self.sched.finishing:
+                    time.sleep(0.0002)          # poll the finishes in flight
+                elif self.sched.waiting:
+                    nxt = self.sched.waiting[0].arrival
+                    wait = nxt - (self.clock() - t0)
+                    if wait > 0:
+                        time.sleep(min(wait, 0.05))
         wall = self.clock() - t0
         lat = [j.done - j.req.arrival for j in self.sched.done]
         parts = sum(j.req.particles for j in self.sched.done)
@@ -169,16 +211,23 @@ class Server:
 
 class GpuExecutor:
     """Device execution for the scheduler: a resident FourierReconstructor per
-    job; each tick's chunks go through one fr_insert_particles_multi call.
+    job; each tick's chunks go through one fr_insert_particles_multi call on
+    the insertion stream; a retiring job's finish is enqueued
+    (fr_finish_async) on one of a few finish streams, into page-locked host
+    buffers, so it overlaps the next ticks.
 
     Finished jobs' reconstructors return to a pool keyed by their parameters;
     a later job with the same parameters takes one (setup() zeroes its
     accumulators) and so reuses its volumes, FFT plans and scratch instead of
     allocating them.  At most ``pool_bytes`` of idle volumes are kept."""
 
-    def __init__(self, doift: bool = False, stream=None, pool_bytes: int = 8 << 30):
+    def __init__(self, doift: bool = False, stream=None, pool_bytes: int = 8 << 30,
+                 finish_streams: int = 4):
         self.doift = doift
         self.stream = stream
+        self.nfinish = max(1, int(finish_streams))
+        self.finish_streams: list = []
+        self._next_fs = 0
         self.pool_bytes = int(pool_bytes)
         self.pool: dict = {}            # key -> [FourierReconstructor]
         self.pooled = 0
@@ -221,15 +270,35 @@ class GpuExecutor:
             items = later
         del recons
 
+    def finish_async(self, handle):
+        """Enqueues the job's finish on the next finish stream."""
+        import torch
+        if not self.finish_streams:
+            self.finish_streams = [torch.cuda.Stream() for _ in range(self.nfinish)]
+        fs = self.finish_streams[self._next_fs % self.nfinish]
+        self._next_fs += 1
+        return handle.finish_async(self.doift, stream=fs)
+
+    def finish_ready(self, pending) -> bool:
+        return pending.ready()
+
+    def finish_result(self, pending):
+        out = pending.result()
+        self._release(pending.owner)
+        return out
+
     def finish(self, handle):
         out = handle.finish(self.doift)
+        self._release(handle)
+        return out
+
+    def _release(self, handle):
         vol = handle._pool_bytes
         if self.pooled + vol <= self.pool_bytes:
             self.pool.setdefault(handle._pool_key, []).append(handle)
             self.pooled += vol
         else:
             handle.close()
-        return out
 
     def close(self):
         for free in self.pool.values():

@@ -243,3 +243,88 @@ def test_served_result_equals_alone(gpu):
         want_final = r.finish(False).numpy()
         got = by_id[k].result.numpy()
         assert oracle.rel_l2(got, want_final) < 1e-5
+
+
+def test_large_finish_does_not_hold_small_request(gpu):
+    """A retiring job's finish (normalise, 480^3 inverse FFT, a 442 MB map
+    copied out) runs on a finish stream of its own: the scheduler issues the
+    small request's next chunks while it is in flight, and on the device those
+    chunks are inserted before it lands.  Both results equal the jobs alone."""
+    import torch
+
+    from eman2_b200 import FourierReconstructor
+    from eman2_b200.particles import particle_meta
+    from eman2_b200.server import GpuExecutor, Request, Scheduler, Server
+    from eman2_b200.synth import make_particles
+
+    class Timed(GpuExecutor):
+        """Timing events around each tick and each finish."""
+        def __init__(self, **kw):
+            super().__init__(**kw)
+            self.ticks, self.finishes = [], {}
+
+        def insert(self, items):
+            super().insert(items)
+            ev = torch.cuda.Event(enable_timing=True)
+            ev.record(self.stream)
+            self.ticks.append(({id(h) for h, _ in items}, ev))
+
+        def finish_async(self, handle):
+            if not self.finish_streams:
+                self.finish_streams = [torch.cuda.Stream() for _ in range(self.nfinish)]
+            fs = self.finish_streams[self._next_fs % self.nfinish]
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(fs)
+            p = super().finish_async(handle)
+            e1.record(fs)
+            self.finishes[id(handle)] = (e0, e1)
+            return p
+
+    def chunks(ps, size):
+        n = len(ps.images)
+        cut = list(range(0, n, size)) + [n]
+        return [(ps.images[a:b], particle_meta(ps.rots[a:b], ps.shifts[a:b], ps.weights[a:b]))
+                for a, b in zip(cut[:-1], cut[1:])]
+
+    big = make_particles(320, 16, seed=401, snr=0.5, device=gpu)
+    small = make_particles(64, 48, seed=402, snr=0.5, device=gpu)
+    pb = {"size": [480] * 3, "sym": "c1", "mode": "gauss_2"}
+    psm = {"size": [96] * 3, "sym": "c1", "mode": "gauss_2"}
+    reqs = [Request(0, pb, chunks(big, 16), 0.0), Request(1, psm, chunks(small, 12), 0.0)]
+    exe = Timed(doift=True)
+    # warm-up with the same requests: plans, scratch and the pooled volumes
+    Server(Scheduler(hbm_budget=16 << 30, max_active=4), exe).run(reqs)
+    torch.cuda.synchronize()
+    exe.ticks.clear()
+    exe.finishes.clear()
+    sched = Scheduler(hbm_budget=16 << 30, max_active=4)
+    srv = Server(sched, exe)
+    srv.run(reqs)
+    torch.cuda.synchronize()
+    by = {j.req.rid: j for j in sched.done}
+    assert set(by) == {0, 1}
+    # host: small chunks issued after the big finish started, before it landed
+    t0 = next(t for t, kind, ids in srv.trace if kind == "finish_start" and 0 in ids)
+    t1 = next(t for t, kind, ids in srv.trace if kind == "done" and 0 in ids)
+    late = [t for t, kind, ids in srv.trace if kind == "tick" and 1 in ids and t0 < t < t1]
+    assert late
+    # device: a small-job tick issued in that window ran while the big finish
+    # was in flight
+    hbig, hsmall = by[0].handle, by[1].handle
+    e0, e1 = exe.finishes[id(hbig)]
+    small_ticks = [ev for ids, ev in exe.ticks if id(hsmall) in ids]
+    first_late = small_ticks[-len([t for t, kind, ids in srv.trace
+                                   if kind == "tick" and 1 in ids and t > t0])]
+    finish_ms = e0.elapsed_time(e1)
+    tick_ms = e0.elapsed_time(first_late)
+    print(f"\nbig finish {finish_ms:.2f} ms; the small job's first tick after it started done "
+          f"{tick_ms:.2f} ms after it began")
+    assert tick_ms < finish_ms
+    exe.close()
+    for rid, params, ps in ((0, pb, big), (1, psm, small)):
+        r = FourierReconstructor(params)
+        r.setup()
+        r.insert_particles(ps.images, particle_meta(ps.rots, ps.shifts, ps.weights))
+        want = r.finish(True).numpy()
+        r.close()
+        assert oracle.rel_l2(by[rid].result.numpy(), want) < 1e-5

@@ -207,6 +207,54 @@ def test_scheduler_joins_late_arrivals_at_next_tick():
     assert len(sched.tick_work()) == 2     # both in the same tick now
 
 
+class FakeAsyncExecutor(FakeExecutor):
+    """Finishes land only after `delay` polls, as a finish enqueued on its own
+    stream lands some ticks later."""
+
+    def __init__(self, delay=3):
+        super().__init__()
+        self.delay = delay
+
+    def finish_async(self, h):
+        return {"h": h, "polls": 0}
+
+    def finish_ready(self, p):
+        p["polls"] += 1
+        return p["polls"] > self.delay
+
+    def finish_result(self, p):
+        self.finished += 1
+        return p["h"]["chunks"]
+
+
+def test_scheduler_keeps_ticking_while_a_finish_is_in_flight():
+    """A retiring job's asynchronous finish does not hold the tick loop: the
+    other job's chunks are inserted while it is in flight, and its memory is
+    released only once it has landed."""
+    from eman2_b200.server import Scheduler, Server, footprint_bytes
+    big, small = _req(0, 192, 1), _req(1, 96, 4)
+    sched = Scheduler(hbm_budget=1 << 40, max_active=4)
+    exe = FakeAsyncExecutor(delay=5)
+    srv = Server(sched, exe)
+    res = srv.run([big, small])
+    assert res["requests"] == 2 and sched.used == 0
+    t_big_start = next(t for t, kind, ids in srv.trace if kind == "finish_start" and 0 in ids)
+    t_big_done = next(t for t, kind, ids in srv.trace if kind == "done" and 0 in ids)
+    small_ticks = [t for t, kind, ids in srv.trace if kind == "tick" and 1 in ids]
+    assert any(t_big_start < t < t_big_done for t in small_ticks)
+    assert sorted(j.result for j in sched.done) == [1, 4]
+    # while in flight the big job still holds its memory
+    sched2 = Scheduler(hbm_budget=1 << 40, max_active=4)
+    sched2.submit(_req(0, 192, 1))
+    sched2.admit(0.0, exe)
+    sched2.tick_work()
+    sched2.retire(0.0, exe)
+    assert not sched2.active and len(sched2.finishing) == 1
+    assert sched2.used == footprint_bytes({"size": [192] * 3}, 128, 8)
+    sched2.collect(0.1, exe, wait=True)
+    assert sched2.used == 0 and sched2.idle()
+
+
 def test_batched_call_argument_marshalling():
     """The batched calls hand the library contiguous float32 particles and the
     addresses of fr_particle arrays: float32 contiguous tensors pass through
