@@ -47,6 +47,10 @@ WORKLOADS = {
 
 
 def nsym_of(sym: str) -> int:
+    sym = sym.lower()
+    platonic = {"tet": 12, "oct": 24, "icos": 60, "icos5": 60}
+    if sym in platonic:
+        return platonic[sym]
     k, n = sym[0], int(sym[1:] or 1)
     return n if k == "c" else 2 * n
 
@@ -189,31 +193,51 @@ def cpu_sample(wl: dict, seed: int, budget_s: float = 15.0, max_n: int = 64, thr
 
 
 # ------------------------------------------------------------------ serving
-def serving_requests(dev, seed: int, nreq: int, rate: float, max_particles: int, chunk: int):
-    """A seeded stream of reconstruction requests: boxes {64, 128, 192, 256}
-    padded x1.5, particle counts log-uniform over [1000, max_particles], sym
-    c1/c4/d7, gauss_2, CTF, chunks of `chunk`; Poisson arrivals at `rate`/s."""
+SERVE_BOXES = (64, 128, 192, 256, 320)
+
+
+def _meta_view(meta, a, b):
+    """Entries a..b-1 of an fr_particle array, without a copy."""
+    from eman2_b200 import _lib
+    sz = ctypes.sizeof(_lib.fr_particle)
+    return (_lib.fr_particle * (b - a)).from_address(ctypes.addressof(meta) + a * sz)
+
+
+def particle_pools(dev, boxes, n: int, seed: int):
+    """Per box, n seeded particles on the device (CTF, SNR 0.05, shifts U(-4, 4),
+    weights U(0.5, 1)) and their metadata.  Requests and jobs take views of
+    these, so their particles repeat every n."""
     from eman2_b200.particles import particle_meta
-    from eman2_b200.server import Request
     from eman2_b200.synth import make_particles
+    out = {}
+    for box in boxes:
+        ps = make_particles(box, n, seed=seed + box, snr=0.05, shift=4.0, weights=(0.5, 1.0),
+                            ctf=True, device=dev)
+        out[box] = (ps.images, particle_meta(ps.rots, ps.shifts, ps.weights, defocus=ps.defocus))
+    return out
+
+
+def serving_requests(pools, seed: int, nreq: int, rate: float, chunk: int,
+                     pmin: int = 1000, pmax: int = 100_000):
+    """A seeded stream of reconstruction requests of the serving configuration:
+    box uniform over SERVE_BOXES padded x1.5, particle count log-uniform over
+    [pmin, pmax], sym c1/c4/d7, gauss_2, CTF, chunks of `chunk`, Poisson
+    arrivals at `rate`/s."""
+    from eman2_b200.server import Request
     rng = np.random.default_rng(seed)
-    boxes = (64, 128, 192, 256)
-    pools = {box: make_particles(box, 1024, seed=seed + box, snr=0.05, shift=4.0,
-                                 weights=(0.5, 1.0), ctf=True, device=dev) for box in boxes}
     reqs, t = [], 0.0
     for k in range(nreq):
-        box = int(rng.choice(boxes))
-        n = int(np.exp(rng.uniform(np.log(1000), np.log(max_particles))))
+        box = int(rng.choice(SERVE_BOXES))
+        n = int(np.exp(rng.uniform(np.log(pmin), np.log(pmax))))
         sym = str(rng.choice(["c1", "c4", "d7"]))
-        ps = pools[box]
+        imgs, meta = pools[box]
         chunks = []
         for a in range(0, n, chunk):
-            idx = np.arange(a, min(n, a + chunk)) % 1024
-            chunks.append((ps.images[idx], particle_meta(ps.rots[idx], ps.shifts[idx],
-                                                         ps.weights[idx], defocus=ps.defocus[idx])))
+            m = min(chunk, n - a)
+            chunks.append((imgs[:m], _meta_view(meta, 0, m)))
         t += float(rng.exponential(1.0 / rate))
         reqs.append(Request(k, {"size": [box * 3 // 2] * 3, "sym": sym, "mode": "gauss_2"},
-                            chunks, arrival=t))
+                            chunks, arrival=t, particles=n))
     return reqs
 
 
@@ -227,34 +251,37 @@ def fifo_latency(arrivals, service):
     return lat
 
 
-def run_serving(dev, seed: int = 4242, nreq: int = 12, rate: float = 4.0,
-                max_particles: int = 8000, chunk: int = 2048, plain_sample: int = 24):
-    """The served form against the plain per-job GPU path on one request stream.
-    Served: continuous batching (fr_insert_particles_multi per tick over every
-    active job), measured saturated (all requests at t=0: throughput) and
-    under Poisson arrivals (p50/p99 latency).  Plain: each request through its
-    own FourierReconstructor with one insert call per particle (the drop-in
-    insert_slice form), timed on `plain_sample` particles per request and
-    scaled to its count; its latency is that of a single FIFO server given
-    those service times and the same arrivals."""
+def run_serving(dev, seed: int = 4242, nreq: int = 128, rate: float = 4.0, chunk: int = 2048,
+                plain_sample: int = 24, plain_every: int = 4):
+    """The served form against the plain per-job GPU path on one request stream
+    of the serving configuration (boxes 64-320 x1.5, 1,000-100,000 particles
+    log-uniform, c1/c4/d7, gauss_2, CTF, chunks of 2048, Poisson arrivals).
+    Served: continuous batching (one fr_insert_particles_multi per tick over
+    every active job; finishes on their own streams), p50/p99 latency and
+    throughput over the stream.  Plain: each request through its own
+    FourierReconstructor with one insert call per particle (the drop-in
+    insert_slice form), timed on `plain_sample` particles of every
+    `plain_every`-th request and scaled to its count; its latency is that of
+    a single FIFO server given those service times and the same arrivals."""
     import dataclasses
 
     import torch
 
-    from eman2_b200 import FourierReconstructor, _lib
+    from eman2_b200 import FourierReconstructor
     from eman2_b200.server import GpuExecutor, Scheduler, Server
-    reqs = serving_requests(dev, seed, nreq, rate, max_particles, chunk)
-    at0 = [dataclasses.replace(r, arrival=0.0) for r in reqs]
+    pools = particle_pools(dev, SERVE_BOXES, chunk, seed)
+    reqs = serving_requests(pools, seed, nreq, rate, chunk)
     parts = sum(r.particles for r in reqs)
     budget = int(torch.cuda.mem_get_info()[0] * 0.5)
     exe = GpuExecutor(doift=False)
-    Server(Scheduler(budget, max_active=16), exe).run(at0)            # warm-up (untimed)
+    warm = [dataclasses.replace(r, arrival=0.0) for r in reqs[:6]]
+    Server(Scheduler(budget, max_active=16), exe).run(warm)            # warm-up (untimed)
     torch.cuda.synchronize()
-    sat = Server(Scheduler(budget, max_active=16), exe).run(at0)
-    torch.cuda.synchronize()
-    poi = Server(Scheduler(budget, max_active=16), exe).run(reqs)
+    srv = Server(Scheduler(budget, max_active=16), exe)
+    poi = srv.run(reqs)
     torch.cuda.synchronize()
     exe.close()
+    lat = sorted(j.done - j.req.arrival for j in srv.sched.done)
 
     def per_job(r, k=None, schedule="scatter"):
         """Seconds for request r alone: setup, insert (k particles one per
@@ -269,10 +296,8 @@ def run_serving(dev, seed: int = 4242, nreq: int = 12, rate: float = 4.0,
                 rec.insert_particles(img, meta, schedule=schedule)
         else:
             img, meta = r.chunks[0]
-            sz = ctypes.sizeof(_lib.fr_particle)
             for i in range(min(k, len(meta))):
-                one = (_lib.fr_particle * 1).from_address(ctypes.addressof(meta) + i * sz)
-                rec.insert_particles(img[i:i + 1], one, schedule=schedule)
+                rec.insert_particles(img[i:i + 1], _meta_view(meta, i, i + 1), schedule=schedule)
         torch.cuda.synchronize()
         t2 = time.perf_counter()
         rec.finish(False)
@@ -280,30 +305,40 @@ def run_serving(dev, seed: int = 4242, nreq: int = 12, rate: float = 4.0,
         rec.close()
         return (t1 - t0) + (t3 - t2), t2 - t1
 
-    for r in reqs[:4]:
+    sample = reqs[::plain_every]
+    for r in sample[:3]:
         per_job(r, 4)                                                  # warm-up
-    service = []
-    for r in reqs:
+    service, s_parts = [], 0
+    for r in sample:
         fixed, ins = per_job(r, plain_sample)
         service.append(fixed + ins * r.particles / min(plain_sample, r.particles))
-    chunked = sum(sum(per_job(r, None, "auto")) for r in reqs)
-    plain_lat = fifo_latency([r.arrival for r in reqs], service)
-    served_sat = parts / sat["wall_s"]
-    plain_rate = parts / sum(service)
+        s_parts += r.particles
+    plain_rate = s_parts / sum(service)
+    # the plain path's latency on the whole stream: each request's service
+    # time from the sampled rate of its (box, sym) class or, failing that,
+    # the overall rate
+    rate_of = {}
+    for r, sv in zip(sample, service):
+        rate_of.setdefault((r.params["size"][0], r.params["sym"]), []).append(r.particles / sv)
+    est = [r.particles / float(np.mean(rate_of.get((r.params["size"][0], r.params["sym"]),
+                                                   [plain_rate])))
+           for r in reqs]
+    plain_lat = fifo_latency([r.arrival for r in reqs], est)
+    served_rate = parts / poi["wall_s"]
     return {
         "served": {"p50_s": poi["p50_s"], "p99_s": poi["p99_s"],
-                   "particle_slices_per_s_saturated": served_sat,
-                   "particle_slices_per_s_poisson": parts / poi["wall_s"],
-                   "ticks_saturated": sat["ticks"], "requests": poi["requests"]},
+                   "p90_s": percentile(lat, 90), "max_s": lat[-1] if lat else None,
+                   "particle_slices_per_s": served_rate, "wall_s": poi["wall_s"],
+                   "ticks": poi["ticks"], "requests": poi["requests"], "particles": parts},
         "plain_per_particle": {"particle_slices_per_s": plain_rate,
                                "p50_s": percentile(plain_lat, 50), "p99_s": percentile(plain_lat, 99),
-                               "sample": f"{plain_sample} particles per request, scaled to its count; "
-                                         "latency from a FIFO single server under the same arrivals"},
-        "per_job_chunked": {"particle_slices_per_s": parts / chunked,
-                            "note": f"each request alone, one insert call per chunk of {chunk}"},
-        "speedup_served_vs_plain": served_sat / plain_rate,
-        "stream": f"{nreq} requests, Poisson {rate}/s, boxes 64/128/192/256 x1.5, "
-                  f"1000-{max_particles} particles, c1/c4/d7, gauss_2, CTF, chunks of {chunk}",
+                               "sample": f"{plain_sample} particles of every {plain_every}th request, "
+                                         "scaled to its count; latency from a FIFO single server "
+                                         "under the same arrivals"},
+        "speedup_served_vs_plain": served_rate / plain_rate,
+        "stream": f"{nreq} requests, Poisson {rate}/s, boxes {'/'.join(map(str, SERVE_BOXES))} x1.5, "
+                  f"1,000-100,000 particles log-uniform, c1/c4/d7, gauss_2, CTF, chunks of {chunk}; "
+                  f"particles repeat within a box's pool of {chunk}",
     }
 
 
@@ -425,112 +460,145 @@ def run_io(dev, wl: dict, n: int = 16384, chunk: int = 4096):
 
 
 # ------------------------------------------------------------------ batched
-def run_batched(dev, seed: int = 33, pairs: int = 32, reps: int = 5, plain_sample: int = 16):
-    """The batched form on a round of 64 reconstructions: 32 even/odd
-    half-map pairs, boxes {64, 96, 128, 160} padded x1.5,
-    sym c1/d7, gauss_2/gauss_5 (each 50/50), CTF; per round every job inserts
-    a chunk of log-uniform [64, 512] particles.  Schedules come from the
-    autotuner; the round is captured once as a CUDA graph and replayed.
-    Reported beside the same rounds without the graph and the plain
-    per-particle path (sampled)."""
+BATCH_BOXES = (64, 96, 128, 160)
+
+
+def config3_jobs(seed: int = 33, pairs: int = 32):
+    """The batched configuration's 64 reconstructions: 32 even/odd half-map
+    pairs, each pair a box from BATCH_BOXES (padded x1.5), sym c1 or d7, mode
+    gauss_2 or gauss_5 (each 50/50); a pair's particle count is log-uniform
+    over [1,000, 100,000] and split evenly, so each reconstruction's count is
+    log-uniform over [500, 50,000]."""
+    rng = np.random.default_rng(seed)
+    jobs = []
+    for _ in range(pairs):
+        b = int(rng.choice(BATCH_BOXES))
+        sym, mode = str(rng.choice(["c1", "d7"])), str(rng.choice(["gauss_2", "gauss_5"]))
+        n = int(np.exp(rng.uniform(np.log(1000), np.log(100_000))))
+        for half in range(2):
+            jobs.append({"params": {"size": [b * 3 // 2] * 3, "sym": sym, "mode": mode},
+                         "box": b, "count": (n + 1 - half) // 2})
+    return jobs
+
+
+def run_batched(dev, seed: int = 33, chunk: int = 2048, graph_chunk: int = 512, reps: int = 3,
+                plain_sample: int = 16):
+    """The batched form on the batched configuration's draw of 64
+    reconstructions (config3_jobs): every particle of every job, inserted in
+    rounds of up to `chunk` particles per job (one multi-job launch sequence
+    per round, schedules from the autotuner), device-timed; and one round of
+    the first `graph_chunk` particles of every job captured as a CUDA graph
+    and replayed.  Beside them the plain per-particle path, sampled."""
     import torch
 
-    from eman2_b200 import FourierReconstructor, _lib
+    from eman2_b200 import FourierReconstructor
     from eman2_b200.batch import BatchReconstructor, autotune, insert_particles_multi, set_tile
-    from eman2_b200.particles import particle_meta
-    from eman2_b200.synth import make_particles
-    rng = np.random.default_rng(seed)
-    sizes = (64, 96, 128, 160)
-    pools = {b: make_particles(b, 1024, seed=seed + b, snr=0.05, shift=4.0, weights=(0.5, 1.0),
-                               ctf=True, device=dev) for b in sizes}
-    params, boxes, counts, imgs, metas = [], [], [], [], []
-    for _ in range(pairs):
-        b = int(rng.choice(sizes))
-        sym, mode = str(rng.choice(["c1", "d7"])), str(rng.choice(["gauss_2", "gauss_5"]))
-        n = int(np.exp(rng.uniform(np.log(64), np.log(512))))
-        for half in range(2):                       # even / odd particles of one phantom
-            idx = np.arange(half, 2 * n, 2) % 1024
-            ps = pools[b]
-            params.append({"size": [b * 3 // 2] * 3, "sym": sym, "mode": mode})
-            boxes.append(b)
-            counts.append(n)
-            imgs.append(ps.images[idx])
-            metas.append(particle_meta(ps.rots[idx], ps.shifts[idx], ps.weights[idx],
-                                       defocus=ps.defocus[idx]))
+    jobs = config3_jobs(seed)
+    params = [j["params"] for j in jobs]
+    boxes = [j["box"] for j in jobs]
+    counts = [j["count"] for j in jobs]
     total = sum(counts)
+    pools = particle_pools(dev, BATCH_BOXES, chunk, seed)
     combos = {}
     for p, n in zip(params, counts):
         key = (p["size"][0], p["mode"], nsym_of(p["sym"]))
-        combos[key] = max(combos.get(key, 0), n)
+        combos[key] = max(combos.get(key, 0), min(n, chunk))
     tuned = {f"N{k[0]} {k[1]} nsym{k[2]}": autotune(k[0], k[1], k[2], nparticles=n)[0]
              for k, n in combos.items()}
     stream = torch.cuda.Stream(device=dev)
 
-    def timed(fn):
-        for _ in range(2):
-            fn()
+    def rounds(recons, upto=None):
+        """Every job's particles (or its first `upto`), round by round."""
+        left = list(counts) if upto is None else [min(c, upto) for c in counts]
+        while any(left):
+            act = [j for j in range(len(jobs)) if left[j] > 0]
+            m = [min(chunk, left[j]) for j in act]
+            insert_particles_multi([recons[j] for j in act],
+                                   [pools[boxes[j]][0][:k] for j, k in zip(act, m)],
+                                   [_meta_view(pools[boxes[j]][1], 0, k) for j, k in zip(act, m)],
+                                   stream)
+            for j, k in zip(act, m):
+                left[j] -= k
+
+    def timed(fn, n):
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        for _ in range(reps):
+        for _ in range(n):
             fn()
         e1.record(stream)
         e1.synchronize()
-        return e0.elapsed_time(e1) / reps
+        return e0.elapsed_time(e1) / n
 
     try:
         b1 = BatchReconstructor(params)
-        ms_multi = timed(lambda: insert_particles_multi(b1.recons, imgs, metas, stream))
+        rounds(b1.recons, upto=chunk)                                   # warm-up: scratch, plans
+        ms_full = timed(lambda: rounds(b1.recons), 1)
         b1.close()
+        gcounts = [min(c, graph_chunk) for c in counts]
         b2 = BatchReconstructor(params)
         t0 = time.perf_counter()
-        g = b2.capture(boxes, counts, [True] * len(params), stream=stream)
+        g = b2.capture(boxes, gcounts, [True] * len(params), stream=stream)
         capture_s = time.perf_counter() - t0
-        ms_graph = timed(lambda: g.launch(imgs, metas))
+        gimgs = [pools[b][0][:k] for b, k in zip(boxes, gcounts)]
+        gmetas = [_meta_view(pools[b][1], 0, k) for b, k in zip(boxes, gcounts)]
+        g.launch(gimgs, gmetas)
+        ms_graph = timed(lambda: g.launch(gimgs, gmetas), reps)
+        ms_multi = timed(lambda: insert_particles_multi(b2.recons, gimgs, gmetas, stream), reps)
         g.close()
         b2.close()
     finally:
         for k in combos:
             set_tile(k[0], k[1], k[2], -1)
-    sz = ctypes.sizeof(_lib.fr_particle)
     spent, done = 0.0, 0
     for j in range(0, len(params), 4):
         rec = FourierReconstructor(params[j])
         rec.setup()
+        imgs, meta = pools[boxes[j]]
+        rec.insert_particles(imgs[:1], _meta_view(meta, 0, 1), schedule="scatter")
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        for i in range(min(plain_sample, counts[j])):
-            one = (_lib.fr_particle * 1).from_address(ctypes.addressof(metas[j]) + i * sz)
-            rec.insert_particles(imgs[j][i:i + 1], one, schedule="scatter")
+        for i in range(plain_sample):
+            rec.insert_particles(imgs[i:i + 1], _meta_view(meta, i, i + 1), schedule="scatter")
         torch.cuda.synchronize()
         spent += time.perf_counter() - t0
-        done += min(plain_sample, counts[j])
+        done += plain_sample
         rec.close()
     plain = done / spent
-    graph_rate = total / (ms_graph / 1e3)
-    overhead = per_job_overhead(params, boxes, imgs, metas, stream, reps)
-    return {"jobs": len(params), "particles_per_round": total,
-            "graph": {"ms_per_round": ms_graph, "particle_slices_per_s": graph_rate,
-                      "capture_s": capture_s},
-            "no_graph": {"ms_per_round": ms_multi, "particle_slices_per_s": total / (ms_multi / 1e3)},
+    full_rate = total / (ms_full / 1e3)
+    gparts = sum(gcounts)
+    graph_rate = gparts / (ms_graph / 1e3)
+    overhead = per_job_overhead(params, boxes, [pools[b][0] for b in boxes],
+                                [pools[b][1] for b in boxes], stream, reps)
+    return {"jobs": len(params), "particles": total,
+            "counts": {"min": min(counts), "median": float(np.median(counts)), "max": max(counts)},
+            "all_particles": {"ms": ms_full, "particle_slices_per_s": full_rate,
+                              "rounds_of": chunk},
+            "graph_round": {"ms_per_round": ms_graph, "particles_per_round": gparts,
+                            "particle_slices_per_s": graph_rate, "capture_s": capture_s,
+                            "no_graph_ms_per_round": ms_multi},
             "plain_per_particle": {"particle_slices_per_s": plain,
                                    "sample": f"{plain_sample} particles of every 4th job"},
-            "speedup_batched_vs_plain": graph_rate / plain,
+            "speedup_batched_vs_plain": full_rate / plain,
             "per_job_overhead": overhead,
-            "autotuned": tuned}
+            "autotuned": tuned,
+            "draw": "32 even/odd pairs, boxes 64/96/128/160 x1.5, c1/d7, gauss_2/gauss_5, "
+                    "500-50,000 particles per job log-uniform, CTF; particles repeat within a "
+                    f"box's pool of {chunk}"}
 
 
-def per_job_overhead(params, boxes, imgs, metas, stream, reps: int = 5):
-    """Per-job latency overhead of the plain path against the batched form,
-    on the round's 64 jobs with ONE particle each.  "empty": the particle has
-    weight 0, so every stage runs (host call, metadata, prologue launches,
-    insertion launch, synchronisation) but no tap is added: the job's time is
-    all fixed cost.  "one_particle": weight as drawn, schedules from the
-    autotuner for one particle; a gauss_5 d7 job at N=240 is still ~7e7 taps,
-    so this one is mostly insertion.  Plain: one insert call per job, waited
-    for before the next (the drop-in loop's latency).  Batched: one replay of
-    a graph of all jobs (and one multi-job call without the graph), divided by
-    the job count.  Wall-clock, since the overhead is host and launch time."""
+def per_job_overhead(params, boxes, pool_imgs, pool_metas, stream, reps: int = 5):
+    """Per-job latency overhead of the plain path against the batched form, on
+    the 64 jobs with ONE particle each, under one rule for both arms: every
+    call is enqueued and the round is waited for once at its end (what a
+    drop-in insert_slice loop does: the ABI returns once work is enqueued).
+    "empty": the particle has weight 0, so every stage runs (host call,
+    metadata, prologue launches, insertion launch) but no tap is added, so
+    the time is all fixed cost; "one_particle": weight as drawn, schedules
+    autotuned for one particle.  Plain: one insert call per job.  Batched: one
+    replay of a graph of all jobs (and one multi-job call without the
+    graph).  Wall-clock per round divided by the job count, since the
+    overhead is host and launch time."""
     import torch
 
     from eman2_b200 import _lib
@@ -539,7 +607,7 @@ def per_job_overhead(params, boxes, imgs, metas, stream, reps: int = 5):
     combos = {(p["size"][0], p["mode"], nsym_of(p["sym"])) for p in params}
     tuned = {f"N{k[0]} {k[1]} nsym{k[2]}": autotune(k[0], k[1], k[2], nparticles=1)[0]
              for k in combos}
-    one_imgs = [im[:1] for im in imgs]
+    one_imgs = [im[:1] for im in pool_imgs]
 
     def first(m, weight=None):
         a = (_lib.fr_particle * 1)()
@@ -551,22 +619,22 @@ def per_job_overhead(params, boxes, imgs, metas, stream, reps: int = 5):
     def wall(fn, n):
         for _ in range(2):
             fn()
-        stream.synchronize()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for _ in range(n):
             fn()
-        stream.synchronize()
         torch.cuda.synchronize()
         return (time.perf_counter() - t0) / n
 
     def measure(one_metas):
         bp = BatchReconstructor(params)
         try:
+            for r in bp.recons:
+                _lib.check(_lib.load().fr_set_stream(r.handle, ctypes.c_void_p(stream.cuda_stream)))
+
             def plain_round():
                 for j in range(nj):
                     bp.recons[j].insert_particles(one_imgs[j], one_metas[j], schedule="scatter")
-                    torch.cuda.synchronize()
             plain_s = wall(plain_round, reps)
             multi_s = wall(lambda: insert_particles_multi(bp.recons, one_imgs, one_metas, stream),
                            reps)
@@ -584,12 +652,105 @@ def per_job_overhead(params, boxes, imgs, metas, stream, reps: int = 5):
                 "graph_ms_per_job": ms(graph_s), "removed_x": plain_s / graph_s}
 
     try:
-        empty = measure([first(m, 0.0) for m in metas])
-        one = measure([first(m) for m in metas])
+        empty = measure([first(m, 0.0) for m in pool_metas])
+        one = measure([first(m) for m in pool_metas])
     finally:
         for k in combos:
             set_tile(k[0], k[1], k[2], -1)
-    return {"jobs": nj, "empty": empty, "one_particle": one, "autotuned_one_particle": tuned}
+    return {"jobs": nj, "rule": "every call enqueued, the round waited for once at its end",
+            "empty": empty, "one_particle": one, "autotuned_one_particle": tuned}
+
+
+# ------------------------------------------------------------------ accuracy
+def run_accuracy(dev):
+    """Accuracy at the configurations' sizes (the harness of
+    tests/test_gpu_accuracy.py): box 64 -> 96, 2,000 particles and box 128 ->
+    192, 20,000 particles in full, and a 16-particle sample of the box 256 ->
+    384, gauss_5, d7 job, each through the plain and the batched form against
+    the FP32-faithful, exact-sum and FP64 oracles."""
+    from tests import accuracy_harness as H
+    out = {}
+    for name, kw in (("c1", {}), ("c2", {}), ("c4", {"n": 16, "tasks": 16})):
+        t0 = time.perf_counter()
+        rep = H.run_case(name, dev, **kw)
+        summary = {"particles": rep["case"]["particles"], "box": rep["case"]["box"],
+                   "pad": rep["case"]["N"], "mode": rep["case"]["mode"], "sym": rep["case"]["sym"],
+                   "fp32_oracle_vs_fp64": {k: rep["fp32_oracle_vs_fp64"][k]
+                                           for k in ("rel_l2_complex", "rel_l2_weight", "fsc_min")}}
+        for form in ("plain", "batched"):
+            summary[form] = {against: {k: rep[form][against][k]
+                                       for k in ("rel_l2_complex", "rel_l2_weight", "fsc_min",
+                                                 "support_mismatch")}
+                             for against in ("vs_fp32_oracle", "vs_exact_sums", "vs_fp64_oracle")}
+        if "agreement_max_rel_diff" in rep:
+            summary["agreement_max_rel_diff"] = rep["agreement_max_rel_diff"]
+        summary["seconds"] = time.perf_counter() - t0
+        out[name] = summary
+    out["bar"] = ("relative L2 <= 1e-5 of finish(False) and normout against the FP32 oracle, "
+                  "FSC >= 0.9999 in every shell (the reference's shell rule)")
+    return out
+
+
+# ------------------------------------------------------------------ target configuration
+def run_target(dev, steps: int = 3, plain_n: int = 64):
+    """Box 256 padded to 384, gauss_2, d7 (the targets' configuration): the
+    batched form (2,048 particles per call through the pixel-major gather
+    kernel) against the plain form (one insert call per particle, scatter),
+    both device-timed on the library stream with particles in HBM, and
+    the pixel kernel's update roofline against the shared-atomic peak."""
+    import torch
+
+    from eman2_b200 import Reconstructors, _lib
+    from eman2_b200.particles import particle_meta
+    from eman2_b200.synth import make_particles
+    lib = _lib.load()
+    wl = WORKLOADS["c4g2"]
+    N, B = wl["N"], wl["box"]
+    ps = make_particles(B, 2048, seed=1300, snr=wl["snr"], shift=wl["shift"], weights=wl["weights"],
+                        ctf=True, device=dev)
+    meta = particle_meta(ps.rots, ps.shifts, ps.weights, defocus=ps.defocus)
+    r = Reconstructors.get("fourier", {"size": [N] * 3, "sym": wl["sym"], "mode": wl["mode"]})
+    r.setup()
+    stream = torch.cuda.Stream(device=dev)
+    _lib.check(lib.fr_set_stream(r.handle, ctypes.c_void_p(stream.cuda_stream)))
+    for _ in range(2):
+        r.insert_particles(ps.images, meta)
+    torch.cuda.synchronize()
+    _lib.check(lib.fr_profile(1))
+    _lib.check(lib.fr_stats_reset())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        r.insert_particles(ps.images, meta)
+    e1.record(stream)
+    e1.synchronize()
+    st = _lib.stats()
+    _lib.check(lib.fr_profile(0))
+    batched = steps * 2048 / (e0.elapsed_time(e1) / 1e3)
+    for i in range(3):
+        r.insert_particles(ps.images[i:i + 1], _meta_view(meta, i, i + 1), schedule="scatter")
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for i in range(plain_n):
+        r.insert_particles(ps.images[i:i + 1], _meta_view(meta, i, i + 1), schedule="scatter")
+    e1.record(stream)
+    e1.synchronize()
+    plain = plain_n / (e0.elapsed_time(e1) / 1e3)
+    r.close()
+    gms = st["gather_ms"] / max(1, st["gather_launches"])
+    taps = nsym_of(wl["sym"]) * pixels_per_slice(N) * 8 * 2048 / (gms / 1e3)
+    upd = update_peaks()
+    out = {"workload": wl["desc"], "batched": {"value": batched, "unit": "particle-slices/s",
+                                               "particles_per_call": 2048, "kernel": "k_pixel",
+                                               "avg_launch_ms": gms},
+           "plain": {"value": plain, "unit": "particle-slices/s", "sample": plain_n,
+                     "kernel": "k_scatter"},
+           "batched_vs_plain": batched / plain}
+    if upd is not None:
+        out["update_roofline"] = {"bound": "shared-memory FP32 atomics (3 per tap)",
+                                  "achieved": taps, "peak": upd["smem_atom"], "unit": "taps/s",
+                                  "frac": taps / upd["smem_atom"]}
+    return out
 
 
 # ------------------------------------------------------------------ GPU run
@@ -706,7 +867,10 @@ def main():
     ap.add_argument("--agree", type=int, default=256,
                     help="slices timed through the agreement pass (0: skip)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--no-serve", action="store_true", help="skip the batched and serving legs")
+    ap.add_argument("--no-serve", action="store_true",
+                    help="skip the target, finish, I/O, batched and serving legs")
+    ap.add_argument("--no-accuracy", action="store_true",
+                    help="skip the accuracy leg (GPU forms against the oracles)")
     ap.add_argument("--tile", type=int, default=-1,
                     help="pin the insertion kernel (0-3 register tiles, 4 staged column, 6 pixel-major, "
                          "5 barrier-free column, -2 scatter); default: library choice")
@@ -784,10 +948,15 @@ def main():
         "clocks": clk,
     }
     if upd is not None:
-        # the binding roof: the rate of the accumulator update the kernel uses
-        key = "smem_rmw" if st["gather_launches"] > 0 else "l2_red"
+        # the binding roof: the rate of the accumulator update the kernel
+        # uses (the column kernel: one shared float4 read-modify-write per
+        # tap; the pixel kernel: three shared FP32 atomics; the scatter:
+        # three L2 reductions)
+        key = ("l2_red" if st["gather_launches"] == 0 else
+               "smem_atom" if kname.startswith("k_pixel") else "smem_rmw")
         line["update_roofline"] = {
             "bound": {"smem_rmw": "shared-memory float4 read-modify-write",
+                      "smem_atom": "shared-memory FP32 atomics (3 per tap)",
                       "l2_red": "L2 red.global.add.f32 (3 per tap)"}[key],
             "achieved": taps_s, "peak": upd[key], "unit": "taps/s", "frac": taps_s / upd[key],
             "peaks_measured": upd, "taps": "upper bound S*p(N)*window"}
@@ -798,10 +967,15 @@ def main():
                              "speedup_batched_vs_plain": value / plain}
     if not args.no_serve and ws == 1:
         import torch
-        line["finish"] = run_finish(torch.device("cuda", local), wl)
-        line["io"] = run_io(torch.device("cuda", local), WORKLOADS["c2"])
-        line["batched"] = run_batched(torch.device("cuda", local))
-        line["serving"] = run_serving(torch.device("cuda", local))
+        dev = torch.device("cuda", local)
+        line["target_c4g2"] = run_target(dev)
+        line["finish"] = run_finish(dev, wl)
+        line["io"] = run_io(dev, WORKLOADS["c2"])
+        line["batched"] = run_batched(dev)
+        line["serving"] = run_serving(dev)
+    if not args.no_accuracy and ws == 1:
+        import torch
+        line["accuracy"] = run_accuracy(torch.device("cuda", local))
     if not args.no_cpu and ws == 1:
         v, n, thr, secs = cpu_sample(wl, seed=7000)
         line["cpu_baseline"] = {"value": v, "unit": "particle-slices/s", "cores": thr,
