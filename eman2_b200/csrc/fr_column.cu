@@ -367,14 +367,18 @@ __device__ void tile_item(const InsertJob &J, int tile, int s0, int s1, const Sm
 // axis A; within a group every thread walks all slices for its own column,
 // computing each candidate pixel's coordinates itself (the same exact
 // operations), so threads never wait for one another until A changes.
+// Three CTAs of 256 threads per SM (24 warps; the kernel is bound by
+// latency, so warps count most): shared memory is the 64 KB accumulator
+// tile plus compact tables (16-bit slice offsets and row limits; the
+// fast_exp table serves gauss_2 too, with the same exact index), ~74 KB.
 struct Smem3 {
   float4 *acc;      // [NV]
-  float4 *steps;    // gauss_2 step table
-  float *exp;       // [1000] fast_exp table (gauss_5)
+  float4 *steps;    // (not used by this kernel)
+  float *exp;       // [1000] fast_exp table
   float *rtab;      // [N+2]
-  int *xmax;        // [N]
-  int *hits;        // [block] grouped by axis
-  int *tmp;         // [block]
+  short *xmax;      // [N]
+  unsigned short *hits;  // [block] slice - s0, grouped by axis
+  unsigned short *tmp;   // [block] (slice - s0) | group << 14
   int *wcount;      // [3 * NT/32]
   int *gcount;      // [3]
   int *state;       // [0] steps mode loaded, [1] job geometry loaded (N)
@@ -396,19 +400,32 @@ __device__ __forceinline__ int tile_index(int L, const int *l) {
   return (l[2] << 8) | (l[1] << 4) | l[0];
 }
 // Moves the tile's accumulators from layout `from` to layout `to` (all
-// threads; barriers inside).
-__device__ __noinline__ void relayout(float4 *acc, int from, int to) {
-  float4 v[NV / NT];
-#pragma unroll
-  for (int j = 0; j < NV / NT; j++) v[j] = acc[threadIdx.x + j * NT];
-  __syncthreads();
-#pragma unroll
-  for (int j = 0; j < NV / NT; j++) {
-    int l[3];
-    tile_cell(from, threadIdx.x + j * NT, l);
-    acc[tile_index(to, l)] = v[j];
+// threads; barriers inside).  Layouts 0 -> 1 swap the x and y digits of the
+// cell index, 1 -> 2 the y and z digits: each an involution, done as pair
+// swaps with no scratch; 0 -> 2 is both.
+__device__ __forceinline__ void swap_digits(float4 *acc, int hi_shift, int lo_shift) {
+  // cells (.., u at hi_shift, .., v at lo_shift, ..) <-> (.., v, .., u, ..), u < v
+  for (int i = threadIdx.x; i < NV; i += blockDim.x) {
+    const int u = (i >> hi_shift) & 15, v = (i >> lo_shift) & 15;
+    if (u < v) {
+      const int j = i + ((v - u) << hi_shift) - ((v - u) << lo_shift);
+      const float4 a = acc[i];
+      acc[i] = acc[j];
+      acc[j] = a;
+    }
   }
+}
+__device__ __noinline__ void relayout(float4 *acc, int from, int to) {
   __syncthreads();
+  if (from == 0) {          // L0 = x:8, z:4, y:0  ->  L1 = y:8, z:4, x:0
+    swap_digits(acc, 8, 0);
+    __syncthreads();
+    from = 1;
+  }
+  if (from == 1 && to == 2) {   // L1 = y:8, z:4, x:0  ->  L2 = z:8, y:4, x:0
+    swap_digits(acc, 8, 4);
+    __syncthreads();
+  }
 }
 
 template <int MODE, int A>
@@ -515,7 +532,10 @@ __device__ __forceinline__ void column_work(const Smem3 &S, const float *M, int 
           else if (A == 1) r = __fadd_rn(__fadd_rn(f0, d2), f1);
           else r = __fadd_rn(f0, d2);
           if (MODE == MODE_GAUSS2) {
-            const float gg = __fmul_rn(step_exp(r, h, steps, S.steps), w);
+            const float f = __fmul_rn(-r, h);
+            const float g = (f > 0.0f || f < -19.98f)
+                                ? expf(f) : S.exp[__double2int_rz(__fma_rn((double)(-f), 50.0, 0.5))];
+            const float gg = __fmul_rn(g, w);
             vre = __fmul_rn(v.x, gg);
             vim = __fmul_rn(v.y, gg);
             vw = gg;
@@ -572,10 +592,10 @@ __device__ __forceinline__ void column_work(const Smem3 &S, const float *M, int 
 template <int MODE, int A>
 __device__ __forceinline__ void group_work(const InsertJob &J, const Smem3 &S, int g0, int g1,
                                            const int *base, const int *ext, float h,
-                                           const ExpSteps &steps) {
+                                           const ExpSteps &steps, int s0) {
   const int N = J.N, w2 = (N >> 1) + 1;
   for (int hI = g0; hI < g1; hI++) {
-    const int s = S.hits[hI];
+    const int s = s0 + S.hits[hI];
     const int p = s / J.nsym;
     float M[9];
 #pragma unroll
@@ -632,7 +652,7 @@ __device__ void tile_item3(const InsertJob &J, int tile, int s0, int s1, const S
     }
     if (grp >= 0) {
       const int at = nhit + off + __popc(b & ((1u << lane) - 1u));
-      S.tmp[at] = s | (grp << 28);
+      S.tmp[at] = (unsigned short)((s - s0) | (grp << 14));
     }
     nhit += tot;
     __syncthreads();
@@ -648,7 +668,7 @@ __device__ void tile_item3(const InsertJob &J, int tile, int s0, int s1, const S
       gstart[g] = base_g;
       for (int r = 0; r < nhit; r += NT) {
         const int i = r + threadIdx.x;
-        const bool in = i < nhit && (S.tmp[i] >> 28) == g;
+        const bool in = i < nhit && (S.tmp[i] >> 14) == g;
         const unsigned b = __ballot_sync(0xffffffffu, in);
         if (lane == 0) S.wcount[warp] = __popc(b);
         __syncthreads();
@@ -659,7 +679,7 @@ __device__ void tile_item3(const InsertJob &J, int tile, int s0, int s1, const S
           off += (q < warp) ? c : 0;
           tot += c;
         }
-        if (in) S.hits[base_g + off + __popc(b & ((1u << lane) - 1u))] = S.tmp[i] & 0x0FFFFFFF;
+        if (in) S.hits[base_g + off + __popc(b & ((1u << lane) - 1u))] = S.tmp[i] & 0x3FFF;
         base_g += tot;
         __syncthreads();
       }
@@ -669,12 +689,7 @@ __device__ void tile_item3(const InsertJob &J, int tile, int s0, int s1, const S
   // ---- per-job tables and this mode's exp table
   if (*(S.state + 1) != J.N) {
     for (int i = threadIdx.x; i < N + 2; i += NT) S.rtab[i] = __ldg(&J.rtab[i]);
-    for (int i = threadIdx.x; i < N; i += NT) S.xmax[i] = __ldg(&J.xmax[i]);
-  }
-  if (MODE == MODE_GAUSS2 && *S.state != MODE) {
-    const int nb = min(steps.nbins, STEP2CAP);
-    for (int i = threadIdx.x; i < nb; i += NT) S.steps[i] = __ldg(&steps.d_bins[i]);
-    if (threadIdx.x == 0 && steps.nbins > STEP2CAP) atomicOr(err, 8);
+    for (int i = threadIdx.x; i < N; i += NT) S.xmax[i] = (short)__ldg(&J.xmax[i]);
   }
   for (int i = threadIdx.x; i < NV; i += NT) S.acc[i] = make_float4(0.f, 0.f, 0.f, 0.f);
   __syncthreads();
@@ -686,19 +701,19 @@ __device__ void tile_item3(const InsertJob &J, int tile, int s0, int s1, const S
   // them, and so does the tile's layout (A-major for group A)
   int layout = -1;   // -1: nothing added yet, any layout holds the zeros
   if (gstart[1] > gstart[0]) {
-    group_work<MODE, 0>(J, S, gstart[0], gstart[1], base, ext, h, steps);
+    group_work<MODE, 0>(J, S, gstart[0], gstart[1], base, ext, h, steps, s0);
     layout = 0;
   }
   __syncthreads();
   if (gstart[2] > gstart[1]) {
     if (layout == 0) relayout(S.acc, 0, 1);
-    group_work<MODE, 1>(J, S, gstart[1], gstart[2], base, ext, h, steps);
+    group_work<MODE, 1>(J, S, gstart[1], gstart[2], base, ext, h, steps, s0);
     layout = 1;
   }
   __syncthreads();
   if (gstart[3] > gstart[2]) {
     if (layout == 0 || layout == 1) relayout(S.acc, layout, 2);
-    group_work<MODE, 2>(J, S, gstart[2], gstart[3], base, ext, h, steps);
+    group_work<MODE, 2>(J, S, gstart[2], gstart[3], base, ext, h, steps, s0);
     layout = 2;
   }
   __syncthreads();
@@ -1087,7 +1102,7 @@ __global__ void __launch_bounds__(col::NT, 2)
   }
 }
 
-__global__ void __launch_bounds__(col::NT, 2)
+__global__ void __launch_bounds__(col::NT, 3)
     k_column3(const InsertJob *__restrict__ jobs, const int4 *__restrict__ work, int nwork,
               int block, int *counter, const float *__restrict__ exp_g, float h2, float h5,
               ExpSteps st2, ExpSteps st5, int maxN, int *err) {
@@ -1098,11 +1113,11 @@ __global__ void __launch_bounds__(col::NT, 2)
   __shared__ int s_state[2];
   col::Smem3 S;
   S.acc = s_dyn;
-  S.steps = s_dyn + col::NV;
-  S.exp = reinterpret_cast<float *>(S.steps + col::STEP2CAP);
+  S.steps = nullptr;
+  S.exp = reinterpret_cast<float *>(s_dyn + col::NV);
   S.rtab = S.exp + 1000;
-  S.xmax = reinterpret_cast<int *>(S.rtab + maxN + 2);
-  S.hits = S.xmax + maxN;
+  S.xmax = reinterpret_cast<short *>(S.rtab + maxN + 2);
+  S.hits = reinterpret_cast<unsigned short *>(S.xmax + maxN + 2);
   S.tmp = S.hits + block;
   S.wcount = s_wcount;
   S.gcount = s_gcount;
@@ -1133,8 +1148,9 @@ cudaError_t launch_column3(const InsertJob *d_jobs, const int4 *d_work, int nwor
                            int *d_counter, int maxN, cudaStream_t st) {
   if (nwork == 0) return cudaSuccess;
   const Consts &c = consts();
-  const size_t smem = sizeof(float4) * (col::NV + col::STEP2CAP) + sizeof(float) * 1000 +
-                      sizeof(float) * (maxN + 2) + sizeof(int) * maxN + 2 * sizeof(int) * block;
+  const size_t smem = sizeof(float4) * col::NV + sizeof(float) * 1000 +
+                      sizeof(float) * (maxN + 2) + sizeof(short) * (maxN + 2) +
+                      2 * sizeof(unsigned short) * block;
   cudaError_t ea = set_max_smem((const void *)k_column3, smem);
   if (ea != cudaSuccess) return ea;
   cudaError_t e = zero_counter(d_counter, st);
