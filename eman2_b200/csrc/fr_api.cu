@@ -348,6 +348,13 @@ size_t norm_floats(int N) { return (size_t)N * N * (N / 2 + 1); }
 size_t slice_floats(int N) { return (size_t)N * (N + 2); }
 
 
+int require_cubic(const fr_recon *r, const char *what) {
+  if (r->NZ != r->N)
+    return fail(FR_EUNSUPPORTED, "%s needs a cubic volume (this one is %d x %d x %d)", what, r->N,
+                r->N, r->NZ);
+  return FR_OK;
+}
+
 int check_state(fr_recon *r) {
   if (!r) return fail(FR_ENULL, "null reconstructor handle");
   if (r->state != 1)
@@ -416,6 +423,7 @@ InsertJob make_job(fr_recon *r, const float2 *slices, const float *t3d, const fl
   j.nsym = r->nsym;
   j.np = np;
   j.tiles_x = j.tiles_y = j.tiles_z = 0;
+  j.nz = r->NZ != r->N ? r->NZ : 0;
   return j;
 }
 
@@ -448,7 +456,8 @@ int insert_device(fr_recon *r, const float2 *d_slices, const float *d_t3d, const
     j.sscale = (float)(2.0 * (nssnr - 1) / (float)r->N);
   }
   const int tuned = tuned_tile(r->N, r->mode, r->nsym);
-  int sched = r->mode == FR_MODE_ITER ? FR_SCHED_SCATTER : schedule;   // its inserter: scatter only
+  // the iterative inserter and non-cubic volumes: scatter only
+  int sched = (r->mode == FR_MODE_ITER || r->NZ != r->N) ? FR_SCHED_SCATTER : schedule;
   if (sched == FR_SCHED_AUTO) {
     // Few slices: the per-tile culling and the volume read/write of the gather
     // pass are not amortised, so atomics win; a measured choice overrides.
@@ -585,8 +594,8 @@ int check_device_error(fr_recon *r) {
 }
 
 int alloc_volume(fr_recon *r) {
-  TRY(r->vol_data.ensure(vol_floats(r->N) * sizeof(float)));
-  TRY(r->vol_norm.ensure(norm_floats(r->N) * sizeof(float)));
+  TRY(r->vol_data.ensure(rvol_floats(r) * sizeof(float)));
+  TRY(r->vol_norm.ensure(rnorm_floats(r) * sizeof(float)));
   TRY(r->d_sym.ensure(sizeof(float) * r->syms.size()));
   CU(cudaMemcpyAsync(r->d_sym.p, r->syms.data(), sizeof(float) * r->syms.size(),
                      cudaMemcpyHostToDevice, r->stream));
@@ -758,12 +767,18 @@ int fr_create(const fr_params *p, fr_recon **out) {
   *out = nullptr;
   if (p->nx <= 0 || p->ny <= 0 || p->nz <= 0)
     return fail(FR_EINVAL_PARAM, "size must be three positive integers");
-  if (p->nx != p->ny || p->ny != p->nz)
-    return fail(FR_EUNSUPPORTED, "only cubic volumes are supported (size %d %d %d)", p->nx, p->ny,
-                p->nz);
-  if (p->nx % 2)
-    return fail(FR_EUNSUPPORTED, "odd sizes (fftodd volumes) are not supported (size %d)", p->nx);
-  if (p->nx < 4 || p->nx > 4094) return fail(FR_EUNSUPPORTED, "size %d outside [4, 4094]", p->nx);
+  // square slices into an nx x nx x nz volume (e.g. programs/e2tomogram.py:2024,
+  // size=[pad,pad,zthick]); a z size other than nx takes the scatter path
+  if (p->nx != p->ny)
+    return fail(FR_EUNSUPPORTED, "size %d %d %d: x and y must be equal (square slices)", p->nx,
+                p->ny, p->nz);
+  if (p->nx % 2 || p->nz % 2)
+    return fail(FR_EUNSUPPORTED, "odd sizes (fftodd volumes) are not supported (size %d %d %d)",
+                p->nx, p->ny, p->nz);
+  if (p->nx < 4 || p->nx > 4094 || p->nz < 4 || p->nz > 4094)
+    return fail(FR_EUNSUPPORTED, "size %d %d %d outside [4, 4094]", p->nx, p->ny, p->nz);
+  if (p->nz != p->nx && p->mode == FR_MODE_ITER)
+    return fail(FR_EUNSUPPORTED, "the iterative reconstructor needs a cubic volume");
   if (p->mode != FR_MODE_NEAREST && p->mode != FR_MODE_GAUSS2 && p->mode != FR_MODE_GAUSS5 &&
       p->mode != FR_MODE_TRILINEAR && p->mode != FR_MODE_ITER)
     return fail(FR_EUNSUPPORTED, "inserter mode %d is not built", p->mode);
@@ -773,6 +788,7 @@ int fr_create(const fr_params *p, fr_recon **out) {
   fr_recon *r = new fr_recon();
   r->p = *p;
   r->N = p->nx;
+  r->NZ = p->nz;
   r->mode = p->mode;
   r->nsym = ns;
   r->syms = ops;
@@ -846,8 +862,8 @@ int fr_setup(fr_recon *r) {
   std::lock_guard<std::mutex> lk(r->mu);
   TRY(stream_enter(r, r->stream));
   TRY(alloc_volume(r));
-  CU(cudaMemsetAsync(r->vol_data.p, 0, vol_floats(r->N) * sizeof(float), r->stream));
-  CU(cudaMemsetAsync(r->vol_norm.p, 0, norm_floats(r->N) * sizeof(float), r->stream));
+  CU(cudaMemsetAsync(r->vol_data.p, 0, rvol_floats(r) * sizeof(float), r->stream));
+  CU(cudaMemsetAsync(r->vol_norm.p, 0, rnorm_floats(r) * sizeof(float), r->stream));
   CU(cudaStreamSynchronize(r->stream));
   r->has_ref = false;   // FourierIterReconstructor::setup drops the reference volume
   if (r->p.verbose) {
@@ -861,6 +877,7 @@ int fr_setup(fr_recon *r) {
 
 int fr_setup_seed(fr_recon *r, const float *seed, float seed_weight) {
   if (!r) return fail(FR_ENULL, "null handle");
+  TRY(require_cubic(r, "setup_seed"));
   if (!seed) return fail(FR_ENULL, "null seed volume");
   std::lock_guard<std::mutex> lk(r->mu);
   TRY(stream_enter(r, r->stream));
@@ -876,6 +893,7 @@ int fr_setup_seed(fr_recon *r, const float *seed, float seed_weight) {
 
 int fr_setup_seedandweights(fr_recon *r, const float *seed, const float *weights) {
   if (!r) return fail(FR_ENULL, "null handle");
+  TRY(require_cubic(r, "setup_seedandweights"));
   if (!seed || !weights) return fail(FR_ENULL, "null seed or weight volume");
   std::lock_guard<std::mutex> lk(r->mu);
   TRY(stream_enter(r, r->stream));
@@ -893,8 +911,8 @@ int fr_clear(fr_recon *r) {
   TRY(check_state(r));
   std::lock_guard<std::mutex> lk(r->mu);
   TRY(stream_enter(r, r->stream));
-  CU(cudaMemsetAsync(r->vol_data.p, 0, vol_floats(r->N) * sizeof(float), r->stream));
-  CU(cudaMemsetAsync(r->vol_norm.p, 0, norm_floats(r->N) * sizeof(float), r->stream));
+  CU(cudaMemsetAsync(r->vol_data.p, 0, rvol_floats(r) * sizeof(float), r->stream));
+  CU(cudaMemsetAsync(r->vol_norm.p, 0, rnorm_floats(r) * sizeof(float), r->stream));
   CU(cudaStreamSynchronize(r->stream));
   return FR_OK;
 }
@@ -992,6 +1010,7 @@ int fr_insert_slices(fr_recon *r, const float *slices, int n, const float *rot, 
 
 int fr_set_reference(fr_recon *r, const float *vol, int is_complex) {
   TRY(check_state(r));
+  TRY(require_cubic(r, "the iterative reconstructor"));
   if (!vol) return fail(FR_ENULL, "null reference volume");
   if (r->mode != FR_MODE_ITER)
     return fail(FR_EINVAL_PARAM, "a reference volume belongs to the iterative reconstructor");
@@ -1031,6 +1050,7 @@ int fr_insert_slices_wiener(fr_recon *r, const float *slices, int n, const float
                             const float *weights, const float *snr, int nsnr, const int *undo,
                             int *status_out) {
   TRY(check_state(r));
+  TRY(require_cubic(r, "wiener_fourier insertion"));
   if (n < 0) return fail(FR_EINVAL_PARAM, "negative count");
   if (n == 0) return FR_OK;
   if (!slices || !rot || !weights) return fail(FR_ENULL, "EMData pointer (input image) is NULL");
@@ -1145,6 +1165,7 @@ int fr_insert_particles(fr_recon *r, const float *imgs, int n, int box, const fr
 int fr_determine_slice_agreement(fr_recon *r, const float *slices, int n, const float *rot,
                                  const float *weights, float apix, int sub, float *out) {
   TRY(check_state(r));
+  TRY(require_cubic(r, "determine_slice_agreement"));
   if (n < 0) return fail(FR_EINVAL_PARAM, "negative count");
   if (n == 0) return FR_OK;
   if (!slices || !rot || !weights || !out) return fail(FR_ENULL, "EMData pointer (input image) is NULL");
@@ -1178,6 +1199,7 @@ int fr_determine_slice_agreement(fr_recon *r, const float *slices, int n, const 
 
 int fr_projection_xf(fr_recon *r, const float *xf, int ret_fourier, float *out) {
   TRY(check_state(r));
+  TRY(require_cubic(r, "projection"));
   if (!xf || !out) return fail(FR_ENULL, "null argument");
   std::lock_guard<std::mutex> lk(r->mu);
   TRY(stream_enter(r, r->stream));
@@ -1225,8 +1247,8 @@ int fr_get_accumulators(fr_recon *r, float *data, float *norm) {
   std::lock_guard<std::mutex> lk(r->mu);
   TRY(stream_enter(r, r->stream));
   TRY(check_device_error(r));
-  if (data) TRY(from_device(data, r->vol_data.p, vol_floats(r->N) * sizeof(float), r->stream));
-  if (norm) TRY(from_device(norm, r->vol_norm.p, norm_floats(r->N) * sizeof(float), r->stream));
+  if (data) TRY(from_device(data, r->vol_data.p, rvol_floats(r) * sizeof(float), r->stream));
+  if (norm) TRY(from_device(norm, r->vol_norm.p, rnorm_floats(r) * sizeof(float), r->stream));
   return FR_OK;
 }
 
@@ -1237,27 +1259,29 @@ int fr_finish(fr_recon *r, int doift, float *out, float *normout) {
   const int N = r->N;
   cudaStream_t st = r->stream;
   TRY(check_device_error(r));
+  const int NZ = r->NZ, nz = NZ != N ? NZ : 0;
   CU(launch_normalize(r->vol_data.as<float>(), r->vol_norm.as<float>(), N, r->p.sqrtnorm, st,
-                      r->wfilt));
-  if (normout) TRY(from_device(normout, r->vol_norm.p, norm_floats(N) * sizeof(float), st));
+                      r->wfilt, nz));
+  if (normout) TRY(from_device(normout, r->vol_norm.p, rnorm_floats(r) * sizeof(float), st));
   if (doift) {
     cufftHandle plan;
-    TRY(r->plans.get3d(N, st, &plan));
+    TRY(r->plans.get3d(N, st, &plan, NZ));
     CUFFT(cufftExecC2R(plan, r->vol_data.as<cufftComplex>(), r->vol_data.as<cufftReal>()));
     // do_ift scale 1.0f / (nx*ny*nz) (libEM/emdata_transform.cpp:411-412)
-    const float scale = 1.0f / (float)((size_t)N * N * N);
+    const size_t nreal = (size_t)N * N * NZ;
+    const float scale = 1.0f / (float)nreal;
     if (out) {
       if (is_device_ptr(out)) {
-        CU(launch_depad_center(r->vol_data.as<float>(), N, scale, out, st));
+        CU(launch_depad_center(r->vol_data.as<float>(), N, scale, out, st, nz));
         CU(cudaStreamSynchronize(st));
       } else {
-        TRY(r->s_out.ensure(sizeof(float) * (size_t)N * N * N));
-        CU(launch_depad_center(r->vol_data.as<float>(), N, scale, r->s_out.as<float>(), st));
-        TRY(from_device(out, r->s_out.p, sizeof(float) * (size_t)N * N * N, st));
+        TRY(r->s_out.ensure(sizeof(float) * nreal));
+        CU(launch_depad_center(r->vol_data.as<float>(), N, scale, r->s_out.as<float>(), st, nz));
+        TRY(from_device(out, r->s_out.p, sizeof(float) * nreal, st));
       }
     }
   } else if (out) {
-    TRY(from_device(out, r->vol_data.p, vol_floats(N) * sizeof(float), st));
+    TRY(from_device(out, r->vol_data.p, rvol_floats(r) * sizeof(float), st));
   }
   CU(cudaStreamSynchronize(st));
   r->state = 2;
@@ -1284,29 +1308,29 @@ int fr_finish_async(fr_recon *r, int doift, float *out, float *normout, void *st
   std::lock_guard<std::mutex> lk(r->mu);
   cudaStream_t st = stream ? (cudaStream_t)stream : r->stream;
   TRY(stream_enter(r, st));
-  const int N = r->N;
+  const int N = r->N, NZ = r->NZ, nz = NZ != N ? NZ : 0;
   CU(launch_normalize(r->vol_data.as<float>(), r->vol_norm.as<float>(), N, r->p.sqrtnorm, st,
-                      r->wfilt));
+                      r->wfilt, nz));
   if (normout)
-    CU(cudaMemcpyAsync(normout, r->vol_norm.p, norm_floats(N) * sizeof(float), cudaMemcpyDefault,
+    CU(cudaMemcpyAsync(normout, r->vol_norm.p, rnorm_floats(r) * sizeof(float), cudaMemcpyDefault,
                        st));
   if (doift) {
     cufftHandle plan;
-    TRY(r->plans.get3d(N, st, &plan));
+    TRY(r->plans.get3d(N, st, &plan, NZ));
     CUFFT(cufftExecC2R(plan, r->vol_data.as<cufftComplex>(), r->vol_data.as<cufftReal>()));
-    const float scale = 1.0f / (float)((size_t)N * N * N);
+    const size_t nreal = (size_t)N * N * NZ;
+    const float scale = 1.0f / (float)nreal;
     if (out) {
       if (is_device_ptr(out)) {
-        CU(launch_depad_center(r->vol_data.as<float>(), N, scale, out, st));
+        CU(launch_depad_center(r->vol_data.as<float>(), N, scale, out, st, nz));
       } else {
-        TRY(r->s_out.ensure(sizeof(float) * (size_t)N * N * N));
-        CU(launch_depad_center(r->vol_data.as<float>(), N, scale, r->s_out.as<float>(), st));
-        CU(cudaMemcpyAsync(out, r->s_out.p, sizeof(float) * (size_t)N * N * N,
-                           cudaMemcpyDeviceToHost, st));
+        TRY(r->s_out.ensure(sizeof(float) * nreal));
+        CU(launch_depad_center(r->vol_data.as<float>(), N, scale, r->s_out.as<float>(), st, nz));
+        CU(cudaMemcpyAsync(out, r->s_out.p, sizeof(float) * nreal, cudaMemcpyDeviceToHost, st));
       }
     }
   } else if (out) {
-    CU(cudaMemcpyAsync(out, r->vol_data.p, vol_floats(N) * sizeof(float), cudaMemcpyDefault, st));
+    CU(cudaMemcpyAsync(out, r->vol_data.p, rvol_floats(r) * sizeof(float), cudaMemcpyDefault, st));
   }
   TRY(stream_leave(r, st));
   r->state = 2;
@@ -1316,6 +1340,7 @@ int fr_finish_async(fr_recon *r, int doift, float *out, float *normout, void *st
 int fr_finish_corrected(fr_recon *r, float gauss_width, int outx, int outy, int outz, float *out,
                         float *normout) {
   TRY(check_state(r));
+  TRY(require_cubic(r, "finish_corrected"));
   if (!out) return fail(FR_ENULL, "null output");
   const int N = r->N;
   if (outx <= 0 || outy <= 0 || outz <= 0 || outx > N || outy > N || outz > N)

@@ -453,6 +453,7 @@ static int batch_insert(std::vector<fr_recon *> &jobs, BatchScratch &bs, int til
   bool host_src = false;
   for (int j = 0; j < nj; j++) {
     TRY(check_state(jobs[j]));
+    TRY(require_cubic(jobs[j], "a batched insertion"));
     if (counts[j] < 0 || (counts[j] > 0 && (boxes[j] <= 0 || !imgs[j] || !meta[j])))
       return fail(FR_EINVAL_PARAM, "job %d: bad particle count, box or buffers", j);
     if (counts[j] > 0 && !is_device_ptr(imgs[j])) host_src = true;
@@ -663,6 +664,7 @@ static int graph_create(const std::vector<fr_recon *> &jobs, cudaStream_t st, in
   int total = 0;
   for (int j = 0; j < nj; j++) {
     TRY(check_state(jobs[j]));
+    TRY(require_cubic(jobs[j], "a batched insertion graph"));
     if (counts[j] < 0 || counts[j] > kBatchChunk || (counts[j] > 0 && boxes[j] <= 0))
       return fail(FR_EINVAL_PARAM, "job %d: count must be in [0, %d] with a positive box", j,
                   kBatchChunk);

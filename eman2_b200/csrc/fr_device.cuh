@@ -49,6 +49,13 @@ __device__ __forceinline__ void pixel_coords(float rx, float ry, const float *M,
   yy = __fmul_rn(__fadd_rn(__fmul_rn(rx, M[1]), __fmul_rn(ry, M[4])), Nf);
   zz = __fmul_rn(__fadd_rn(__fmul_rn(rx, M[2]), __fmul_rn(ry, M[5])), Nf);
 }
+// The same into a volume of z size NZf (x and y: Nf).
+__device__ __forceinline__ void pixel_coords_z(float rx, float ry, const float *M, float Nf,
+                                               float NZf, float &xx, float &yy, float &zz) {
+  xx = __fmul_rn(__fadd_rn(__fmul_rn(rx, M[0]), __fmul_rn(ry, M[3])), Nf);
+  yy = __fmul_rn(__fadd_rn(__fmul_rn(rx, M[1]), __fmul_rn(ry, M[4])), Nf);
+  zz = __fmul_rn(__fadd_rn(__fmul_rn(rx, M[2]), __fmul_rn(ry, M[5])), NZf);
+}
 
 // Util::hypot3sq (libEM/util.h:816-819) of (i-xx, j-yy, k-zz).
 __device__ __forceinline__ float dist2(int i, int j, int k, float xx, float yy, float zz) {
@@ -97,14 +104,15 @@ __device__ __forceinline__ void tap_value(int i, int j, int k, float xx, float y
 // add at the returned index, with FP32 atomics.  data: [N][N][N+2] floats,
 // norm: [N][N][N/2+1].  The two "imaginary := 0" cells are written with a
 // plain store: no other tap ever adds to their imaginary parts.
+// NZ: the volume's z size (N for the cubic volume; [NZ][N][N+2] otherwise).
 __device__ __forceinline__ void add_tap_atomic(float *__restrict__ data, float *__restrict__ norm,
-                                               int N, int x, int y, int z, float re, float im,
-                                               float wt) {
+                                               int N, int NZ, int x, int y, int z, float re,
+                                               float im, float wt) {
   const int h = N >> 1;
-  if (abs(x) > h || abs(y) > h || abs(z) > h) return;
+  if (abs(x) > h || abs(y) > h || abs(z) > (NZ >> 1)) return;
   const size_t nxf = (size_t)N + 2;
   const size_t nxy = nxf * (size_t)N;
-  const size_t rc = (size_t)(y <= 0 ? -y : N - y) * nxf + (size_t)(z <= 0 ? -z : N - z) * nxy;
+  const size_t rc = (size_t)(y <= 0 ? -y : N - y) * nxf + (size_t)(z <= 0 ? -z : NZ - z) * nxy;
   if (x == 0) {
     if (y == 0 && z == 0) {
       atomicAdd(&data[0], re);
@@ -130,7 +138,7 @@ __device__ __forceinline__ void add_tap_atomic(float *__restrict__ data, float *
     return;
   }
   const size_t idx = (size_t)x * 2 + (size_t)(y < 0 ? N + y : y) * nxf +
-                     (size_t)(z < 0 ? N + z : z) * nxy;
+                     (size_t)(z < 0 ? NZ + z : z) * nxy;
   atomicAdd(reinterpret_cast<float2 *>(&data[idx]), make_float2(re, im));
   atomicAdd(&norm[idx >> 1], wt);
 }

@@ -13,15 +13,16 @@ namespace fr {
 // x=N/2 planes are summed into both cells; five special cells are doubled.
 // The pairs are disjoint from one another and from the special cells, so one
 // thread per (z, y) pair does them all.
-__global__ void k_norm_pairs(float *__restrict__ norm, int N) {
+// NZ: the volume's z size (N when cubic).
+__global__ void k_norm_pairs(float *__restrict__ norm, int N, int NZ) {
   const long nnx = N / 2 + 1, nnxy = (long)N * nnx;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int ny2 = N / 2 + 1;
-  if (i < N * ny2) {
-    const int z = i / ny2 - N / 2, y = i % ny2;
+  if (i < NZ * ny2) {
+    const int z = i / ny2 - NZ / 2, y = i % ny2;
     if (z <= 0 && (y == 0 || y == N / 2)) return;
-    long idx1 = (long)(y == 0 ? 0 : N - y) * nnx + (long)(z <= 0 ? -z : N - z) * nnxy;
-    long idx2 = (long)y * nnx + (long)(z < 0 ? N + z : z) * nnxy;
+    long idx1 = (long)(y == 0 ? 0 : N - y) * nnx + (long)(z <= 0 ? -z : NZ - z) * nnxy;
+    long idx2 = (long)y * nnx + (long)(z < 0 ? NZ + z : z) * nnxy;
     if (idx1 == idx2) return;
     float s = __fadd_rn(norm[idx1], norm[idx2]);
     norm[idx1] = s;
@@ -31,15 +32,15 @@ __global__ void k_norm_pairs(float *__restrict__ norm, int N) {
     s = __fadd_rn(norm[idx1], norm[idx2]);
     norm[idx1] = s;
     norm[idx2] = s;
-  } else if (i < N * ny2 + 5) {
-    const int c = i - N * ny2;
-    const long h = N / 2;
+  } else if (i < NZ * ny2 + 5) {
+    const int c = i - NZ * ny2;
+    const long h = N / 2, hz = NZ / 2;
     long idx;
     switch (c) {
-      case 0: idx = 0 + 0 * nnx + h * nnxy; break;
+      case 0: idx = 0 + 0 * nnx + hz * nnxy; break;
       case 1: idx = 0 + h * nnx + 0 * nnxy; break;
-      case 2: idx = 0 + h * nnx + h * nnxy; break;
-      case 3: idx = (nnx - 1) + 0 * nnx + h * nnxy; break;
+      case 2: idx = 0 + h * nnx + hz * nnxy; break;
+      case 3: idx = (nnx - 1) + 0 * nnx + hz * nnxy; break;
       default: idx = (nnx - 1) + h * nnx + 0 * nnxy; break;
     }
     norm[idx] = __fmul_rn(norm[idx], 2.0f);
@@ -66,11 +67,12 @@ __global__ void k_divide(float2 *__restrict__ data, const float *__restrict__ no
 }
 
 cudaError_t launch_normalize(float *d_data, float *d_norm, int N, int sqrtnorm, cudaStream_t st,
-                             float wfilt) {
-  const int np = N * (N / 2 + 1) + 5;
+                             float wfilt, int nz) {
+  const int NZ = nz ? nz : N;
+  const int np = NZ * (N / 2 + 1) + 5;
   note_launch();
-  k_norm_pairs<<<(np + 255) / 256, 256, 0, st>>>(d_norm, N);
-  const long n = (long)N * N * (N / 2 + 1);
+  k_norm_pairs<<<(np + 255) / 256, 256, 0, st>>>(d_norm, N, NZ);
+  const long n = (long)NZ * N * (N / 2 + 1);
   note_launch();
   k_divide<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(reinterpret_cast<float2 *>(d_data), d_norm,
                                                          n, sqrtnorm, wfilt);
@@ -79,22 +81,23 @@ cudaError_t launch_normalize(float *d_data, float *d_norm, int N, int sqrtnorm, 
 
 // do_ift scale x 1/N^3, depad (drop the two x padding floats) and phase origin
 // to centre (libEM/reconstructor.cpp:1593-1597) in one pass.
-__global__ void k_depad_center(const float *__restrict__ in, int N, float scale,
+__global__ void k_depad_center(const float *__restrict__ in, int N, int NZ, float scale,
                                float *__restrict__ out) {
   const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long n3 = (long)N * N * N;
+  const long n3 = (long)N * N * NZ;
   if (i >= n3) return;
   const int x = (int)(i % N), y = (int)((i / N) % N), z = (int)(i / ((long)N * N));
   const int h = N / 2;
-  const int sx = (x + h) % N, sy = (y + h) % N, sz = (z + h) % N;
+  const int sx = (x + h) % N, sy = (y + h) % N, sz = (z + NZ / 2) % NZ;
   out[i] = __fmul_rn(in[((long)sz * N + sy) * (N + 2) + sx], scale);
 }
 
 cudaError_t launch_depad_center(const float *d_real_padded, int N, float scale, float *d_out,
-                                cudaStream_t st) {
-  const long n3 = (long)N * N * N;
+                                cudaStream_t st, int nz) {
+  const int NZ = nz ? nz : N;
+  const long n3 = (long)N * N * NZ;
   note_launch();
-  k_depad_center<<<(unsigned)((n3 + 255) / 256), 256, 0, st>>>(d_real_padded, N, scale, d_out);
+  k_depad_center<<<(unsigned)((n3 + 255) / 256), 256, 0, st>>>(d_real_padded, N, NZ, scale, d_out);
   return cudaGetLastError();
 }
 

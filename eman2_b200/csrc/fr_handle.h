@@ -207,12 +207,15 @@ struct PlanCache {
     }
     return FR_OK;
   }
-  int get3d(int N, cudaStream_t st, cufftHandle *out) {
-    if (!c2r3 || c2r3_N != N) {
+  int c2r3_NZ = 0;
+  int get3d(int N, cudaStream_t st, cufftHandle *out, int NZ = 0) {
+    if (!NZ) NZ = N;
+    if (!c2r3 || c2r3_N != N || c2r3_NZ != NZ) {
       if (c2r3) cufftDestroy(c2r3);
       c2r3 = 0;
-      CUFFT(cufftPlan3d(&c2r3, N, N, N, CUFFT_C2R));
+      CUFFT(cufftPlan3d(&c2r3, NZ, N, N, CUFFT_C2R));
       c2r3_N = N;
+      c2r3_NZ = NZ;
     }
     CUFFT(cufftSetStream(c2r3, st));
     *out = c2r3;
@@ -236,6 +239,7 @@ int default_tile(int mode, int N, int nsym, int np);
 struct fr_recon {
   fr_params p;
   int N = 0;
+  int NZ = 0;                 // the volume's z size (N for the cubic volume)
   int mode = FR_MODE_GAUSS2;
   int nsym = 1;
   std::vector<float> syms;
@@ -284,6 +288,11 @@ struct fr_recon {
 
 namespace fr {
 int check_state(fr_recon *r);
+// Floats of the handle's complex and weight volumes: [NZ][N][N+2], [NZ][N][N/2+1].
+inline size_t rvol_floats(const fr_recon *r) { return (size_t)r->NZ * r->N * (r->N + 2); }
+inline size_t rnorm_floats(const fr_recon *r) { return (size_t)r->NZ * r->N * (r->N / 2 + 1); }
+// Paths built for the cubic volume only: FR_EUNSUPPORTED otherwise.
+int require_cubic(const fr_recon *r, const char *what);
 // Orders work enqueued on st after the handle's earlier work on other streams.
 int stream_enter(fr_recon *r, cudaStream_t st);
 // Marks the end of the handle's work enqueued so far on st.

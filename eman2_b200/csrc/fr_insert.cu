@@ -61,44 +61,46 @@ cudaError_t launch_compose(const float *d_arg, const float *d_sym, int np, int n
 // rules follow libEM/reconstructor_tools.cpp:113-126 (nearest),
 // :128-166 (gauss_2), :191-230 (trilinear), :315-376 (gauss_5).
 // face_only: process only taps with a coordinate at +-N/2 (edge kernel).
+// NZ: the volume's z size (its window clamps and placement; N when cubic).
 template <int MODE>
 __device__ __forceinline__ void insert_pixel_atomic(float *__restrict__ data, float *__restrict__ norm,
-                                                    int N, float xx, float yy, float zz, float re,
-                                                    float im, float w, float h,
+                                                    int N, int NZ, float xx, float yy, float zz,
+                                                    float re, float im, float w, float h,
                                                     const float *__restrict__ table, bool face_only) {
-  const int n2 = N >> 1;
+  const int n2 = N >> 1, nz2 = NZ >> 1;
   if (MODE == MODE_NEAREST) {
     const int x0 = (int)floorf(__fadd_rn(xx, 0.5f));
     const int y0 = (int)floorf(__fadd_rn(yy, 0.5f));
     const int z0 = (int)floorf(__fadd_rn(zz, 0.5f));
-    if (face_only && abs(x0) != n2 && abs(y0) != n2 && abs(z0) != n2) return;
-    add_tap_atomic(data, norm, N, x0, y0, z0, __fmul_rn(re, w), __fmul_rn(im, w), w);
+    if (face_only && abs(x0) != n2 && abs(y0) != n2 && abs(z0) != nz2) return;
+    add_tap_atomic(data, norm, N, NZ, x0, y0, z0, __fmul_rn(re, w), __fmul_rn(im, w), w);
   } else if (MODE == MODE_GAUSS2 || MODE == MODE_TRILINEAR) {
     const int x0 = (int)floorf(xx), y0 = (int)floorf(yy), z0 = (int)floorf(zz);
-    if (x0 < -n2 - 1 || y0 < -n2 - 1 || z0 < -n2 - 1 || x0 > n2 || y0 > n2 || z0 > n2) return;
+    if (x0 < -n2 - 1 || y0 < -n2 - 1 || z0 < -nz2 - 1 || x0 > n2 || y0 > n2 || z0 > nz2) return;
     for (int k = z0; k <= z0 + 1; k++)
       for (int j = y0; j <= y0 + 1; j++)
         for (int i = x0; i <= x0 + 1; i++) {
-          if (face_only && abs(i) != n2 && abs(j) != n2 && abs(k) != n2) continue;
+          if (face_only && abs(i) != n2 && abs(j) != n2 && abs(k) != nz2) continue;
           float vre, vim, vw;
           tap_value<MODE>(i, j, k, xx, yy, zz, re, im, w, h, table, vre, vim, vw);
-          add_tap_atomic(data, norm, N, i, j, k, vre, vim, vw);
+          add_tap_atomic(data, norm, N, NZ, i, j, k, vre, vim, vw);
         }
   } else {  // MODE_GAUSS5
     int x0 = floor_minus_2p5(xx), y0 = floor_minus_2p5(yy), z0 = floor_minus_2p5(zz);
-    if (x0 < -n2 - 4 || y0 < -n2 - 4 || z0 < -n2 - 4 || x0 > n2 + 3 || y0 > n2 + 3 || z0 > n2 + 3)
+    if (x0 < -n2 - 4 || y0 < -n2 - 4 || z0 < -nz2 - 4 || x0 > n2 + 3 || y0 > n2 + 3 ||
+        z0 > nz2 + 3)
       return;
     int x1 = x0 + 5, y1 = y0 + 5, z1 = z0 + 5;
     x0 = max(x0, -n2); x1 = min(x1, n2);
     y0 = max(y0, -n2); y1 = min(y1, n2);
-    z0 = max(z0, -n2); z1 = min(z1, n2);
+    z0 = max(z0, -nz2); z1 = min(z1, nz2);
     for (int k = z0; k <= z1; k++)
       for (int j = y0; j <= y1; j++)
         for (int i = x0; i <= x1; i++) {
-          if (face_only && abs(i) != n2 && abs(j) != n2 && abs(k) != n2) continue;
+          if (face_only && abs(i) != n2 && abs(j) != n2 && abs(k) != nz2) continue;
           float vre, vim, vw;
           tap_value<MODE>(i, j, k, xx, yy, zz, re, im, w, h, table, vre, vim, vw);
-          add_tap_atomic(data, norm, N, i, j, k, vre, vim, vw);
+          add_tap_atomic(data, norm, N, NZ, i, j, k, vre, vim, vw);
         }
   }
 }
@@ -179,7 +181,7 @@ __device__ __forceinline__ void insert_pixel_iter(const InsertJob &J, float xx, 
           vre = __fmul_rn(__fmul_rn(re, gg), w);
           vim = __fmul_rn(__fmul_rn(im, gg), w);
         }
-        add_tap_atomic(J.data, J.norm, N, i, j, k, vre, vim, __fmul_rn(gg, w));
+        add_tap_atomic(J.data, J.norm, N, N, i, j, k, vre, vim, __fmul_rn(gg, w));
       }
 }
 
@@ -259,8 +261,10 @@ __device__ __forceinline__ void scatter_pixel(const InsertJob &J, int s, int pix
   float M[6];
 #pragma unroll
   for (int i = 0; i < 6; i++) M[i] = __ldg(&J.t3d[9 * s + i]);
+  const int NZ = J.nz ? J.nz : N;
   float xx, yy, zz;
-  pixel_coords(__ldg(&J.rtab[x + n2]), __ldg(&J.rtab[y + n2]), M, (float)N, xx, yy, zz);
+  pixel_coords_z(__ldg(&J.rtab[x + n2]), __ldg(&J.rtab[y + n2]), M, (float)N, (float)NZ, xx, yy,
+                 zz);
   float2 v = slice_value(J.slices + (size_t)p * N * w2, N, x, y);
   float pw;
   if (J.wsnr) {
@@ -270,7 +274,7 @@ __device__ __forceinline__ void scatter_pixel(const InsertJob &J, int s, int pix
   } else {
     pw = pixel_weight(J, p, x, y, w);
   }
-  insert_pixel_atomic<MODE>(J.data, J.norm, N, xx, yy, zz, v.x, v.y, pw, h, table, false);
+  insert_pixel_atomic<MODE>(J.data, J.norm, N, NZ, xx, yy, zz, v.x, v.y, pw, h, table, false);
 }
 
 // The iterative reconstructor's insertion of one pixel of its disk.
@@ -309,7 +313,7 @@ __device__ __forceinline__ void edge_pixel(const InsertJob &J, int s, int r,
   float xx, yy, zz;
   pixel_coords(__ldg(&J.rtab[x + n2]), __ldg(&J.rtab[y + n2]), M, (float)N, xx, yy, zz);
   const float2 v = slice_value(J.slices + (size_t)p * N * w2, N, x, y);
-  insert_pixel_atomic<MODE>(J.data, J.norm, N, xx, yy, zz, v.x, v.y, pixel_weight(J, p, x, y, w),
+  insert_pixel_atomic<MODE>(J.data, J.norm, N, N, xx, yy, zz, v.x, v.y, pixel_weight(J, p, x, y, w),
                             h, table, true);
 }
 

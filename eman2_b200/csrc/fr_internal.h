@@ -53,6 +53,7 @@ struct InsertJob {
   float sscale;              // 2*(nssnr-1)/N (libEM/reconstructor.cpp:1162)
   int N, mode, nsym, np;
   int tiles_x, tiles_y, tiles_z;
+  int nz;                    // the volume's z size when it differs from N (scatter only); 0: N
 };
 
 // Launch accounting (fr_api.cu).
@@ -175,10 +176,11 @@ cudaError_t launch_shift_corner(const float *d_img_off, const float *d_img_on, c
                                 bool fuse_mean = false);
 
 // Finish / agreement (fr_finish.cu).
+// nz: the volume's z size (0: N, the cubic volume).
 cudaError_t launch_normalize(float *d_data, float *d_norm, int N, int sqrtnorm, cudaStream_t st,
-                             float wfilt = 0.0f);
+                             float wfilt = 0.0f, int nz = 0);
 cudaError_t launch_depad_center(const float *d_real_padded, int N, float scale, float *d_out,
-                                cudaStream_t st);
+                                cudaStream_t st, int nz = 0);
 cudaError_t launch_tocorner3(const float *d_in, int N, float *d_out, cudaStream_t st);
 cudaError_t launch_kernel_fix(float *d_vol, int nx, int ny, int nz, float gauss_width,
                               cudaStream_t st);

@@ -187,6 +187,12 @@ class FourierReconstructor:
     def N(self) -> int:
         return int(self._size()[0])
 
+    @property
+    def NZ(self) -> int:
+        """The volume's z size (N for the usual cubic volume; a different z
+        size, with square N x N slices, takes the scatter insertion)."""
+        return int(self._size()[2])
+
     def _size(self):
         if "size" not in self.params:
             raise NotExistingObjectException("The requested key does not exist: size")
@@ -437,9 +443,9 @@ class FourierReconstructor:
     def get_accumulators(self):
         """Un-normalised (complex, weight) volumes: what finish(False) + normout
         give before normalisation."""
-        N = self.N
-        d = np.empty((N, N, N + 2), np.float32)
-        n = np.empty((N, N, N // 2 + 1), np.float32)
+        N, NZ = self.N, self.NZ
+        d = np.empty((NZ, N, N + 2), np.float32)
+        n = np.empty((NZ, N, N // 2 + 1), np.float32)
         _lib.check(_lib.load().fr_get_accumulators(self._h, _lib.ptr(d), _lib.ptr(n)))
         return d, n
 
@@ -449,9 +455,9 @@ class FourierReconstructor:
         complex volume.  Fills the ``normout`` EMData if that param is set."""
         if self._state != 1:
             self._require_setup()
-        N = self.N
-        out = np.empty((N, N, N) if doift else (N, N, N + 2), np.float32)
-        norm = np.empty((N, N, N // 2 + 1), np.float32)
+        N, NZ = self.N, self.NZ
+        out = np.empty((NZ, N, N) if doift else (NZ, N, N + 2), np.float32)
+        norm = np.empty((NZ, N, N // 2 + 1), np.float32)
         _lib.check(_lib.load().fr_finish(self._h, int(bool(doift)), _lib.ptr(out), _lib.ptr(norm)))
         self._state = 2
         if "normout" in self.params and isinstance(self.params["normout"], EMData):
@@ -469,10 +475,10 @@ class FourierReconstructor:
         import torch
         if self._state != 1:
             self._require_setup()
-        N = self.N
-        out = torch.empty((N, N, N) if doift else (N, N, N + 2), dtype=torch.float32,
+        N, NZ = self.N, self.NZ
+        out = torch.empty((NZ, N, N) if doift else (NZ, N, N + 2), dtype=torch.float32,
                           pin_memory=True)
-        norm = torch.empty((N, N, N // 2 + 1), dtype=torch.float32, pin_memory=True)
+        norm = torch.empty((NZ, N, N // 2 + 1), dtype=torch.float32, pin_memory=True)
         if stream is None:
             dev = torch.device("cuda", torch.cuda.current_device())
             stream = _join_parts(library_stream(self._h), dev)[0]

@@ -62,9 +62,11 @@ enum {
 
 /* FourierReconstructor parameters (libEM/reconstructor.h:501-516). */
 typedef struct {
-  int nx, ny, nz;        /* "size": padded real-space volume (cubic, even) */
+  int nx, ny, nz;        /* "size": padded real-space volume, even sizes with nx == ny
+                            (square slices); nz != nx takes the scatter insertion and
+                            has no batched forms, agreement, projection or seeds */
   int mode;              /* FR_MODE_* */
-  char sym[16];          /* "c<n>" or "d<n>" */
+  char sym[16];          /* "c<n>", "d<n>", "tet", "oct", "icos" */
   int corners;           /* "corners" */
   int sqrtnorm;          /* "sqrtnorm" */
   int usessnr;           /* "usessnr" */

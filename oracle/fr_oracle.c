@@ -318,16 +318,16 @@ static inline void or_slice_at(const float *s, int nx, int ny, int x, int y, rea
  * blocks t3d[nsym*9] (arg*sym, libEM/transform.cpp:1384).
  * vol_data [N][N][N+2], vol_norm [N][N][N/2+1]; slice [N][N+2] (complex).
  * weight < 0 selects the SSNR path (ssnr table of nssnr entries). */
-OR_EXPORT int or_insert_slice(acc_t *vol_data, acc_t *vol_norm, int N, int mode,
+static int or_insert_slice_nz(acc_t *vol_data, acc_t *vol_norm, int N, int NZ, int mode,
                               const float *slice, const float *t3d, int nsym,
                               float weight, int corners, const float *ssnr, int nssnr) {
   or_init_tables();
   or_vol v;
   v.data = vol_data; v.norm = vol_norm;
-  v.nx = N + 2; v.ny = N; v.nz = N;
+  v.nx = N + 2; v.ny = N; v.nz = NZ;
   v.nxyz = (long)v.nx * v.ny * v.nz;
   const float inx = (float)(N + 2), iny = (float)N;
-  const int nx = N + 2, ny = N, nz = N;   /* FourierReconstructor members after setup() */
+  const int nx = N + 2, ny = N, nz = NZ;  /* FourierReconstructor members after setup() */
   float sscale = 1.0f;
   if (weight < 0) {
     if (!ssnr || nssnr < 1) return -1;
@@ -379,6 +379,32 @@ OR_EXPORT int or_insert_slice(acc_t *vol_data, acc_t *vol_norm, int N, int mode,
       }
     }
   }
+  return 0;
+}
+
+OR_EXPORT int or_insert_slice(acc_t *vol_data, acc_t *vol_norm, int N, int mode,
+                              const float *slice, const float *t3d, int nsym,
+                              float weight, int corners, const float *ssnr, int nssnr) {
+  return or_insert_slice_nz(vol_data, vol_norm, N, N, mode, slice, t3d, nsym, weight, corners,
+                            ssnr, nssnr);
+}
+
+/* The same into a volume of size [NZ][N][N+2] (square N x N slices; the z
+ * coordinate scaled by NZ, libEM/reconstructor.cpp:1193-1196). */
+OR_EXPORT int or_insert_batch_nz(acc_t *vol_data, acc_t *vol_norm, int N, int NZ, int mode,
+                                 const float *slices, int n, const float *arg, const float *sym,
+                                 int nsym, const float *weights) {
+  float *t3d = (float *)malloc(sizeof(float) * 9 * nsym);
+  if (!t3d) return -3;
+  const long sl = (long)N * (N + 2);
+  for (int p = 0; p < n; p++) {
+    if (weights[p] == 0) continue;
+    for (int s = 0; s < nsym; s++) or_compose(arg + 9 * p, sym + 9 * s, t3d + 9 * s);
+    int rc = or_insert_slice_nz(vol_data, vol_norm, N, NZ, mode, slices + sl * p, t3d, nsym,
+                                weights[p], 0, NULL, 0);
+    if (rc) { free(t3d); return rc; }
+  }
+  free(t3d);
   return 0;
 }
 
@@ -566,8 +592,9 @@ OR_EXPORT int or_insert_batch(acc_t *vol_data, acc_t *vol_norm, int N, int mode,
 
 /* ReconstructorVolumeData::normalize_threed (libEM/reconstructor.cpp:315-390),
  * full-volume case; wiener adds 1 to each nonzero denominator (:376-390). */
-OR_EXPORT void or_normalize_w(acc_t *rdata, acc_t *norm, int N, int sqrtnorm, int wiener) {
-  const int nx = N + 2, ny = N, nz = N;
+OR_EXPORT void or_normalize_nz(acc_t *rdata, acc_t *norm, int N, int NZ, int sqrtnorm,
+                               int wiener) {
+  const int nx = N + 2, ny = N, nz = NZ;
   const long nnx = nx / 2, nnxy = (long)ny * nnx;
   for (int z = -nz / 2; z < nz / 2; z++) {
     for (int y = 0; y <= ny / 2; y++) {
@@ -599,6 +626,10 @@ OR_EXPORT void or_normalize_w(acc_t *rdata, acc_t *norm, int N, int sqrtnorm, in
       rdata[i + 1] /= dd;
     }
   }
+}
+
+OR_EXPORT void or_normalize_w(acc_t *rdata, acc_t *norm, int N, int sqrtnorm, int wiener) {
+  or_normalize_nz(rdata, norm, N, N, sqrtnorm, wiener);
 }
 
 OR_EXPORT void or_normalize(acc_t *rdata, acc_t *norm, int N, int sqrtnorm) {

@@ -67,6 +67,9 @@ def _lib(kind: str = "fp32"):
     lib.or_insert_pixels.argtypes = [ctypes.c_int, R, R, ctypes.c_int, _F, ctypes.c_long]
     lib.or_normalize.argtypes = [R, R, ctypes.c_int, ctypes.c_int]
     lib.or_normalize_w.argtypes = [R, R, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    lib.or_normalize_nz.argtypes = [R, R, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    lib.or_insert_batch_nz.argtypes = [R, R, ctypes.c_int, ctypes.c_int, ctypes.c_int, _F,
+                                       ctypes.c_int, _F, _F, ctypes.c_int, _F]
     lib.or_insert_slice_iter.argtypes = [R, R, ctypes.c_int, _F, _F, ctypes.c_int, ctypes.c_float,
                                          _F]
     lib.or_insert_slice_wiener.argtypes = [R, R, ctypes.c_int, ctypes.c_int, _F, _F, ctypes.c_int,
@@ -149,12 +152,13 @@ def compose(a: np.ndarray, b: np.ndarray) -> np.ndarray:
 class OracleVolume:
     """Un-normalised (complex, weight) accumulators in the reference layout."""
 
-    def __init__(self, N: int, precision: str = "fp32"):
+    def __init__(self, N: int, precision: str = "fp32", NZ: int | None = None):
         self.N = N
+        self.NZ = N if NZ is None else int(NZ)    # the volume's z size (square N x N slices)
         self.kind = precision
         dt = np.float32 if precision in ("fp32", "omp") else np.float64   # accumulators
-        self.data = np.zeros((N, N, N + 2), dt)
-        self.norm = np.zeros((N, N, N // 2 + 1), dt)
+        self.data = np.zeros((self.NZ, N, N + 2), dt)
+        self.norm = np.zeros((self.NZ, N, N // 2 + 1), dt)
 
     @property
     def lib(self):
@@ -168,9 +172,14 @@ class OracleVolume:
         rots = np.ascontiguousarray(rots, np.float32).reshape(n, 9)
         weights = np.ascontiguousarray(weights, np.float32).reshape(n)
         ops = np.ascontiguousarray(sym_ops(sym)).reshape(-1, 9)
-        rc = self.lib.or_insert_batch(_rp(self.data), _rp(self.norm), self.N, MODES[mode],
-                                      _fp(slices), n, _fp(rots), _fp(ops), ops.shape[0],
-                                      _fp(weights), int(bool(corners)))
+        if self.NZ != self.N:
+            rc = self.lib.or_insert_batch_nz(_rp(self.data), _rp(self.norm), self.N, self.NZ,
+                                             MODES[mode], _fp(slices), n, _fp(rots), _fp(ops),
+                                             ops.shape[0], _fp(weights))
+        else:
+            rc = self.lib.or_insert_batch(_rp(self.data), _rp(self.norm), self.N, MODES[mode],
+                                          _fp(slices), n, _fp(rots), _fp(ops), ops.shape[0],
+                                          _fp(weights), int(bool(corners)))
         if rc:
             raise RuntimeError(f"oracle insert failed rc={rc}")
 
@@ -262,13 +271,13 @@ class OracleVolume:
 
     def copy(self):
         o = OracleVolume.__new__(OracleVolume)
-        o.N, o.kind = self.N, self.kind
+        o.N, o.NZ, o.kind = self.N, self.NZ, self.kind
         o.data, o.norm = self.data.copy(), self.norm.copy()
         return o
 
     def normalize(self, sqrtnorm=False, wiener=False):
-        self.lib.or_normalize_w(_rp(self.data), _rp(self.norm), self.N, int(bool(sqrtnorm)),
-                                int(bool(wiener)))
+        self.lib.or_normalize_nz(_rp(self.data), _rp(self.norm), self.N, self.NZ,
+                                 int(bool(sqrtnorm)), int(bool(wiener)))
 
     def finish(self, doift=True, sqrtnorm=False, wiener=False):
         """FourierReconstructor::finish (libEM/reconstructor.cpp:1552-1641):
@@ -277,14 +286,14 @@ class OracleVolume:
         self.normalize(sqrtnorm, wiener)
         if not doift:
             return self.data, self.norm
-        N = self.N
+        N, NZ = self.N, self.NZ
         c = self.data.astype(np.float64).view(np.complex128)
-        real = np.fft.irfftn(c, s=(N, N, N), axes=(0, 1, 2), norm="forward")
+        real = np.fft.irfftn(c, s=(NZ, N, N), axes=(0, 1, 2), norm="forward")
         if self.data.dtype == np.float64:
-            real = real * (1.0 / (N * N * N))
+            real = real * (1.0 / (N * N * NZ))
         else:
-            real = real.astype(np.float32) * np.float32(1.0 / (N * N * N))
-        real = np.roll(real, (N // 2, N // 2, N // 2), axis=(0, 1, 2))
+            real = real.astype(np.float32) * np.float32(1.0 / (N * N * NZ))
+        real = np.roll(real, (NZ // 2, N // 2, N // 2), axis=(0, 1, 2))
         return real, self.norm
 
 

@@ -553,3 +553,59 @@ def test_projection_matches_oracle(gpu, ret_fourier, shift):
         c = got[:, 0] + 1j * got[:, 1]
         for y in range(1, N // 2):
             assert c[y] == np.conj(c[N - y])
+
+
+@pytest.mark.parametrize("mode", ["gauss_2", "gauss_5", "nearest_neighbor", "trilinear"])
+@pytest.mark.parametrize("NZ", [16, 48])
+def test_noncubic_volume_matches_oracle(gpu, mode, NZ):
+    """size=[N, N, NZ] (square slices, e.g. programs/e2tomogram.py:2024): the
+    z coordinate scaled by NZ, windows clamped to +-NZ/2, the volume
+    [NZ][N][N+2]; accumulators, finish(False) and finish(True) against the
+    oracle, through the batched call and the plain insert_slice loop."""
+    from eman2_b200 import EMData, Transform
+    N, n = 32, 12
+    sl, rt = rand_slices(N, n, 171), rand_rots(n, 172)
+    w = np.random.default_rng(173).uniform(0.5, 1.0, n).astype(np.float32)
+    o = oracle.OracleVolume(N, "fp32", NZ=NZ)
+    o.insert(sl, rt, w, mode, "c2")
+    for form in ("batched", "plain"):
+        from eman2_b200 import Reconstructors
+        r = Reconstructors.get("fourier", {"size": [N, N, NZ], "sym": "c2", "mode": mode})
+        r.setup()
+        if form == "batched":
+            r.insert_slices(sl, rt, w)
+        else:
+            for i in range(n):
+                img = EMData(sl[i], is_complex=True, attrs={"reconstruct_preproc": 1})
+                assert r.insert_slice(img, Transform(rt[i]), float(w[i])) == 0
+        d, nm = r.get_accumulators()
+        assert d.shape == (NZ, N, N + 2) and nm.shape == (NZ, N, N // 2 + 1)
+        assert rel(d, o.data) < RTOL_ACC and rel(nm, o.norm) < RTOL_ACC
+        assert np.array_equal(nm != 0, o.norm != 0)
+        real = r.finish(True).numpy()
+        want, _ = o.copy().finish(True)
+        assert real.shape == (NZ, N, N)
+        assert rel(real, want) < RTOL_FFT
+    r = Reconstructors.get("fourier", {"size": [N, N, NZ], "sym": "c2", "mode": mode})
+    r.setup()
+    r.insert_slices(sl, rt, w)
+    got = r.finish(False).numpy()
+    want, _ = o.copy().finish(False)
+    assert rel(got, want) < RTOL_ACC
+
+
+def test_noncubic_volume_refuses_cubic_only_paths(gpu):
+    from eman2_b200 import Reconstructors, Transform
+    from eman2_b200.batch import BatchReconstructor
+    from eman2_b200.exceptions import UnsupportedParameterException
+    from eman2_b200.particles import particle_meta
+    N, NZ = 32, 16
+    r = Reconstructors.get("fourier", {"size": [N, N, NZ], "sym": "c1"})
+    r.setup()
+    with pytest.raises(UnsupportedParameterException):
+        r.projection(Transform(), 1)
+    with pytest.raises(UnsupportedParameterException):
+        r.slice_agreement(rand_slices(N, 1, 1), rand_rots(1, 2), np.ones(1, np.float32))
+    b = BatchReconstructor([{"size": [N, N, NZ], "sym": "c1"}])
+    with pytest.raises(UnsupportedParameterException):
+        b.insert_particles([np.zeros((2, 24, 24), np.float32)], [particle_meta(rand_rots(2, 3))])

@@ -48,6 +48,10 @@ def test_abi_errors_without_touching_the_device(lib):
     p.sym = b"c1"
     assert lib.fr_create(ctypes.byref(p), ctypes.byref(h)) == 7   # odd size unsupported
     assert b"odd" in lib.fr_last_error()
+    p.nx, p.ny, p.nz = 32, 24, 32
+    assert lib.fr_create(ctypes.byref(p), ctypes.byref(h)) == 7   # slices must be square
+    p.nx, p.ny, p.nz = 32, 32, 17
+    assert lib.fr_create(ctypes.byref(p), ctypes.byref(h)) == 7   # odd z size
     p.nx = p.ny = p.nz = 32
     p.mode = 3
     assert lib.fr_create(ctypes.byref(p), ctypes.byref(h)) == 7   # gauss_3 not built
