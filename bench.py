@@ -166,10 +166,12 @@ def update_peaks():
 # ------------------------------------------------------------------ CPU baseline
 def cpu_sample(wl: dict, seed: int, budget_s: float = 15.0, max_n: int = 64, threads: int = 0):
     """The oracle's FP32 restatement (-O3 -ffast-math, OpenMP with private
-    volumes) on a bounded sample of the workload: prologue (numpy FFT) and
-    insertion.  Returns (particle-slices/s, sample size, threads, seconds)."""
+    volumes) on a bounded sample of the workload: prologue (numpy FFTs over
+    batches of particles on the host threads, the same slices as the
+    per-particle restatement) and insertion.  Returns (particle-slices/s,
+    sample size, threads, seconds)."""
     from eman2_b200.synth import make_particles
-    from oracle import oracle
+    from oracle import accuracy, oracle
     threads = threads or os.cpu_count() or 1
     N, box = wl["N"], wl["box"]
     n = max(1, min(max_n, threads))
@@ -180,9 +182,9 @@ def cpu_sample(wl: dict, seed: int, budget_s: float = 15.0, max_n: int = 64, thr
         ps = make_particles(box, n, seed=seed + k, snr=wl["snr"], shift=wl["shift"],
                             weights=wl["weights"], ctf=wl["ctf"])
         t0 = time.perf_counter()
-        sl = np.stack([oracle.particle_to_slice(ps.images[i], N, ps.shifts[i],
-                                                {"defocus": float(ps.defocus[i])} if wl["ctf"] else None)
-                       for i in range(n)])
+        sl = accuracy.slices_from_particles(ps.images, N, ps.shifts,
+                                            ps.defocus if wl["ctf"] else None, threads=threads,
+                                            chunk=max(1, -(-n // threads)))
         vol.insert_omp(sl, ps.rots, ps.weights, wl["mode"], wl["sym"], threads=threads)
         total_t += time.perf_counter() - t0
         total_n += n

@@ -48,12 +48,21 @@ int default_tile(int mode, int N, int nsym, int np) {
 
 // ------------------------------------------------------------------ batch
 namespace fr {
-// Scratch of one prologue group (see ProGroup).
+// Scratch of one prologue group (see ProGroup), with the group's own FFT
+// plans: the scratch, not a member handle, owns them, so a batched call
+// leaves no plans behind on the handles it served and a captured graph's
+// transforms use plans and a work area that only the graph holds.
 struct ProBufs {
   DevBuf img, slices, spec, t3d, img2;
+  std::unique_ptr<PlanCache> plans;
   ProScratch view() { return {&img, &slices, &spec, &t3d, &img2}; }
+  PlanCache &fft() {
+    if (!plans) plans.reset(new PlanCache());
+    return *plans;
+  }
   void release() {
     for (DevBuf *b : {&img, &slices, &spec, &t3d, &img2}) b->release();
+    plans.reset();
   }
 };
 
@@ -337,7 +346,7 @@ struct ProGroup {
   int N = 0, box = 0, n = 0;
   long nslices = 0;                     // symmetry copies of all its particles
   bool ctf = false;                     // the group runs the CTF round trip
-  fr_recon *lead = nullptr;             // its FFT plans serve the group
+  fr_recon *lead = nullptr;             // its symmetry table serves the group
   std::vector<int> jobs, first, count;  // job indices, first particle and count of each
   std::vector<long> slice0;             // each job's first slice in the group
   size_t meta_off = 0;                  // the group's block in the round's block
@@ -421,7 +430,7 @@ static int group_run(const std::vector<fr_recon *> &jobs, const ProGroup &g, Pro
                      bool exact_fft = false) {
   const float *const *tab = reinterpret_cast<const float *const *>(d_blk + group_tab_off(g.n));
   const PartSym *ps = reinterpret_cast<const PartSym *>(d_blk + group_psym_off(g.n));
-  TRY(prologue_run(g.lead->plans, b.view(), d_blk, nullptr, tab, g.n, g.box, g.N,
+  TRY(prologue_run(b.fft(), b.view(), d_blk, nullptr, tab, g.n, g.box, g.N,
                    g.lead->d_sym.as<float>(), g.lead->nsym, g.ctf, st, exact_fft, ps, g.nslices));
   if (!P) return FR_OK;
   const MetaView mv = meta_view(d_blk, g.n);

@@ -144,25 +144,95 @@ int to_device(const void *src, size_t bytes, DevBuf &stage, cudaStream_t st, con
 int from_device(void *dst, const void *dsrc, size_t bytes, cudaStream_t st);
 
 // ------------------------------------------------------------- cuFFT plans
+// Plans made with cuFFT's own work-area allocation turned off: every plan of
+// one cache runs in stream order on one stream at a time, so they share ONE
+// work area, sized to the largest plan, instead of holding one each (a cache
+// of power-of-two batches up to 1024 would otherwise keep twice the largest
+// transform's work area per direction).
 struct PlanCache {
   std::map<std::pair<int, int>, cufftHandle> r2c, c2r;   // key (N, batch)
+  std::map<cufftHandle, size_t> need;                   // each plan's work-area bytes
   cufftHandle c2r3 = 0, r2c3 = 0;
-  int c2r3_N = 0, r2c3_N = 0;
-  ~PlanCache() {
+  int c2r3_N = 0, r2c3_N = 0, c2r3_NZ = 0;
+  DevBuf work;
+  PlanCache() = default;
+  PlanCache(const PlanCache &) = delete;
+  PlanCache &operator=(const PlanCache &) = delete;
+  ~PlanCache() { release(); }
+  void release() {
     for (auto &kv : r2c) cufftDestroy(kv.second);
     for (auto &kv : c2r) cufftDestroy(kv.second);
     if (c2r3) cufftDestroy(c2r3);
     if (r2c3) cufftDestroy(r2c3);
+    r2c.clear();
+    c2r.clear();
+    need.clear();
+    c2r3 = r2c3 = 0;
+    c2r3_N = r2c3_N = c2r3_NZ = 0;
+    work.release();
+  }
+  // Drops one plan (a 3-D plan replaced by another size).
+  void drop(cufftHandle &h) {
+    if (!h) return;
+    need.erase(h);
+    cufftDestroy(h);
+    h = 0;
+  }
+  // A fresh handle with the work area left to this cache.
+  static int fresh(cufftHandle *h) {
+    CUFFT(cufftCreate(h));
+    const cufftResult r = cufftSetAutoAllocation(*h, 0);
+    if (r != CUFFT_SUCCESS) {
+      cufftDestroy(*h);
+      return fail(FR_ECUDA, "cufftSetAutoAllocation: cufft error %d", (int)r);
+    }
+    return FR_OK;
+  }
+  // Points h at the shared work area (grown to h's need) and at stream st.
+  int bind(cufftHandle h, cudaStream_t st) {
+    const size_t bytes = need[h];
+    if (bytes > work.cap) {
+      // a larger area replaces the old one; queued transforms that use the
+      // old one end first (the free waits for the device)
+      TRY(work.ensure(bytes));
+    }
+    if (bytes) CUFFT(cufftSetWorkArea(h, work.p));
+    CUFFT(cufftSetStream(h, st));
+    return FR_OK;
+  }
+  int make3d(cufftHandle *h, int nz, int ny, int nx, cufftType type) {
+    TRY(fresh(h));
+    size_t ws = 0;
+    const cufftResult r = cufftMakePlan3d(*h, nz, ny, nx, type, &ws);
+    if (r != CUFFT_SUCCESS) {
+      cufftDestroy(*h);
+      *h = 0;
+      return fail(r == CUFFT_ALLOC_FAILED ? FR_ENOMEM : FR_ECUDA,
+                  "cufftMakePlan3d(%d, %d, %d): cufft error %d", nz, ny, nx, (int)r);
+    }
+    need[*h] = ws;
+    return FR_OK;
   }
   int get3d_r2c(int N, cudaStream_t st, cufftHandle *out) {
     if (!r2c3 || r2c3_N != N) {
-      if (r2c3) cufftDestroy(r2c3);
-      r2c3 = 0;
-      CUFFT(cufftPlan3d(&r2c3, N, N, N, CUFFT_R2C));
+      drop(r2c3);
+      TRY(make3d(&r2c3, N, N, N, CUFFT_R2C));
       r2c3_N = N;
     }
-    CUFFT(cufftSetStream(r2c3, st));
+    TRY(bind(r2c3, st));
     *out = r2c3;
+    return FR_OK;
+  }
+  int get3d(int N, cudaStream_t st, cufftHandle *out, int NZ = 0) {
+    if (!NZ) NZ = N;
+    if (!c2r3 || c2r3_N != N || c2r3_NZ != NZ) {
+      drop(c2r3);
+      TRY(make3d(&c2r3, NZ, N, N, CUFFT_C2R));
+      c2r3_N = N;
+      c2r3_NZ = NZ;
+    }
+    TRY(bind(c2r3, st));
+    *out = c2r3;
     return FR_OK;
   }
   int get2d(bool forward, int N, int batch, cudaStream_t st, cufftHandle *out) {
@@ -171,15 +241,25 @@ struct PlanCache {
     auto it = m.find(key);
     if (it == m.end()) {
       cufftHandle h;
+      TRY(fresh(&h));
       int n[2] = {N, N};
       const int dist_r = N * N, dist_c = N * (N / 2 + 1);
-      if (forward)
-        CUFFT(cufftPlanMany(&h, 2, n, nullptr, 1, dist_r, nullptr, 1, dist_c, CUFFT_R2C, batch));
-      else
-        CUFFT(cufftPlanMany(&h, 2, n, nullptr, 1, dist_c, nullptr, 1, dist_r, CUFFT_C2R, batch));
+      size_t ws = 0;
+      const cufftResult r =
+          forward ? cufftMakePlanMany(h, 2, n, nullptr, 1, dist_r, nullptr, 1, dist_c, CUFFT_R2C,
+                                      batch, &ws)
+                  : cufftMakePlanMany(h, 2, n, nullptr, 1, dist_c, nullptr, 1, dist_r, CUFFT_C2R,
+                                      batch, &ws);
+      if (r != CUFFT_SUCCESS) {
+        cufftDestroy(h);
+        return fail(r == CUFFT_ALLOC_FAILED ? FR_ENOMEM : FR_ECUDA,
+                    "cufftMakePlanMany(%s, N %d, batch %d): cufft error %d",
+                    forward ? "R2C" : "C2R", N, batch, (int)r);
+      }
+      need[h] = ws;
       it = m.emplace(key, h).first;
     }
-    CUFFT(cufftSetStream(it->second, st));
+    TRY(bind(it->second, st));
     *out = it->second;
     return FR_OK;
   }
@@ -205,20 +285,6 @@ struct PlanCache {
         CUFFT(cufftExecC2R(h, (cufftComplex *)in + done * spec, (cufftReal *)out + done * img));
       done += b;
     }
-    return FR_OK;
-  }
-  int c2r3_NZ = 0;
-  int get3d(int N, cudaStream_t st, cufftHandle *out, int NZ = 0) {
-    if (!NZ) NZ = N;
-    if (!c2r3 || c2r3_N != N || c2r3_NZ != NZ) {
-      if (c2r3) cufftDestroy(c2r3);
-      c2r3 = 0;
-      CUFFT(cufftPlan3d(&c2r3, NZ, N, N, CUFFT_C2R));
-      c2r3_N = N;
-      c2r3_NZ = NZ;
-    }
-    CUFFT(cufftSetStream(c2r3, st));
-    *out = c2r3;
     return FR_OK;
   }
 };
