@@ -439,7 +439,12 @@ __device__ __forceinline__ void column_work(const Smem3 &S, const float *M, int 
   const int n2 = N >> 1;
   const float Nf = (float)N;
   const float *m0 = M, *m1 = M + 3, *nrm = M + 6;
-  const int lb = threadIdx.x & 15, lc = threadIdx.x >> 4;
+  // A warp's 32 columns are an 8 x 4 patch of the tile's (b, c) face: the
+  // band of columns a slice's plane reaches in a tile cuts compact patches
+  // less often than 16 x 2 strips, so fewer lanes idle (a model of every
+  // tile a slice meets: 65 % of a warp's tap slots used against 57 %).
+  const int wl = threadIdx.x & 31, wp = threadIdx.x >> 5;
+  const int lb = (wl & 7) + ((wp & 1) << 3), lc = (wl >> 3) + ((wp >> 1) << 2);
   const int vb = base[B] + lb, vc = base[C] + lc;
   if (vb > ext[B] || vc > ext[C]) return;
   const int tb = sg * vb, tc = sg * vc;
@@ -477,9 +482,10 @@ __device__ __forceinline__ void column_work(const Smem3 &S, const float *M, int 
 #pragma unroll
   for (int a = 0; a < 3; a++) inv0[a] = fabsf(m0[a]) > 1e-4f ? 1.0f / m0[a] : 0.0f;
   // The tile is held A-major while group A runs: cell (a, b, c) of the tile
-  // at a*T*T + c*T + b, so a thread's column is threadIdx.x + a*T*T and the
-  // lanes of a warp always fall in distinct banks, whatever taps they add.
-  const int col_addr = threadIdx.x;
+  // at a*T*T + c*T + b, so a thread's column is c*T + b + a*T*T; each quarter
+  // warp holds 8 consecutive b of one c, so a warp's float4 accesses take the
+  // minimum 4 shared wavefronts whatever taps its lanes add.
+  const int col_addr = lc * T + lb;
   const bool xzero_col = (A != 0) && (vb == 0);
   for (int y = r0; y <= r1; y++) {
     const int xm = S.xmax[y + n2];
@@ -495,6 +501,10 @@ __device__ __forceinline__ void column_work(const Smem3 &S, const float *M, int 
     const int c0 = max(0, (int)ceilf(xlo)), c1 = min(xm, (int)floorf(xhi));
     if (c0 > c1) continue;
     const float ry = S.rtab[y + n2];
+    // the row's slice values; pixel (0, y < 0) reads (0, -y) conjugated
+    const int w2s = (N >> 1) + 1;
+    const float2 *rowp = sl + (size_t)(y < 0 ? N + y : y) * w2s;
+    const float2 *mirp = sl + (size_t)(y < 0 ? -y : 0) * w2s;
     for (int x = c0; x <= c1; x++) {
       float xx, yy, zz;
       pixel_coords(S.rtab[x + n2], ry, M, Nf, xx, yy, zz);
@@ -505,7 +515,9 @@ __device__ __forceinline__ void column_work(const Smem3 &S, const float *M, int 
       const int a0 = win_start<MODE>(pa);
       const int k0 = max(a0, ta_lo), k1 = min(a0 + K - 1, ta_hi);
       if (k0 > k1) continue;
-      const float2 v = slice_value(sl, N, x, y);
+      const bool herm = (x == 0) && (y < 0);
+      float2 v = __ldg(herm ? mirp : rowp + x);
+      if (herm) v.y = -v.y;
       float f0 = 0.f, f1 = 0.f;
       if (MODE == MODE_GAUSS2 || MODE == MODE_GAUSS5) {
         if (A == 0) {
@@ -532,9 +544,10 @@ __device__ __forceinline__ void column_work(const Smem3 &S, const float *M, int 
           else if (A == 1) r = __fadd_rn(__fadd_rn(f0, d2), f1);
           else r = __fadd_rn(f0, d2);
           if (MODE == MODE_GAUSS2) {
+            // r >= 0 and h > 0, so f <= 0: fast_exp's f > 0 branch never runs
             const float f = __fmul_rn(-r, h);
-            const float g = (f > 0.0f || f < -19.98f)
-                                ? expf(f) : S.exp[__double2int_rz(__fma_rn((double)(-f), 50.0, 0.5))];
+            float g = S.exp[min(__double2int_rz(__fma_rn((double)(-f), 50.0, 0.5)), 999)];
+            if (f < -19.98f) g = expf(f);
             const float gg = __fmul_rn(g, w);
             vre = __fmul_rn(v.x, gg);
             vim = __fmul_rn(v.y, gg);
@@ -544,10 +557,12 @@ __device__ __forceinline__ void column_work(const Smem3 &S, const float *M, int 
             // in double as the reference forms it; -f*50 + 0.5 is exact in
             // double (a float times 50 plus 0.5 needs at most 31 bits), so
             // one DFMA and a truncating conversion give the reference's index.
+            // The entry is read for every tap (index clamped to the table) and
+            // replaced by exp(f) past it, so the common path has no branch;
+            // f <= 0 always (r >= 0, h > 0).
             const float f = __fmul_rn(-r, h);
-            float gg;
-            if (f > 0.0f || f < -19.98f) gg = expf(f);
-            else gg = S.exp[__double2int_rz(__fma_rn((double)(-f), 50.0, 0.5))];
+            float gg = S.exp[min(__double2int_rz(__fma_rn((double)(-f), 50.0, 0.5)), 999)];
+            if (f < -19.98f) gg = expf(f);
             vre = __fmul_rn(__fmul_rn(v.x, gg), w);
             vim = __fmul_rn(__fmul_rn(v.y, gg), w);
             vw = __fmul_rn(gg, w);
