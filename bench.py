@@ -639,13 +639,15 @@ def per_job_overhead(params, boxes, pool_imgs, pool_metas, stream, reps: int = 5
                     bp.recons[j].insert_particles(one_imgs[j], one_metas[j], schedule="scatter")
             plain_s = wall(plain_round, reps)
             multi_s = wall(lambda: insert_particles_multi(bp.recons, one_imgs, one_metas, stream),
-                           reps)
+                           reps * 8)
         finally:
             bp.close()
         bg = BatchReconstructor(params)
         try:
             g = bg.capture(boxes, [1] * nj, [True] * nj, stream=stream)
-            graph_s = wall(lambda: g.launch(one_imgs, one_metas), reps * 4)
+            # a replay lasts ~0.1 ms: enough of them that the closing wait
+            # and the clock ramp do not weigh on the per-replay time
+            graph_s = wall(lambda: g.launch(one_imgs, one_metas), reps * 40)
             g.close()
         finally:
             bg.close()
