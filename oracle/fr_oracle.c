@@ -389,6 +389,42 @@ OR_EXPORT int or_insert_slice(acc_t *vol_data, acc_t *vol_norm, int N, int mode,
                             ssnr, nssnr);
 }
 
+/* The pixel stream of do_insert_slice_work (libEM/reconstructor.cpp:1122-1210)
+ * for one slice of weight > 0 and its composed rotations t3d[nsym*9]: for
+ * every symmetry copy and every pixel inside the radius, (xx, yy, zz, re, im,
+ * weight) as that loop hands them to FourierPixelInserter3D::insert_pixel, six
+ * floats each, into px (room for cap pixels).  Returns the pixel count, or -1
+ * when px is too small.  Lets the reference's own inserter (oracle/_ref)
+ * consume exactly the pixels the restatement inserts. */
+OR_EXPORT long or_slice_pixels(int N, const float *slice, const float *t3d, int nsym, float weight,
+                               float *px, long cap) {
+  const float inx = (float)(N + 2), iny = (float)N;
+  const int nx = N + 2, ny = N, nz = N;
+  long n = 0;
+  for (int s = 0; s < nsym; s++) {
+    const float *M = t3d + 9 * s;
+    for (int y = (int)(-iny / 2); y < iny / 2; y++) {
+      for (int x = 0; x < inx / 2; x++) {
+        int r = or_hypot_fast_int(x, y);
+        if (r > iny / 2 && fabsf(inx - iny) < 3) continue;
+        if (n >= cap) return -1;
+        const float rx = (float)x / (inx - 2.0f), ry = (float)y / iny;
+        float xx = rx * M[0] + ry * M[3];
+        float yy = rx * M[1] + ry * M[4];
+        float zz = rx * M[2] + ry * M[5];
+        xx = xx * (float)(nx - 2);
+        yy = yy * (float)ny;
+        zz = zz * (float)nz;
+        real dre, dim;
+        or_slice_at(slice, nx, ny, x, y, &dre, &dim);
+        float *q = px + 6 * n++;
+        q[0] = xx; q[1] = yy; q[2] = zz; q[3] = (float)dre; q[4] = (float)dim; q[5] = weight;
+      }
+    }
+  }
+  return n;
+}
+
 /* The same into a volume of size [NZ][N][N+2] (square N x N slices; the z
  * coordinate scaled by NZ, libEM/reconstructor.cpp:1193-1196). */
 OR_EXPORT int or_insert_batch_nz(acc_t *vol_data, acc_t *vol_norm, int N, int NZ, int mode,

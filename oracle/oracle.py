@@ -20,6 +20,10 @@ FP32 path rounds each FFT result to float32, so it differs from an FFTW float
 transform at the 1e-7 level.  The restatement's insert_pixel/add_complex_at
 arithmetic is pinned bitwise against the reference's own inserter source
 (``build_ref.sh`` -> ``_ref/libfr_ref.so``; ``tests/test_oracle_ref.py``).
+The same source built with the reference's release flags
+(``_ref/libfr_ref_fast.so``) is the timed CPU reference arm
+(``ref_insert_threaded``): the reference's own inserter fed the restatement's
+pixel stream.
 """
 from __future__ import annotations
 
@@ -32,6 +36,9 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 BUILD = os.path.join(HERE, "_build")
 REF_SO = os.path.join(HERE, "_ref", "libfr_ref.so")
+# the same reference source built with its default release flags (-O3
+# -ffast-math, CMakeLists.txt): the timed CPU reference arm
+REF_FAST_SO = os.path.join(HERE, "_ref", "libfr_ref_fast.so")
 
 MODES = {"nearest_neighbor": 1, "gauss_2": 2, "gauss_5": 5, "trilinear": 6}
 
@@ -95,6 +102,63 @@ def _lib(kind: str = "fp32"):
                                             _F, ctypes.c_int, _F, ctypes.c_int]
     _libs[kind] = lib
     return lib
+
+
+def ref_available() -> bool:
+    """Whether the reference's own inserter was built (``build_ref.sh``)."""
+    return os.path.exists(REF_FAST_SO)
+
+
+def ref_insert_threaded(N: int, slices, rots, weights, mode: str, sym: str, threads: int,
+                        lib_path: str = REF_FAST_SO):
+    """The reference's own pixel inserter (FourierPixelInserter3D::insert_pixel,
+    libEM/reconstructor_tools.cpp, compiled from the reference tree with its
+    release flags) on every pixel of every symmetry copy of n slices, the
+    pixels formed by the restatement of do_insert_slice_work
+    (``or_slice_pixels``).  Particle p runs on host thread p % threads into
+    that thread's own volume, as parallel reconstructors do, and the volumes
+    are added at the end.  ``lib_path``: the release build (timing) or
+    ``REF_SO``, the strict build (bitwise checks).  Returns (data, norm)."""
+    from concurrent.futures import ThreadPoolExecutor
+    slices = np.ascontiguousarray(slices, np.float32).reshape(-1, N, N + 2)
+    n = slices.shape[0]
+    rots = np.asarray(rots, np.float32).reshape(n, 3, 3)
+    weights = np.asarray(weights, np.float32).reshape(n)
+    ops = sym_ops(sym).reshape(-1, 3, 3)
+    nsym = ops.shape[0]
+    ref = ctypes.CDLL(lib_path)
+    ref.ref_insert_pixels.argtypes = [ctypes.c_char_p, _F, _F, ctypes.c_int, _F, ctypes.c_long]
+    lib = _lib("fp32")
+    lib.or_slice_pixels.argtypes = [ctypes.c_int, _F, _F, ctypes.c_int, ctypes.c_float, _F,
+                                    ctypes.c_long]
+    lib.or_slice_pixels.restype = ctypes.c_long
+    cap = nsym * N * (N // 2 + 1)
+    threads = max(1, min(int(threads), n))
+
+    def run(t):
+        data = np.zeros((N, N, N + 2), np.float32)
+        norm = np.zeros((N, N, N // 2 + 1), np.float32)
+        px = np.empty(cap * 6, np.float32)
+        for p in range(t, n, threads):
+            if weights[p] == 0:
+                continue
+            t3d = np.ascontiguousarray(
+                np.stack([compose(rots[p], o) for o in ops]).astype(np.float32).reshape(-1))
+            k = lib.or_slice_pixels(N, _fp(slices[p]), _fp(t3d), nsym, float(weights[p]),
+                                    _fp(px), cap)
+            if k < 0:
+                raise RuntimeError("pixel stream overflow")
+            if ref.ref_insert_pixels(mode.encode(), _fp(data), _fp(norm), N, _fp(px), k):
+                raise RuntimeError(f"reference inserter refused mode {mode}")
+        return data, norm
+
+    with ThreadPoolExecutor(threads) as ex:
+        parts = list(ex.map(run, range(threads)))
+    data, norm = parts[0]
+    for d, m in parts[1:]:
+        data += d
+        norm += m
+    return data, norm
 
 
 def _fp(a: np.ndarray):

@@ -88,3 +88,27 @@ def test_add_complex_at_fast_indices_and_hermitian_rules():
                 else:
                     assert flat[idx] >= 1.0
                 del v
+
+
+@pytest.mark.parametrize("mode,sym", [("gauss_5", "d2"), ("gauss_2", "c3"), ("nearest_neighbor", "c1")])
+def test_reference_arm_matches_restatement(mode, sym):
+    """The timed CPU reference arm: the restatement's pixel stream of
+    do_insert_slice_work (or_slice_pixels) through the reference's own
+    inserter.  With the strict build and one thread it is bitwise the
+    restatement's insert_slice; with the release build on several threads it
+    stays within FP32 order noise of it."""
+    N, n = 24, 6
+    rng = np.random.default_rng(7)
+    sl = rng.normal(size=(n, N, N + 2)).astype(np.float32)
+    rots = np.stack([oracle.quaternion_matrix(q / np.linalg.norm(q))
+                     for q in rng.normal(size=(n, 4))]).astype(np.float32)
+    w = rng.uniform(0.5, 1.0, n).astype(np.float32)
+    want = oracle.OracleVolume(N, "fp32")
+    ops = oracle.sym_ops(sym).reshape(-1, 3, 3)
+    want.insert(sl, rots, w, mode=mode, sym=sym)
+    d, m = oracle.ref_insert_threaded(N, sl, rots, w, mode, sym, 1, lib_path=oracle.REF_SO)
+    assert np.array_equal(d, want.data) and np.array_equal(m, want.norm)
+    if oracle.ref_available():
+        d, m = oracle.ref_insert_threaded(N, sl, rots, w, mode, sym, 3)
+        assert oracle.rel_l2(d, want.data) < 1e-5 and oracle.rel_l2(m, want.norm) < 1e-5
+    assert ops.shape[0] >= 1
