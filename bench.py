@@ -229,16 +229,17 @@ def cpu_sample_reference(wl: dict, seed: int, budget_s: float = 15.0, max_n: int
     return total_n / total_t, total_n, threads, total_t
 
 
-def cpu_baseline_sample(wl: dict, seed: int, budget_s: float = 15.0, max_n: int = 64):
+def cpu_baseline_sample(wl: dict, seed: int, budget_s: float = 15.0, max_n: int = 64,
+                        threads: int = 0):
     """(rate, sample, threads, seconds, kind, what): the reference's own
     inserter when oracle/_ref was built, else the oracle's restatement."""
-    r = cpu_sample_reference(wl, seed, budget_s, max_n)
+    r = cpu_sample_reference(wl, seed, budget_s, max_n, threads)
     if r is not None:
         return (*r, "reference",
                 "reference FourierPixelInserter3D (libEM/reconstructor_tools.cpp, -O3 "
                 "-ffast-math) fed by the restated do_insert_slice_work pixel loop; numpy "
                 "prologue")
-    r = cpu_sample(wl, seed, budget_s, max_n)
+    r = cpu_sample(wl, seed, budget_s, max_n, threads)
     return (*r, "port", "the oracle's OpenMP restatement; numpy prologue")
 
 
@@ -1035,6 +1036,12 @@ def main():
         line["cpu_baseline"] = {"value": v, "unit": "particle-slices/s", "cores": thr,
                                 "kind": kind,
                                 "sample": f"{n} particles of the workload, {secs:.1f} s; {what}"}
+        # the same code on one host core (a per-core figure beside the all-core one)
+        v1, n1, _, secs1, _, _ = cpu_baseline_sample(wl, seed=7100, budget_s=6.0, max_n=8,
+                                                     threads=1)
+        line["cpu_baseline"]["single_thread"] = {
+            "value": v1, "unit": "particle-slices/s", "cores": 1,
+            "sample": f"{n1} particles, {secs1:.1f} s"}
     print(json.dumps(line))
 
 
