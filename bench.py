@@ -303,7 +303,7 @@ def fifo_latency(arrivals, service):
 
 
 def run_serving(dev, seed: int = 4242, nreq: int = 128, rate: float = 4.0, chunk: int = 2048,
-                plain_sample: int = 24, plain_every: int = 4):
+                plain_sample: int = 24, plain_every: int = 4, plain: bool = True):
     """The served form against the plain per-job GPU path on one request stream
     of the serving configuration (boxes 64-320 x1.5, 1,000-100,000 particles
     log-uniform, c1/c4/d7, gauss_2, CTF, chunks of 2048, Poisson arrivals).
@@ -333,6 +333,15 @@ def run_serving(dev, seed: int = 4242, nreq: int = 128, rate: float = 4.0, chunk
     torch.cuda.synchronize()
     exe.close()
     lat = sorted(j.done - j.req.arrival for j in srv.sched.done)
+    stream = (f"{nreq} requests, Poisson {rate}/s, boxes {'/'.join(map(str, SERVE_BOXES))} x1.5, "
+              f"1,000-100,000 particles log-uniform, c1/c4/d7, gauss_2, CTF, chunks of {chunk}; "
+              f"particles repeat within a box's pool of {chunk}")
+    served = {"p50_s": poi["p50_s"], "p99_s": poi["p99_s"], "p90_s": percentile(lat, 90),
+              "max_s": lat[-1] if lat else None, "particle_slices_per_s": parts / poi["wall_s"],
+              "wall_s": poi["wall_s"], "ticks": poi["ticks"], "requests": poi["requests"],
+              "particles": parts}
+    if not plain:
+        return {"served": served, "stream": stream}
 
     def per_job(r, k=None, schedule="scatter"):
         """Seconds for request r alone: setup, insert (k particles one per
@@ -377,19 +386,14 @@ def run_serving(dev, seed: int = 4242, nreq: int = 128, rate: float = 4.0, chunk
     plain_lat = fifo_latency([r.arrival for r in reqs], est)
     served_rate = parts / poi["wall_s"]
     return {
-        "served": {"p50_s": poi["p50_s"], "p99_s": poi["p99_s"],
-                   "p90_s": percentile(lat, 90), "max_s": lat[-1] if lat else None,
-                   "particle_slices_per_s": served_rate, "wall_s": poi["wall_s"],
-                   "ticks": poi["ticks"], "requests": poi["requests"], "particles": parts},
+        "served": served,
         "plain_per_particle": {"particle_slices_per_s": plain_rate,
                                "p50_s": percentile(plain_lat, 50), "p99_s": percentile(plain_lat, 99),
                                "sample": f"{plain_sample} particles of every {plain_every}th request, "
                                          "scaled to its count; latency from a FIFO single server "
                                          "under the same arrivals"},
         "speedup_served_vs_plain": served_rate / plain_rate,
-        "stream": f"{nreq} requests, Poisson {rate}/s, boxes {'/'.join(map(str, SERVE_BOXES))} x1.5, "
-                  f"1,000-100,000 particles log-uniform, c1/c4/d7, gauss_2, CTF, chunks of {chunk}; "
-                  f"particles repeat within a box's pool of {chunk}",
+        "stream": stream,
     }
 
 
@@ -1028,6 +1032,9 @@ def main():
         line["io"] = run_io(dev, WORKLOADS["c2"])
         line["batched"] = run_batched(dev)
         line["serving"] = run_serving(dev)
+        # the same configuration at the low end of its arrival rates, where
+        # the stream does not saturate the device: latency without queueing
+        line["serving_1rps"] = run_serving(dev, seed=4343, nreq=48, rate=1.0, plain=False)
     if not args.no_accuracy and ws == 1:
         import torch
         line["accuracy"] = run_accuracy(torch.device("cuda", local))
