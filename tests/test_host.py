@@ -280,3 +280,44 @@ def test_batched_call_argument_marshalling():
                          np.ones(1, np.float32))
     assert _meta_address(meta) == ctypes.cast(meta, ctypes.c_void_p).value
     assert _meta_address(None) is None
+
+
+def test_bench_workload_draws_follow_the_configurations():
+    """The batched and served legs' seeded draws have the configurations'
+    shapes: 64 jobs as 32 even/odd pairs over boxes 64-160 x1.5 with
+    500-50,000 particles each; requests over boxes 64-320 x1.5 with
+    1,000-100,000 particles in chunks of 2048 and Poisson arrivals."""
+    import ctypes
+
+    import bench
+    from eman2_b200 import _lib
+    jobs = bench.config3_jobs(33)
+    assert len(jobs) == 64
+    for a, b in zip(jobs[0::2], jobs[1::2]):
+        assert a["params"] == b["params"] and a["box"] == b["box"]
+        assert abs(a["count"] - b["count"]) <= 1
+    for j in jobs:
+        assert j["box"] in bench.BATCH_BOXES
+        assert j["params"]["size"] == [j["box"] * 3 // 2] * 3
+        assert j["params"]["sym"] in ("c1", "d7") and j["params"]["mode"] in ("gauss_2", "gauss_5")
+        assert 500 <= j["count"] <= 50_000
+    meta = (_lib.fr_particle * 2048)()
+    pools = {b: (np.zeros((2048, 1, 1), np.float32), meta) for b in bench.SERVE_BOXES}
+    reqs = bench.serving_requests(pools, 4242, 200, 4.0, 2048)
+    arr = np.array([r.arrival for r in reqs])
+    assert np.all(np.diff(arr) > 0) and 0.15 < np.mean(np.diff(arr)) < 0.35
+    for r in reqs:
+        assert 1000 <= r.particles <= 100_000
+        assert r.params["size"][0] in [b * 3 // 2 for b in bench.SERVE_BOXES]
+        assert r.params["sym"] in ("c1", "c4", "d7") and r.params["mode"] == "gauss_2"
+        assert sum(c[0].shape[0] for c in r.chunks) == r.particles
+        assert all(c[0].shape[0] <= 2048 for c in r.chunks)
+    assert ctypes.sizeof(meta) > 0
+
+
+def test_bench_fifo_latency():
+    """A single FIFO server: waits when busy, starts at arrival when idle."""
+    import bench
+    assert bench.fifo_latency([0.0, 1.0, 10.0], [2.0, 2.0, 1.0]) == [2.0, 3.0, 1.0]
+    assert bench.percentile([], 50) is None
+    assert bench.percentile([1.0, 2.0, 3.0], 50) == 2.0
