@@ -96,12 +96,18 @@ __global__ void __launch_bounds__(256) k_pad(const float *__restrict__ raw,
   // Region origin (box - N) // 2 (Python floor division).
   const int o = (box - N) >= 0 ? (box - N) / 2 : -((N - box + 1) / 2);
   float *dst = out + (size_t)p * N * N;
-  for (int i = blockIdx.y * blockDim.x + threadIdx.x; i < N * N; i += gridDim.y * blockDim.x) {
-    const int y = i / N, x = i % N;
+  // (row, column) of i carried along the stride instead of divided out
+  const int stride = gridDim.y * blockDim.x, dy = stride / N, dx = stride % N;
+  int i = blockIdx.y * blockDim.x + threadIdx.x;
+  int y = i / N, x = i % N;
+  for (; i < N * N; i += stride) {
     const int sy = y + o, sx = x + o;
     float v = 0.0f;
     if (sy >= 0 && sy < box && sx >= 0 && sx < box) v = __fsub_rn(src[(size_t)sy * box + sx], mean);
     dst[i] = v;
+    x += dx;
+    y += dy;
+    if (x >= N) { x -= N; y++; }
   }
 }
 
@@ -144,11 +150,10 @@ static int blocks_per_particle(int n, int npx, int waves) {
   return (int)std::max(1L, std::min<long>(want, (npx + 255) / 256));
 }
 
-// One spectrum element i of a particle: x CTF_SIGN at its frequency.
+// One spectrum element i = r*(N/2+1) + x of a particle: x CTF_SIGN at its
+// frequency.
 __device__ __forceinline__ void flip_one(cufftComplex *__restrict__ spec, const CtfDev &k, int N,
-                                         int i) {
-  const int w = N / 2 + 1;
-  const int r = i / w, x = i % w;
+                                         int i, int r, int x) {
   const int y = r < N / 2 ? r : r - N;
   const float s = __fmul_rn(hypot_int(x, y), k.ds);
   float gam;
@@ -176,8 +181,16 @@ __global__ void k_ctf_flip(cufftComplex *__restrict__ spec, const CtfDev *__rest
   const int p = blockIdx.y;
   const CtfDev k = c[p];
   if (k.on == 0.0f) return;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N * w; i += gridDim.x * blockDim.x)
-    flip_one(spec + (size_t)p * N * w, k, N, i);
+  // (row, column) of i carried along the stride instead of divided out
+  const int stride = gridDim.x * blockDim.x, dr = stride / w, dx = stride % w;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int r = i / w, x = i % w;
+  for (; i < N * w; i += stride) {
+    flip_one(spec + (size_t)p * N * w, k, N, i, r, x);
+    x += dx;
+    r += dr;
+    if (x >= w) { x -= w; r++; }
+  }
 }
 
 cudaError_t launch_ctf_flip_dev(cufftComplex *d_spec, const void *d_ctf, int n, int N,
@@ -256,8 +269,12 @@ __global__ void __launch_bounds__(256) k_shift_corner(SrcSel sel, const float *_
   if (txy) { tx = txy[(size_t)p * txy_stride]; ty = txy[(size_t)p * txy_stride + 1]; }
   const bool copy = fabsf(tx) < 1e-6f && fabsf(ty) < 1e-6f;
   const int h = N / 2;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N * N; i += gridDim.x * blockDim.x) {
-    const int yo = i / N, xo = i % N;
+  // (row, column) of i carried along the stride instead of divided out
+  const int stride = gridDim.x * blockDim.x, dyo = stride / N, dxo = stride % N;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int yo = i / N, xo = i % N;
+  for (; i < N * N; i += stride, xo += dxo, yo += dyo) {
+    if (xo >= N) { xo -= N; yo++; }
     // phase origin to corner (even N): out[y][x] = in[(y+N/2)%N][(x+N/2)%N]
     const int j = (yo + h) % N, ii = (xo + h) % N;
     float v;
