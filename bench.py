@@ -807,6 +807,15 @@ def run_target(dev, steps: int = 3, plain_n: int = 64):
         out["update_roofline"] = {"bound": "shared-memory FP32 atomics (3 per tap)",
                                   "achieved": taps, "peak": upd["smem_atom"], "unit": "taps/s",
                                   "frac": taps / upd["smem_atom"]}
+    # the HBM roofline of the same launch, as the main line's (algorithmic
+    # bytes over the launch time) with its committed DRAM traffic
+    peak, peak_kind = load_peaks()
+    V = (N // 2 + 1) * N * N
+    alg = 2048 * (8 * (N // 2 + 1) * N + 64) + 24 * V
+    achieved = alg / (gms / 1e3) / 1e9
+    out["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                       "frac": achieved / peak, "traffic": load_traffic("c4g2", 2048),
+                       "peak_source": peak_kind, "alg_bytes_per_launch": alg}
     return out
 
 
